@@ -1,0 +1,176 @@
+/*
+ * b200md.h -- C ABI of the B200 short-range MD engine (libb200md.so).
+ *
+ * One context (b200_ctx) holds one periodic orthogonal box of atoms resident
+ * in the GPU's memory, its cell-sorted neighbor list and its pair potential.
+ * A LAMMPS Pair/Fix subclass (lammps_b200/lammps/) or any other host drives
+ * it with plain pointers and sizes; no C++ or torch types cross the boundary.
+ *
+ * Reference interfaces replaced (LAMMPS 8 Aug 2014, paths inside the
+ * reference project):
+ *   - the GPU package's C ABI for pair styles: ljl_gpu_init / ljl_gpu_compute /
+ *     ljl_gpu_compute_n / ljl_gpu_clear (lib/gpu/lal_lj_ext.cpp:25-141, bound
+ *     in src/GPU/pair_lj_cut_gpu.cpp:42-65) and eam_gpu_* with
+ *     eam_gpu_compute_force (lib/gpu/lal_eam_ext.cpp:30,122,133);
+ *   - the per-step callbacks a Pair and a Fix implement: Pair::compute
+ *     (src/pair.h:135), FixNVE::initial_integrate / final_integrate
+ *     (src/fix_nve.cpp:65-142), Neighbor::build (src/neighbor.cpp:1380) and
+ *     the NeighList arrays (src/neigh_list.h:35-39).
+ *
+ * Conventions
+ *   - Every entry point returns an int status: 0 (B200_OK) or a negative
+ *     B200_ERR_* code; b200_last_error() gives the message.  Nothing throws
+ *     across the ABI and no kernel traps: device-side failures set a status
+ *     word that the host reads (as src/GPU/gpu_extra.h:26-64 maps the GPU
+ *     package's negative codes to error->all).
+ *   - Per-type tables use LAMMPS's 1-based layout flattened row-major:
+ *     an (ntypes+1) x (ntypes+1) array t has t[i*(ntypes+1)+j] for types
+ *     i,j in 1..ntypes; per-type vectors have ntypes+1 entries.
+ *   - Per-atom arrays are in the caller's order (the order of the last
+ *     b200_upload_atoms), xyz interleaved: x[3*i+0..2].
+ *   - Calls on one context are stream-ordered on that context's CUDA stream
+ *     and must come from one host thread at a time.
+ */
+#ifndef B200MD_H
+#define B200MD_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define B200MD_ABI_VERSION 1
+
+typedef struct b200_ctx b200_ctx;
+
+enum b200_status {
+  B200_OK = 0,
+  B200_ERR_ARG = -1,            /* bad argument (error->all "Illegal ...") */
+  B200_ERR_CUDA = -2,           /* CUDA runtime error */
+  B200_ERR_NOMEM = -3,          /* device allocation failed */
+  B200_ERR_STATE = -4,          /* call out of order (e.g. compute before atoms) */
+  B200_ERR_NEIGH_OVERFLOW = -5, /* "Neighbor list overflow, boost neigh_modify one" */
+  B200_ERR_BOX = -6,            /* box edge not larger than the ghost cutoff */
+  B200_ERR_LOST_ATOMS = -7,     /* non-finite coordinate or atom beyond one box image */
+  B200_ERR_TIMEOUT = -8         /* a bounded device wait expired */
+};
+
+enum b200_precision {
+  B200_PREC_FP64 = 0,  /* all pair arithmetic in FP64: the drop-in form */
+  B200_PREC_MIXED = 1  /* FP32 pair math on cell-relative coordinates,
+                          FP64 positions, per-atom force sums and global sums */
+};
+
+enum b200_pair_style { B200_PAIR_NONE = 0, B200_PAIR_LJ_CUT = 1, B200_PAIR_EAM = 2 };
+
+/* ---- context ------------------------------------------------------------ */
+
+/* Create a context on CUDA device `device` (replaces ljl_gpu_init's device
+   and precision selection, lib/gpu/lal_lj_ext.cpp:25-97). */
+int b200_create(int device, int precision, b200_ctx **out);
+/* Free every device buffer of the context (ljl_gpu_clear,
+   lib/gpu/lal_lj_ext.cpp:101-103). */
+int b200_destroy(b200_ctx *ctx);
+/* Message of the last failing call on this context (or of b200_create). */
+const char *b200_last_error(const b200_ctx *ctx);
+int b200_abi_version(void);
+/* Device bytes held by the context (ljl_gpu_bytes, lib/gpu/lal_lj_ext.cpp:139). */
+long long b200_bytes(const b200_ctx *ctx);
+
+/* ---- settings ----------------------------------------------------------- */
+
+/* Orthogonal periodic box [lo,hi) in every dimension (Domain boxlo/boxhi,
+   src/domain.cpp:213-217). */
+int b200_set_box(b200_ctx *ctx, const double lo[3], const double hi[3]);
+/* `neighbor skin bin` + `neigh_modify every/delay/check/one`
+   (src/neighbor.cpp:1731-1790).  one <= 0 picks a capacity from the density. */
+int b200_set_neighbor(b200_ctx *ctx, double skin, int every, int delay, int check, int one);
+/* Per-type masses, mass[1..ntypes] (Atom::mass). */
+int b200_set_mass(b200_ctx *ctx, int ntypes, const double *mass);
+/* pair_style lj/cut tables after PairLJCut::init_one
+   (src/pair_lj_cut.cpp:545-602): cutsq, lj1..lj4, offset. */
+int b200_set_lj(b200_ctx *ctx, int ntypes, const double *cutsq, const double *lj1,
+                const double *lj2, const double *lj3, const double *lj4, const double *offset);
+/* pair_style eam / eam/alloy / eam/fs spline tables after PairEAM::file2array
+   and array2spline (src/MANYBODY/pair_eam.cpp:488-719): 7 coefficients per
+   knot, knots 0..n (row 0 unused), tables back to back:
+     frho_spline[nfrho][nrho+1][7], rhor_spline[nrhor][nr+1][7],
+     z2r_spline[nz2r][nr+1][7];
+   type2frho[ntypes+1], type2rhor and type2z2r [(ntypes+1)^2]. */
+int b200_set_eam(b200_ctx *ctx, int ntypes, int nrho, double drho, int nr, double dr,
+                 double rhomax, double cutmax, int nfrho, const double *frho_spline, int nrhor,
+                 const double *rhor_spline, int nz2r, const double *z2r_spline,
+                 const int *type2frho, const int *type2rhor, const int *type2z2r);
+
+/* ---- atoms ----------------------------------------------------------------- */
+
+/* Copy n atoms to the device (AtomVec x, v, type, tag; ljl_gpu_compute's x
+   upload, lib/gpu/lal_base_atomic.cpp:176-241).  v may be NULL (zero). */
+int b200_upload_atoms(b200_ctx *ctx, int n, const double *x, const double *v, const int *type,
+                      const int *tag);
+/* Copy positions, velocities, forces and image flags back, in the caller's
+   order (NULL pointers are skipped; image is 3 ints per atom). */
+int b200_download_atoms(b200_ctx *ctx, double *x, double *v, double *f, int *image);
+int b200_natoms(const b200_ctx *ctx);
+
+/* ---- per-step entry points ------------------------------------------------- */
+
+/* Domain::pbc + periodic images + cell counting sort + full neighbor list
+   (Domain::pbc src/domain.cpp:478, CommBrick::borders src/comm_brick.cpp:696,
+   Neighbor::build src/neighbor.cpp:1380). */
+int b200_neigh_build(b200_ctx *ctx);
+/* Pair::compute(eflag, vflag) (src/pair.h:135): forces on the device;
+   eflag/vflag as Integrate::ev_set (src/integrate.cpp:114-149).  Energy and
+   virial go to *eng and virial[6] when the global flags are set (NULL to keep
+   them on the device), per-atom eatom[n] / vatom[6n] when the atom flags are
+   set (NULL to skip). */
+int b200_pair_compute(b200_ctx *ctx, int eflag, int vflag, double *eng, double virial[6],
+                      double *eatom, double *vatom);
+/* FixNVE::initial_integrate / final_integrate (src/fix_nve.cpp:65-142):
+   dtv = dt, dtf = 0.5 dt ftm2v. */
+int b200_nve_initial(b200_ctx *ctx, double dtv, double dtf);
+int b200_nve_final(b200_ctx *ctx, double dtf);
+
+/* Verlet::setup (src/verlet.cpp:88-142): wrap, build, forces at the current
+   step with energy and virial.  Returns the thermo row of that step. */
+int b200_setup(b200_ctx *ctx, double *row);
+/* Verlet::run(nsteps) (src/verlet.cpp:207-309) with fix nve and the
+   neighbor schedule of b200_set_neighbor, entirely on the device (CUDA graph
+   per step, rebuild taken by a device-side decision).  Every `thermo_every`
+   steps and at the last step a thermo row is recorded:
+     row = {step, sum m v^2, eng_vdwl, virial[0..5]}  (9 doubles)
+   from which the host forms Temp, E_pair, TotEng and Press exactly as
+   ComputeTemp/ComputePressure do.  rows may be NULL; *nrows receives the
+   number of rows recorded (at most maxrows are written). */
+int b200_run(b200_ctx *ctx, int nsteps, double dt, double ftm2v, int thermo_every, double *rows,
+             int maxrows, int *nrows);
+
+/* ---- neighbor list and diagnostics ----------------------------------------- */
+
+/* The half neighbor list that Neighbor::half_bin_newton
+   (src/neigh_half_bin.cpp:285-419) builds from the same atoms and index
+   order: per atom numneigh[n]; entries (jowner = caller index of the atom,
+   jimage = (sx+1)+3(sy+1)+9(sz+1) periodic image) concatenated in atom
+   order.  *total receives the entry count; at most cap entries are written. */
+int b200_neigh_half(b200_ctx *ctx, int *numneigh, int *jowner, int *jimage, long long cap,
+                    long long *total);
+/* Full-list statistics: entries (2x the half-list count), builds since
+   b200_setup (Neighbor::ncalls), dangerous builds (ndanger), the largest
+   per-atom count and the list capacity per atom. */
+int b200_neigh_stats(b200_ctx *ctx, long long *full_total, int *ncalls, int *ndanger,
+                     int *maxneigh, int *capacity);
+/* EAM density and embedding derivative of the last compute (PairEAM rho, fp). */
+int b200_get_rho_fp(b200_ctx *ctx, double *rho, double *fp);
+
+/* Launch shape of the pair kernels: threads per atom (1,2,4,8; 0 = chosen by
+   the autotuner on the next b200_setup) and threads per block. */
+int b200_set_launch(b200_ctx *ctx, int threads_per_atom, int block_size);
+int b200_get_launch(const b200_ctx *ctx, int *threads_per_atom, int *block_size);
+/* Kernel launches issued by the context since creation (for accounting). */
+long long b200_kernel_launches(const b200_ctx *ctx);
+/* CUDA stream of the context, as a void* (cudaStream_t). */
+void *b200_stream(const b200_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

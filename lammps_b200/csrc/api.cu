@@ -1,0 +1,889 @@
+// api.cu -- the C ABI of libb200md (include/b200md.h): context lifetime,
+// settings, atom transfer, setup, the per-step entry points and the
+// graph-captured Verlet loop.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "md_state.h"
+
+namespace {
+
+int set_err(b200_ctx *c, int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  return code;
+}
+
+#define CK(call)                                                                        \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      return set_err(c, B200_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                     __FILE__, __LINE__);                                               \
+  } while (0)
+
+template <typename T>
+cudaError_t dalloc(T **p, size_t count) {
+  if (*p) {
+    cudaFree(*p);
+    *p = nullptr;
+  }
+  if (count == 0) return cudaSuccess;
+  return cudaMalloc((void **)p, count * sizeof(T));
+}
+
+template <typename T>
+void dfree(T *&p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+void invalidate_graphs(b200_ctx *c) {
+  for (auto &g : c->step_exec)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+  c->graph_valid = false;
+}
+
+// ---- kernels local to the ABI ------------------------------------------------
+
+__global__ void k_upload(int n, int stride, const double *__restrict__ x,
+                         const double *__restrict__ v, const int *__restrict__ type,
+                         double4 *__restrict__ x4, double *__restrict__ vd,
+                         int *__restrict__ orig, int *__restrict__ image,
+                         int *__restrict__ cell) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  x4[i] = make_double4(x[3 * i], x[3 * i + 1], x[3 * i + 2], (double)type[i]);
+  vd[i] = v ? v[3 * i] : 0.0;
+  vd[stride + i] = v ? v[3 * i + 1] : 0.0;
+  vd[2 * stride + i] = v ? v[3 * i + 2] : 0.0;
+  orig[i] = i;
+  image[i] = md_img_pack(0, 0, 0);
+  cell[i] = 0;
+}
+
+__global__ void k_unsort(int n, int stride, const int *__restrict__ orig,
+                         const double4 *__restrict__ x4, const double *__restrict__ v,
+                         const double *__restrict__ f, const int *__restrict__ image,
+                         double *__restrict__ xo, double *__restrict__ vo, double *__restrict__ fo,
+                         int *__restrict__ io) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int o = orig[i];
+  if (xo) {
+    const double4 p = x4[i];
+    xo[3 * o] = p.x;
+    xo[3 * o + 1] = p.y;
+    xo[3 * o + 2] = p.z;
+  }
+  if (vo) {
+    vo[3 * o] = v[i];
+    vo[3 * o + 1] = v[stride + i];
+    vo[3 * o + 2] = v[2 * stride + i];
+  }
+  if (fo) {
+    fo[3 * o] = f[i];
+    fo[3 * o + 1] = f[stride + i];
+    fo[3 * o + 2] = f[2 * stride + i];
+  }
+  if (io) {
+    const int img = image[i];
+    io[3 * o] = (img & MD_IMGMASK) - MD_IMGMAX;
+    io[3 * o + 1] = ((img >> 10) & MD_IMGMASK) - MD_IMGMAX;
+    io[3 * o + 2] = ((img >> 20) & MD_IMGMASK) - MD_IMGMAX;
+  }
+}
+
+__global__ void k_unsort_scalar(int n, const int *__restrict__ orig, const double *__restrict__ a,
+                                double *__restrict__ out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[orig[i]] = a[i];
+}
+
+__global__ void k_full_total(int n, const int *__restrict__ numneigh,
+                             unsigned long long *__restrict__ total) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long v = i < n ? (unsigned long long)numneigh[i] : 0ull;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0 && v) atomicAdd(total, v);
+}
+
+// ---- host helpers --------------------------------------------------------------
+
+int check_ready(b200_ctx *c) {
+  if (!c->box_set) return set_err(c, B200_ERR_STATE, "box not set");
+  if (!c->have_atoms) return set_err(c, B200_ERR_STATE, "no atoms uploaded");
+  if (c->pstyle == B200_PAIR_NONE) return set_err(c, B200_ERR_STATE, "no pair style set");
+  if (!c->mass_set) return set_err(c, B200_ERR_STATE, "masses not set");
+  return B200_OK;
+}
+
+// Neighbor::init cutoffs (src/neighbor.cpp:255-279) and the cell grid
+int init_cutoffs_and_cells(b200_ctx *c) {
+  const int ntp1 = c->ntypes + 1;
+  double cutsq[TABSZ];
+  for (int i = 0; i < TABSZ; i++) cutsq[i] = 0.0;
+  if (c->pstyle == B200_PAIR_LJ_CUT) {
+    for (int i = 1; i <= c->ntypes; i++)
+      for (int j = 1; j <= c->ntypes; j++) cutsq[i * ntp1 + j] = c->lj.cutsq[i * ntp1 + j];
+  } else {
+    for (int i = 1; i <= c->ntypes; i++)
+      for (int j = 1; j <= c->ntypes; j++) cutsq[i * ntp1 + j] = c->eam.cutmax * c->eam.cutmax;
+  }
+  c->cutneighmax = 0.0;
+  c->cutforce_max = 0.0;
+  for (int i = 1; i <= c->ntypes; i++)
+    for (int j = 1; j <= c->ntypes; j++) {
+      const double cutoff = std::sqrt(cutsq[i * ntp1 + j]);
+      const double delta = cutoff > 0.0 ? c->skin : 0.0;
+      const double cut = cutoff + delta;
+      c->cutneighsq[i * ntp1 + j] = cut * cut;
+      if (cut > c->cutneighmax) c->cutneighmax = cut;
+      if (cutoff > c->cutforce_max) c->cutforce_max = cutoff;
+    }
+  if (!(c->cutneighmax > 0.0)) return set_err(c, B200_ERR_ARG, "zero neighbor cutoff");
+  long long ncells = 1;
+  for (int d = 0; d < 3; d++) {
+    // CommBrick::setup needs one periodic image per side: cutghost < prd
+    int maxneed = (int)(c->cutneighmax * 1 / c->box.prd[d]) + 1;
+    if (maxneed != 1)
+      return set_err(c, B200_ERR_BOX, "box edge %g in dim %d is not larger than the ghost cutoff %g",
+                     c->box.prd[d], d, c->cutneighmax);
+    int nc = (int)(c->box.prd[d] / c->cutneighmax);
+    if (nc < 1) nc = 1;
+    if (nc > MD_MAX_CELLS_DIM - 1) nc = MD_MAX_CELLS_DIM - 1;
+    c->box.ncell[d] = nc;
+    c->box.cs[d] = c->box.prd[d] / nc;
+    c->box.cinv[d] = nc / c->box.prd[d];
+    ncells *= nc;
+  }
+  if (ncells > (long long)4096 * 4096 - 1)
+    return set_err(c, B200_ERR_ARG, "too many cells (%lld)", ncells);
+  c->ncells = (int)ncells;
+  return B200_OK;
+}
+
+int upload_tables(b200_ctx *c) {
+  const int ntp1 = c->ntypes + 1;
+  std::vector<double> tab(TAB_COUNT * TABSZ, 0.0);
+  for (int k = 0; k < ntp1 * ntp1; k++) {
+    tab[TAB_CUTNEIGHSQ * TABSZ + k] = c->cutneighsq[k];
+    tab[TAB_CUTSQ * TABSZ + k] = c->lj.cutsq[k];
+    tab[TAB_LJ1 * TABSZ + k] = c->lj.lj1[k];
+    tab[TAB_LJ2 * TABSZ + k] = c->lj.lj2[k];
+    tab[TAB_LJ3 * TABSZ + k] = c->lj.lj3[k];
+    tab[TAB_LJ4 * TABSZ + k] = c->lj.lj4[k];
+    tab[TAB_OFFSET * TABSZ + k] = c->lj.offset[k];
+  }
+  std::vector<int> maps((MD_MAXTYPES + 1) + 2 * TABSZ, 0);
+  for (int k = 0; k < ntp1; k++) maps[k] = c->eam.type2frho[k];
+  for (int k = 0; k < ntp1 * ntp1; k++) {
+    maps[(MD_MAXTYPES + 1) + k] = c->eam.type2rhor[k];
+    maps[(MD_MAXTYPES + 1) + TABSZ + k] = c->eam.type2z2r[k];
+  }
+  if (!c->tables_dev) {
+    size_t bytes = TAB_COUNT * TABSZ * sizeof(double) + maps.size() * sizeof(int);
+    CK(cudaMalloc((void **)&c->tables_dev, bytes));
+    c->cutneighsq_dev = c->tables_dev + TAB_CUTNEIGHSQ * TABSZ;
+  }
+  CK(cudaMemcpyAsync(c->tables_dev, tab.data(), tab.size() * sizeof(double),
+                     cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->tables_dev + TAB_COUNT * TABSZ, maps.data(), maps.size() * sizeof(int),
+                     cudaMemcpyHostToDevice, c->stream));
+  std::vector<double> m(MD_MAXTYPES + 1, 1.0);
+  for (int t = 1; t <= c->ntypes; t++) m[t] = c->mass[t];
+  if (!c->mass_dev) CK(cudaMalloc((void **)&c->mass_dev, (MD_MAXTYPES + 1) * sizeof(double)));
+  CK(cudaMemcpyAsync(c->mass_dev, m.data(), m.size() * sizeof(double), cudaMemcpyHostToDevice,
+                     c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return B200_OK;
+}
+
+int alloc_cells(b200_ctx *c) {
+  if (c->ncells + 1 > c->ncell_alloc) {
+    int m = c->ncells + 1;
+    CK(dalloc(&c->cell_count, (size_t)m));
+    CK(dalloc(&c->cell_start, (size_t)m));
+    CK(dalloc(&c->scan_tmp, (size_t)4096 + 1));
+    c->ncell_alloc = m;
+  }
+  return B200_OK;
+}
+
+int alloc_list(b200_ctx *c, int capacity) {
+  long long need = (long long)capacity * c->stride;
+  if (need > c->nlist_alloc) {
+    CK(dalloc(&c->nlist, (size_t)need));
+    c->nlist_alloc = need;
+  }
+  c->capacity = capacity;
+  return B200_OK;
+}
+
+int default_capacity(const b200_ctx *c) {
+  const double vol = c->box.prd[0] * c->box.prd[1] * c->box.prd[2];
+  const double dens = c->n / vol;
+  const double pi = 3.14159265358979323846;
+  const double expect = 4.0 / 3.0 * pi * c->cutneighmax * c->cutneighmax * c->cutneighmax * dens;
+  int cap = (int)(1.4 * expect + 32.0);
+  cap = (cap + 7) & ~7;
+  return cap;
+}
+
+int read_status(b200_ctx *c) {
+  CK(cudaMemcpyAsync(c->status_host, c->status, ST_COUNT * sizeof(int), cudaMemcpyDeviceToHost,
+                     c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return B200_OK;
+}
+
+int status_errors(b200_ctx *c) {
+  if (c->status_host[ST_LOST])
+    return set_err(c, B200_ERR_LOST_ATOMS,
+                   "Lost atoms: a coordinate is not finite or moved beyond one box length");
+  if (c->status_host[ST_OVERFLOW])
+    return set_err(c, B200_ERR_NEIGH_OVERFLOW,
+                   "Neighbor list overflow, boost neigh_modify one (need %d, have %d)",
+                   c->status_host[ST_MAXNEIGH], c->capacity);
+  return B200_OK;
+}
+
+int pair_compute_dev(b200_ctx *c, bool ev, bool atom, double *eatom, double *vatom) {
+  cudaError_t e;
+  if (c->pstyle == B200_PAIR_LJ_CUT) e = md_lj_compute(c, ev, atom, eatom, vatom);
+  else e = md_eam_compute(c, ev, atom, eatom, vatom);
+  if (e != cudaSuccess) return set_err(c, B200_ERR_CUDA, "pair kernel: %s", cudaGetErrorString(e));
+  return B200_OK;
+}
+
+// rebuild with overflow recovery (host-synchronous; setup and b200_neigh_build)
+int rebuild_sync(b200_ctx *c) {
+  for (int attempt = 0; attempt < 3; attempt++) {
+    CK(cudaMemsetAsync(c->status + ST_MAXNEIGH, 0, sizeof(int), c->stream));
+    CK(cudaMemsetAsync(c->status + ST_OVERFLOW, 0, sizeof(int), c->stream));
+    CK(md_rebuild(c, nullptr));
+    int rc = read_status(c);
+    if (rc) return rc;
+    if (c->status_host[ST_LOST]) return status_errors(c);
+    if (!c->status_host[ST_OVERFLOW]) return B200_OK;
+    if (c->one_user > 0) return status_errors(c);
+    int need = c->status_host[ST_MAXNEIGH];
+    int cap = ((int)(need * 1.2) + 32 + 7) & ~7;
+    rc = alloc_list(c, cap);
+    if (rc) return rc;
+    invalidate_graphs(c);
+    // the atoms are already in cell order; the repeat rebuild keeps them
+  }
+  return set_err(c, B200_ERR_NEIGH_OVERFLOW, "Neighbor list overflow, boost neigh_modify one");
+}
+
+int autotune(b200_ctx *c) {
+  // Launch-shape search: time the force pass for each threads-per-atom
+  // value and keep the fastest (ties to fewer threads per atom).
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  float best = 1e30f;
+  int best_tpa = 1;
+  const int cand[4] = {1, 2, 4, 8};
+  for (int k = 0; k < 4; k++) {
+    c->tpa = cand[k];
+    int rc = pair_compute_dev(c, false, false, nullptr, nullptr);
+    if (rc) return rc;
+    CK(cudaEventRecord(e0, c->stream));
+    for (int r = 0; r < 3; r++) {
+      rc = pair_compute_dev(c, false, false, nullptr, nullptr);
+      if (rc) return rc;
+    }
+    CK(cudaEventRecord(e1, c->stream));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms < best * 0.97f) {
+      best = ms;
+      best_tpa = cand[k];
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->tpa = best_tpa;
+  c->tuned = true;
+  return B200_OK;
+}
+
+int capture_step(b200_ctx *c, bool out, double dtv, double dtf, cudaGraphExec_t *exec) {
+  cudaGraph_t g = nullptr;
+  CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = md_nve_initial(c, dtv, dtf);
+  if (e == cudaSuccess) e = md_decide(c);
+  if (e == cudaSuccess) e = md_rebuild(c, c->status + ST_REBUILD);
+  if (e == cudaSuccess) {
+    if (c->pstyle == B200_PAIR_LJ_CUT) e = md_lj_compute(c, out, false, nullptr, nullptr);
+    else e = md_eam_compute(c, out, false, nullptr, nullptr);
+  }
+  if (e == cudaSuccess) e = md_nve_final(c, dtf, out);
+  if (e == cudaSuccess && out) e = md_record_row(c);
+  cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
+  if (e != cudaSuccess || e2 != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return set_err(c, B200_ERR_CUDA, "graph capture: %s / %s", cudaGetErrorString(e),
+                   cudaGetErrorString(e2));
+  }
+  e = cudaGraphInstantiate(exec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return set_err(c, B200_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+  return B200_OK;
+}
+
+}  // namespace
+
+// ============================================================================
+// C ABI
+// ============================================================================
+
+extern "C" {
+
+int b200_abi_version(void) { return B200MD_ABI_VERSION; }
+
+int b200_create(int device, int precision, b200_ctx **out) {
+  if (!out) return B200_ERR_ARG;
+  *out = nullptr;
+  if (precision != B200_PREC_FP64 && precision != B200_PREC_MIXED) return B200_ERR_ARG;
+  b200_ctx *c = new (std::nothrow) b200_ctx();
+  if (!c) return B200_ERR_NOMEM;
+  c->device = device;
+  c->prec = precision;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&c->status, ST_COUNT * sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(c->status, 0, ST_COUNT * sizeof(int));
+  if (e == cudaSuccess) e = cudaMallocHost((void **)&c->status_host, ST_COUNT * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc((void **)&c->ev, 8 * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemset(c->ev, 0, 8 * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc((void **)&c->counter, sizeof(unsigned int));
+  if (e == cudaSuccess) e = cudaMemset(c->counter, 0, sizeof(unsigned int));
+  if (e != cudaSuccess) {
+    // report through a context so the caller can read the message
+    c->err = std::string("b200_create: ") + cudaGetErrorString(e);
+    *out = c;
+    return B200_ERR_CUDA;
+  }
+  *out = c;
+  return B200_OK;
+}
+
+int b200_destroy(b200_ctx *c) {
+  if (!c) return B200_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  invalidate_graphs(c);
+  dfree(c->x4); dfree(c->x4b); dfree(c->v); dfree(c->vb); dfree(c->f);
+  dfree(c->orig); dfree(c->origb); dfree(c->image); dfree(c->imageb); dfree(c->cell);
+  dfree(c->xr); dfree(c->xhold); dfree(c->rho); dfree(c->fp); dfree(c->fpf); dfree(c->mass_dev);
+  dfree(c->cell_count); dfree(c->cell_start); dfree(c->scan_tmp);
+  dfree(c->slot); dfree(c->perm); dfree(c->cell_tmp);
+  dfree(c->nlist); dfree(c->numneigh); dfree(c->partial); dfree(c->counter); dfree(c->ev);
+  dfree(c->status); dfree(c->rows); dfree(c->tables_dev);
+  dfree(c->eam.frho); dfree(c->eam.rhor); dfree(c->eam.z2r);
+  dfree(c->eam.frho_f); dfree(c->eam.rhor_f); dfree(c->eam.z2r_f);
+  if (c->status_host) cudaFreeHost(c->status_host);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return B200_OK;
+}
+
+const char *b200_last_error(const b200_ctx *c) { return c ? c->err.c_str() : "null context"; }
+
+long long b200_bytes(const b200_ctx *c) {
+  if (!c) return 0;
+  long long s = (long long)c->stride;
+  long long b = s * (2 * 32 + 2 * 24 + 24 + 5 * 4 + 16 + 32 + 16 + 4) + c->nlist_alloc * 4 +
+                (long long)c->ncell_alloc * 8;
+  return b;
+}
+
+int b200_set_box(b200_ctx *c, const double lo[3], const double hi[3]) {
+  if (!c || !lo || !hi) return B200_ERR_ARG;
+  for (int d = 0; d < 3; d++) {
+    if (!(hi[d] > lo[d]) || !std::isfinite(lo[d]) || !std::isfinite(hi[d]))
+      return set_err(c, B200_ERR_ARG, "Illegal box: hi <= lo in dim %d", d);
+    c->box.lo[d] = lo[d];
+    c->box.hi[d] = hi[d];
+    c->box.prd[d] = hi[d] - lo[d];  // Domain::set_global_box
+  }
+  c->box_set = true;
+  invalidate_graphs(c);
+  return B200_OK;
+}
+
+int b200_set_neighbor(b200_ctx *c, double skin, int every, int delay, int check, int one) {
+  if (!c) return B200_ERR_ARG;
+  if (!(skin >= 0.0) || every <= 0 || delay < 0)
+    return set_err(c, B200_ERR_ARG, "Illegal neighbor command");
+  c->skin = skin;
+  c->every = every;
+  c->delay = delay;
+  c->check = check ? 1 : 0;
+  c->one_user = one > 0 ? one : 0;
+  invalidate_graphs(c);
+  return B200_OK;
+}
+
+int b200_set_mass(b200_ctx *c, int ntypes, const double *mass) {
+  if (!c || !mass || ntypes < 1 || ntypes > MD_MAXTYPES)
+    return set_err(c, B200_ERR_ARG, "Illegal mass: ntypes must be 1..%d", MD_MAXTYPES);
+  for (int t = 1; t <= ntypes; t++) {
+    if (!(mass[t] > 0.0)) return set_err(c, B200_ERR_ARG, "Invalid mass value for type %d", t);
+    c->mass[t] = mass[t];
+  }
+  if (c->ntypes && c->ntypes != ntypes)
+    return set_err(c, B200_ERR_ARG, "mass table has %d types, pair style %d", ntypes, c->ntypes);
+  c->ntypes = ntypes;
+  c->mass_set = true;
+  invalidate_graphs(c);
+  return B200_OK;
+}
+
+int b200_set_lj(b200_ctx *c, int ntypes, const double *cutsq, const double *lj1, const double *lj2,
+                const double *lj3, const double *lj4, const double *offset) {
+  if (!c || ntypes < 1 || ntypes > MD_MAXTYPES || !cutsq || !lj1 || !lj2 || !lj3 || !lj4 || !offset)
+    return set_err(c, B200_ERR_ARG, "Illegal lj/cut tables");
+  if (c->ntypes && c->ntypes != ntypes)
+    return set_err(c, B200_ERR_ARG, "lj/cut tables have %d types, masses %d", ntypes, c->ntypes);
+  const int ntp1 = ntypes + 1;
+  for (int i = 0; i < ntp1 * ntp1; i++) {
+    c->lj.cutsq[i] = cutsq[i];
+    c->lj.lj1[i] = lj1[i];
+    c->lj.lj2[i] = lj2[i];
+    c->lj.lj3[i] = lj3[i];
+    c->lj.lj4[i] = lj4[i];
+    c->lj.offset[i] = offset[i];
+  }
+  c->ntypes = ntypes;
+  c->pstyle = B200_PAIR_LJ_CUT;
+  invalidate_graphs(c);
+  return B200_OK;
+}
+
+int b200_set_eam(b200_ctx *c, int ntypes, int nrho, double drho, int nr, double dr, double rhomax,
+                 double cutmax, int nfrho, const double *frho_spline, int nrhor,
+                 const double *rhor_spline, int nz2r, const double *z2r_spline,
+                 const int *type2frho, const int *type2rhor, const int *type2z2r) {
+  if (!c || ntypes < 1 || ntypes > MD_MAXTYPES || nrho < 3 || nr < 3 || !(drho > 0) || !(dr > 0) ||
+      nfrho < 1 || nrhor < 1 || nz2r < 1 || !frho_spline || !rhor_spline || !z2r_spline ||
+      !type2frho || !type2rhor || !type2z2r || !(cutmax > 0))
+    return set_err(c, B200_ERR_ARG, "Illegal eam tables");
+  if (c->ntypes && c->ntypes != ntypes)
+    return set_err(c, B200_ERR_ARG, "eam tables have %d types, masses %d", ntypes, c->ntypes);
+  const int ntp1 = ntypes + 1;
+  for (int i = 1; i <= ntypes; i++) {
+    if (type2frho[i] < 0 || type2frho[i] >= nfrho)
+      return set_err(c, B200_ERR_ARG, "type2frho out of range");
+    for (int j = 1; j <= ntypes; j++) {
+      if (type2rhor[i * ntp1 + j] < 0 || type2rhor[i * ntp1 + j] >= nrhor ||
+          type2z2r[i * ntp1 + j] < 0 || type2z2r[i * ntp1 + j] >= nz2r)
+        return set_err(c, B200_ERR_ARG, "type2rhor/type2z2r out of range");
+    }
+  }
+  EAMDev &E = c->eam;
+  E.nrho = nrho;
+  E.nr = nr;
+  E.drho = drho;
+  E.dr = dr;
+  E.rdr = 1.0 / dr;      // PairEAM::array2spline (src/MANYBODY/pair_eam.cpp:700-701)
+  E.rdrho = 1.0 / drho;
+  E.rhomax = rhomax;
+  E.cutmax = cutmax;
+  E.cutforcesq = cutmax * cutmax;  // PairEAM::init_one (:423)
+  E.nfrho = nfrho;
+  E.nrhor = nrhor;
+  E.nz2r = nz2r;
+  for (int i = 0; i < ntp1; i++) E.type2frho[i] = i == 0 ? 0 : type2frho[i];
+  for (int i = 0; i < ntp1 * ntp1; i++) {
+    E.type2rhor[i] = (i / ntp1 == 0 || i % ntp1 == 0) ? 0 : type2rhor[i];
+    E.type2z2r[i] = (i / ntp1 == 0 || i % ntp1 == 0) ? 0 : type2z2r[i];
+  }
+  // repack [table][knot][7] -> [table][knot][8]; FP32 copies reordered
+  // [c3 c4 c5 c6 | c0 c1 c2 0] for one-float4 value / derivative loads
+  auto pack = [&](const double *src, int ntab, int nk, double **dd, float **df) -> int {
+    std::vector<double> d8((size_t)ntab * (nk + 1) * 8, 0.0);
+    std::vector<float> f8((size_t)ntab * (nk + 1) * 8, 0.0f);
+    for (size_t r = 0; r < (size_t)ntab * (nk + 1); r++) {
+      for (int k = 0; k < 7; k++) d8[r * 8 + k] = src[r * 7 + k];
+      for (int k = 0; k < 4; k++) f8[r * 8 + k] = (float)src[r * 7 + 3 + k];
+      for (int k = 0; k < 3; k++) f8[r * 8 + 4 + k] = (float)src[r * 7 + k];
+    }
+    CK(dalloc(dd, d8.size()));
+    CK(dalloc(df, f8.size()));
+    CK(cudaMemcpy(*dd, d8.data(), d8.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(*df, f8.data(), f8.size() * sizeof(float), cudaMemcpyHostToDevice));
+    return B200_OK;
+  };
+  int rc = pack(frho_spline, nfrho, nrho, &E.frho, &E.frho_f);
+  if (!rc) rc = pack(rhor_spline, nrhor, nr, &E.rhor, &E.rhor_f);
+  if (!rc) rc = pack(z2r_spline, nz2r, nr, &E.z2r, &E.z2r_f);
+  if (rc) return rc;
+  c->ntypes = ntypes;
+  c->pstyle = B200_PAIR_EAM;
+  invalidate_graphs(c);
+  return B200_OK;
+}
+
+int b200_upload_atoms(b200_ctx *c, int n, const double *x, const double *v, const int *type,
+                      const int *tag) {
+  (void)tag;
+  if (!c || n < 1 || !x || !type) return set_err(c, B200_ERR_ARG, "Illegal atoms");
+  if (n > MD_MAX_ATOMS) return set_err(c, B200_ERR_ARG, "too many atoms (%d > %d)", n, MD_MAX_ATOMS);
+  if (c->ntypes < 1) return set_err(c, B200_ERR_STATE, "set masses or a pair style before atoms");
+  for (int i = 0; i < n; i++)
+    if (type[i] < 1 || type[i] > c->ntypes)
+      return set_err(c, B200_ERR_ARG, "Invalid atom type %d of atom %d", type[i], i);
+  CK(cudaSetDevice(c->device));
+  invalidate_graphs(c);
+  if (n > c->nalloc) {
+    const int stride = (n + 31) & ~31;
+    CK(dalloc(&c->x4, stride));
+    CK(dalloc(&c->x4b, stride));
+    CK(dalloc(&c->v, 3 * (size_t)stride));
+    CK(dalloc(&c->vb, 3 * (size_t)stride));
+    CK(dalloc(&c->f, 3 * (size_t)stride));
+    CK(dalloc(&c->orig, stride));
+    CK(dalloc(&c->origb, stride));
+    CK(dalloc(&c->image, stride));
+    CK(dalloc(&c->imageb, stride));
+    CK(dalloc(&c->cell, stride));
+    CK(dalloc(&c->xr, stride));
+    CK(dalloc(&c->xhold, stride));
+    CK(dalloc(&c->rho, stride));
+    CK(dalloc(&c->fp, stride));
+    CK(dalloc(&c->fpf, stride));
+    CK(dalloc(&c->slot, stride));
+    CK(dalloc(&c->perm, stride));
+    CK(dalloc(&c->cell_tmp, stride));
+    CK(dalloc(&c->numneigh, stride));
+    c->partial_blocks = stride / 16 + 64;
+    CK(dalloc(&c->partial, (size_t)c->partial_blocks * 8));
+    c->nalloc = n;
+    c->stride = stride;
+    c->nlist_alloc = 0;
+    dfree(c->nlist);
+  }
+  c->n = n;
+  CK(cudaMemsetAsync(c->f, 0, 3 * (size_t)c->stride * sizeof(double), c->stream));
+  double *dx = nullptr, *dv = nullptr;
+  int *dt = nullptr;
+  CK(cudaMallocAsync((void **)&dx, 3 * (size_t)n * sizeof(double), c->stream));
+  if (v) CK(cudaMallocAsync((void **)&dv, 3 * (size_t)n * sizeof(double), c->stream));
+  CK(cudaMallocAsync((void **)&dt, (size_t)n * sizeof(int), c->stream));
+  CK(cudaMemcpyAsync(dx, x, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  if (v) CK(cudaMemcpyAsync(dv, v, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(dt, type, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  k_upload<<<md_blocks(n, 256), 256, 0, c->stream>>>(n, c->stride, dx, dv, dt, c->x4, c->v,
+                                                     c->orig, c->image, c->cell);
+  c->launches++;
+  CK(cudaGetLastError());
+  CK(cudaFreeAsync(dx, c->stream));
+  if (dv) CK(cudaFreeAsync(dv, c->stream));
+  CK(cudaFreeAsync(dt, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->have_atoms = true;
+  c->sorted_once = false;
+  return B200_OK;
+}
+
+int b200_natoms(const b200_ctx *c) { return c ? c->n : 0; }
+
+int b200_download_atoms(b200_ctx *c, double *x, double *v, double *f, int *image) {
+  if (!c) return B200_ERR_ARG;
+  if (!c->have_atoms) return set_err(c, B200_ERR_STATE, "no atoms uploaded");
+  CK(cudaSetDevice(c->device));
+  const int n = c->n;
+  double *dx = nullptr, *dv = nullptr, *df = nullptr;
+  int *di = nullptr;
+  if (x) CK(cudaMallocAsync((void **)&dx, 3 * (size_t)n * sizeof(double), c->stream));
+  if (v) CK(cudaMallocAsync((void **)&dv, 3 * (size_t)n * sizeof(double), c->stream));
+  if (f) CK(cudaMallocAsync((void **)&df, 3 * (size_t)n * sizeof(double), c->stream));
+  if (image) CK(cudaMallocAsync((void **)&di, 3 * (size_t)n * sizeof(int), c->stream));
+  k_unsort<<<md_blocks(n, 256), 256, 0, c->stream>>>(n, c->stride, c->orig, c->x4, c->v, c->f,
+                                                     c->image, dx, dv, df, di);
+  c->launches++;
+  CK(cudaGetLastError());
+  if (x) CK(cudaMemcpyAsync(x, dx, 3 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (v) CK(cudaMemcpyAsync(v, dv, 3 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (f) CK(cudaMemcpyAsync(f, df, 3 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (image) CK(cudaMemcpyAsync(image, di, 3 * (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  if (dx) CK(cudaFreeAsync(dx, c->stream));
+  if (dv) CK(cudaFreeAsync(dv, c->stream));
+  if (df) CK(cudaFreeAsync(df, c->stream));
+  if (di) CK(cudaFreeAsync(di, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return B200_OK;
+}
+
+static int prepare(b200_ctx *c) {
+  int rc = check_ready(c);
+  if (rc) return rc;
+  CK(cudaSetDevice(c->device));
+  rc = init_cutoffs_and_cells(c);
+  if (!rc) rc = upload_tables(c);
+  if (!rc) rc = alloc_cells(c);
+  if (!rc && (c->capacity == 0 || c->one_user > 0 || !c->nlist)) {
+    int cap = c->one_user > 0 ? c->one_user : (c->capacity > 0 ? c->capacity : default_capacity(c));
+    rc = alloc_list(c, cap);
+  }
+  return rc;
+}
+
+int b200_neigh_build(b200_ctx *c) {
+  if (!c) return B200_ERR_ARG;
+  int rc = prepare(c);
+  if (rc) return rc;
+  rc = rebuild_sync(c);
+  if (rc) return rc;
+  c->sorted_once = true;
+  return B200_OK;
+}
+
+int b200_pair_compute(b200_ctx *c, int eflag, int vflag, double *eng, double virial[6],
+                      double *eatom, double *vatom) {
+  if (!c) return B200_ERR_ARG;
+  if (!c->sorted_once) return set_err(c, B200_ERR_STATE, "neighbor list not built");
+  CK(cudaSetDevice(c->device));
+  // Integrate::ev_set flags: eflag 1 global, 2 per-atom; vflag 1|2 global, 4 per-atom
+  const bool eg = (eflag & 1) != 0, ea = (eflag & 2) != 0;
+  const bool vg = (vflag % 4) != 0, va = (vflag & 4) != 0;
+  const bool ev = eg || ea || vg || va;
+  const bool atom = ea || va;
+  double *de = nullptr, *dv = nullptr;
+  const int n = c->n;
+  if (ea && eatom) {
+    CK(cudaMallocAsync((void **)&de, (size_t)n * sizeof(double), c->stream));
+    CK(cudaMemsetAsync(de, 0, (size_t)n * sizeof(double), c->stream));
+  }
+  if (va && vatom) CK(cudaMallocAsync((void **)&dv, 6 * (size_t)n * sizeof(double), c->stream));
+  int rc = pair_compute_dev(c, ev, atom, de, dv);
+  if (rc) return rc;
+  double h[8];
+  if (ev) CK(cudaMemcpyAsync(h, c->ev, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (de) CK(cudaMemcpyAsync(eatom, de, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (dv) CK(cudaMemcpyAsync(vatom, dv, 6 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (de) CK(cudaFreeAsync(de, c->stream));
+  if (dv) CK(cudaFreeAsync(dv, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (ev) {
+    if (eg && eng) *eng = h[0];
+    if (vg && virial)
+      for (int k = 0; k < 6; k++) virial[k] = h[1 + k];
+  }
+  return B200_OK;
+}
+
+int b200_nve_initial(b200_ctx *c, double dtv, double dtf) {
+  if (!c) return B200_ERR_ARG;
+  if (!c->sorted_once) return set_err(c, B200_ERR_STATE, "neighbor list not built");
+  CK(cudaSetDevice(c->device));
+  CK(md_nve_initial(c, dtv, dtf));
+  CK(cudaStreamSynchronize(c->stream));
+  return B200_OK;
+}
+
+int b200_nve_final(b200_ctx *c, double dtf) {
+  if (!c) return B200_ERR_ARG;
+  if (!c->sorted_once) return set_err(c, B200_ERR_STATE, "neighbor list not built");
+  CK(cudaSetDevice(c->device));
+  CK(md_nve_final(c, dtf, false));
+  CK(cudaStreamSynchronize(c->stream));
+  return B200_OK;
+}
+
+int b200_setup(b200_ctx *c, double *row) {
+  if (!c) return B200_ERR_ARG;
+  int rc = prepare(c);
+  if (rc) return rc;
+  CK(cudaMemsetAsync(c->status, 0, ST_COUNT * sizeof(int), c->stream));
+  rc = rebuild_sync(c);
+  if (rc) return rc;
+  c->sorted_once = true;
+  // Verlet::setup resets the build counter after the setup build
+  CK(cudaMemsetAsync(c->status + ST_NCALLS, 0, sizeof(int), c->stream));
+  CK(cudaMemsetAsync(c->status + ST_AGO, 0, sizeof(int), c->stream));
+  if (c->tpa == 0 || !c->tuned) {
+    if (c->tpa == 0) {
+      rc = autotune(c);
+      if (rc) return rc;
+    }
+    c->tuned = true;
+  }
+  rc = pair_compute_dev(c, true, false, nullptr, nullptr);
+  if (rc) return rc;
+  CK(md_ke(c));
+  double h[8];
+  CK(cudaMemcpyAsync(h, c->ev, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (row) {
+    row[0] = 0.0;
+    row[1] = h[7];
+    row[2] = h[0];
+    for (int k = 0; k < 6; k++) row[3 + k] = h[1 + k];
+  }
+  return B200_OK;
+}
+
+int b200_run(b200_ctx *c, int nsteps, double dt, double ftm2v, int thermo_every, double *rows,
+             int maxrows, int *nrows) {
+  if (!c || nsteps < 0) return B200_ERR_ARG;
+  if (!c->sorted_once) return set_err(c, B200_ERR_STATE, "b200_setup not called");
+  CK(cudaSetDevice(c->device));
+  const double dtv = dt, dtf = 0.5 * dt * ftm2v;  // FixNVE::init (src/fix_nve.cpp:52-59)
+  // thermo rows: room for every output step of this run
+  int nout = 1 + (thermo_every > 0 ? nsteps / thermo_every : 0);
+  if (nout > c->rows_cap) {
+    CK(dalloc(&c->rows, (size_t)9 * nout));
+    c->rows_cap = nout;
+    invalidate_graphs(c);
+  }
+  if (c->graph_valid && (c->graph_dt != dtv || c->graph_ftm2v != ftm2v || c->graph_tpa != c->tpa))
+    invalidate_graphs(c);
+  if (!c->graph_valid) {
+    int rc = capture_step(c, false, dtv, dtf, &c->step_exec[0]);
+    if (!rc) rc = capture_step(c, true, dtv, dtf, &c->step_exec[1]);
+    if (rc) return rc;
+    c->graph_valid = true;
+    c->graph_dt = dtv;
+    c->graph_ftm2v = ftm2v;
+    c->graph_tpa = c->tpa;
+  }
+  CK(cudaMemsetAsync(c->status + ST_ROW, 0, sizeof(int), c->stream));
+  CK(cudaMemsetAsync(c->status + ST_OVERFLOW, 0, sizeof(int), c->stream));
+  // host view of the current step for the output schedule
+  CK(cudaMemcpyAsync(c->status_host, c->status, ST_COUNT * sizeof(int), cudaMemcpyDeviceToHost,
+                     c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  long long step0 = ((long long)(unsigned int)c->status_host[ST_STEP_HI] << 32) |
+                    (long long)(unsigned int)c->status_host[ST_STEP_LO];
+  const long long last = step0 + nsteps;
+  for (long long s = step0 + 1; s <= last; s++) {
+    const bool out = (s == last) || (thermo_every > 0 && s % thermo_every == 0);
+    CK(cudaGraphLaunch(c->step_exec[out ? 1 : 0], c->stream));
+  }
+  c->launches += 0;  // kernel launches inside graphs are counted at capture
+  int rc = read_status(c);
+  if (rc) return rc;
+  int nr = c->status_host[ST_ROW];
+  if (nrows) *nrows = nr;
+  if (rows && maxrows > 0 && nr > 0) {
+    int cpy = nr < maxrows ? nr : maxrows;
+    if (cpy > c->rows_cap) cpy = c->rows_cap;
+    CK(cudaMemcpy(rows, c->rows, (size_t)9 * cpy * sizeof(double), cudaMemcpyDeviceToHost));
+  }
+  return status_errors(c);
+}
+
+int b200_neigh_half(b200_ctx *c, int *numneigh, int *jowner, int *jimage, long long cap,
+                    long long *total) {
+  if (!c) return B200_ERR_ARG;
+  if (!c->sorted_once) return set_err(c, B200_ERR_STATE, "neighbor list not built");
+  CK(cudaSetDevice(c->device));
+  const int n = c->n;
+  int *dn = nullptr, *dj = nullptr, *di = nullptr;
+  CK(cudaMalloc((void **)&dn, (size_t)n * sizeof(int)));
+  if (cap > 0 && jowner && jimage) {
+    CK(cudaMalloc((void **)&dj, (size_t)cap * sizeof(int)));
+    CK(cudaMalloc((void **)&di, (size_t)cap * sizeof(int)));
+  }
+  long long tot = 0;
+  cudaError_t e = md_half_list(c, dn, dj, di, dj ? cap : 0, &tot);
+  if (e == cudaSuccess && numneigh)
+    e = cudaMemcpy(numneigh, dn, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost);
+  long long m = tot < cap ? tot : cap;
+  if (e == cudaSuccess && dj && m > 0) {
+    e = cudaMemcpy(jowner, dj, (size_t)m * sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(jimage, di, (size_t)m * sizeof(int), cudaMemcpyDeviceToHost);
+  }
+  cudaFree(dn);
+  if (dj) cudaFree(dj);
+  if (di) cudaFree(di);
+  if (e != cudaSuccess) return set_err(c, B200_ERR_CUDA, "half list: %s", cudaGetErrorString(e));
+  if (total) *total = tot;
+  return B200_OK;
+}
+
+int b200_neigh_stats(b200_ctx *c, long long *full_total, int *ncalls, int *ndanger, int *maxneigh,
+                     int *capacity) {
+  if (!c) return B200_ERR_ARG;
+  if (!c->sorted_once) return set_err(c, B200_ERR_STATE, "neighbor list not built");
+  CK(cudaSetDevice(c->device));
+  unsigned long long *d = nullptr, h = 0;
+  CK(cudaMallocAsync((void **)&d, sizeof(unsigned long long), c->stream));
+  CK(cudaMemsetAsync(d, 0, sizeof(unsigned long long), c->stream));
+  k_full_total<<<md_blocks(c->n, 256), 256, 0, c->stream>>>(c->n, c->numneigh, d);
+  c->launches++;
+  CK(cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaFreeAsync(d, c->stream));
+  int rc = read_status(c);
+  if (rc) return rc;
+  if (full_total) *full_total = (long long)h;
+  if (ncalls) *ncalls = c->status_host[ST_NCALLS];
+  if (ndanger) *ndanger = c->status_host[ST_NDANGER];
+  if (maxneigh) *maxneigh = c->status_host[ST_MAXNEIGH];
+  if (capacity) *capacity = c->capacity;
+  return B200_OK;
+}
+
+int b200_get_rho_fp(b200_ctx *c, double *rho, double *fp) {
+  if (!c) return B200_ERR_ARG;
+  if (c->pstyle != B200_PAIR_EAM) return set_err(c, B200_ERR_STATE, "pair style is not eam");
+  if (!c->sorted_once) return set_err(c, B200_ERR_STATE, "neighbor list not built");
+  CK(cudaSetDevice(c->device));
+  const int n = c->n;
+  double *d = nullptr;
+  CK(cudaMallocAsync((void **)&d, (size_t)n * sizeof(double), c->stream));
+  if (rho) {
+    k_unsort_scalar<<<md_blocks(n, 256), 256, 0, c->stream>>>(n, c->orig, c->rho, d);
+    CK(cudaMemcpyAsync(rho, d, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  }
+  if (fp) {
+    k_unsort_scalar<<<md_blocks(n, 256), 256, 0, c->stream>>>(n, c->orig, c->fp, d);
+    CK(cudaMemcpyAsync(fp, d, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  }
+  c->launches += 2;
+  CK(cudaFreeAsync(d, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return B200_OK;
+}
+
+int b200_set_launch(b200_ctx *c, int tpa, int block) {
+  if (!c) return B200_ERR_ARG;
+  if (!(tpa == 0 || tpa == 1 || tpa == 2 || tpa == 4 || tpa == 8))
+    return set_err(c, B200_ERR_ARG, "threads per atom must be 0, 1, 2, 4 or 8");
+  if (block != 0 && block != 128) return set_err(c, B200_ERR_ARG, "block size must be 128");
+  c->tpa = tpa;
+  c->tuned = tpa != 0;
+  invalidate_graphs(c);
+  return B200_OK;
+}
+
+int b200_get_launch(const b200_ctx *c, int *tpa, int *block) {
+  if (!c) return B200_ERR_ARG;
+  if (tpa) *tpa = c->tpa;
+  if (block) *block = c->block;
+  return B200_OK;
+}
+
+long long b200_kernel_launches(const b200_ctx *c) { return c ? c->launches : 0; }
+
+void *b200_stream(const b200_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+}  // extern "C"

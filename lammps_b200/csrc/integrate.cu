@@ -1,0 +1,178 @@
+// integrate.cu -- velocity-Verlet (fix nve), the kinetic-energy reduction,
+// the device-side rebuild decision and thermo-row recording.
+//
+// FixNVE::initial_integrate / final_integrate (src/fix_nve.cpp:65-142) with
+// dtfm = dtf / mass[type]; every product and sum is rounded separately as in
+// the reference.  The initial half-kick also refreshes the FP32
+// cell-relative copy used by the mixed-precision pair kernels and flags any
+// atom that moved more than half the skin since the last build
+// (Neighbor::check_distance, src/neighbor.cpp:1322-1372).
+#include "md_state.h"
+
+namespace {
+
+__global__ void __launch_bounds__(256) k_nve_initial(int n, int stride, double dtv, double dtf,
+                                                      const double *__restrict__ mass,
+                                                      double4 *__restrict__ x4,
+                                                      double *__restrict__ v,
+                                                      const double *__restrict__ f,
+                                                      float4 *__restrict__ xr,
+                                                      const int *__restrict__ cell, BoxGeom box,
+                                                      const double4 *__restrict__ xhold,
+                                                      double triggersq, int *__restrict__ status) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool moved = false;
+  if (i < n) {
+    double4 p = x4[i];
+    const double dtfm = dtf / mass[(int)p.w];
+    double vx = __dadd_rn(v[i], __dmul_rn(dtfm, f[i]));
+    double vy = __dadd_rn(v[stride + i], __dmul_rn(dtfm, f[stride + i]));
+    double vz = __dadd_rn(v[2 * stride + i], __dmul_rn(dtfm, f[2 * stride + i]));
+    p.x = __dadd_rn(p.x, __dmul_rn(dtv, vx));
+    p.y = __dadd_rn(p.y, __dmul_rn(dtv, vy));
+    p.z = __dadd_rn(p.z, __dmul_rn(dtv, vz));
+    v[i] = vx;
+    v[stride + i] = vy;
+    v[2 * stride + i] = vz;
+    x4[i] = p;
+    if (xr) {
+      int cx, cy, cz;
+      md_cell_unpack(cell[i], cx, cy, cz);
+      const double ox = box.lo[0] + (cx + 0.5) * box.cs[0];
+      const double oy = box.lo[1] + (cy + 0.5) * box.cs[1];
+      const double oz = box.lo[2] + (cz + 0.5) * box.cs[2];
+      xr[i] = make_float4((float)(p.x - ox), (float)(p.y - oy), (float)(p.z - oz),
+                          __int_as_float((int)p.w));
+    }
+    if (xhold) {
+      const double4 h = xhold[i];
+      const double rsq = dsq3(__dsub_rn(p.x, h.x), __dsub_rn(p.y, h.y), __dsub_rn(p.z, h.z));
+      moved = rsq > triggersq;
+    }
+  }
+  if (xhold && __any_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0)
+    atomicExch(&status[ST_MOVED], 1);
+}
+
+template <bool KE>
+__global__ void __launch_bounds__(256) k_nve_final(int n, int stride, double dtf,
+                                                    const double *__restrict__ mass,
+                                                    const double4 *__restrict__ x4,
+                                                    double *__restrict__ v,
+                                                    const double *__restrict__ f,
+                                                    double *partial, unsigned int *counter,
+                                                    double *out) {
+  __shared__ double red[8];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double acc[1] = {0.0};
+  if (i < n) {
+    const double m = mass[(int)x4[i].w];
+    const double dtfm = dtf / m;
+    const double vx = __dadd_rn(v[i], __dmul_rn(dtfm, f[i]));
+    const double vy = __dadd_rn(v[stride + i], __dmul_rn(dtfm, f[stride + i]));
+    const double vz = __dadd_rn(v[2 * stride + i], __dmul_rn(dtfm, f[2 * stride + i]));
+    v[i] = vx;
+    v[stride + i] = vy;
+    v[2 * stride + i] = vz;
+    // ComputeTemp::compute_scalar term (src/compute_temp.cpp:84-86)
+    if (KE) acc[0] = (vx * vx + vy * vy + vz * vz) * m;
+  }
+  if (KE) block_partials_finish<1>(acc, red, partial, counter, out, false);
+}
+
+__global__ void __launch_bounds__(256) k_ke(int n, int stride, const double *__restrict__ mass,
+                                             const double4 *__restrict__ x4,
+                                             const double *__restrict__ v, double *partial,
+                                             unsigned int *counter, double *out) {
+  __shared__ double red[8];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double acc[1] = {0.0};
+  if (i < n) {
+    const double m = mass[(int)x4[i].w];
+    const double vx = v[i], vy = v[stride + i], vz = v[2 * stride + i];
+    acc[0] = (vx * vx + vy * vy + vz * vz) * m;
+  }
+  block_partials_finish<1>(acc, red, partial, counter, out, false);
+}
+
+// Neighbor::decide (src/neighbor.cpp:1294-1309) on the device
+__global__ void k_decide(int *status, int every, int delay, int check) {
+  const int ago = status[ST_AGO] + 1;
+  status[ST_AGO] = ago;
+  int rebuild = 0;
+  if (ago >= delay && ago % every == 0) {
+    if (!check) rebuild = 1;
+    else {
+      rebuild = status[ST_MOVED] != 0;
+      if (rebuild && ago == (every > delay ? every : delay)) status[ST_NDANGER] += 1;
+    }
+  }
+  status[ST_MOVED] = 0;
+  status[ST_REBUILD] = rebuild;
+  unsigned int lo = (unsigned int)status[ST_STEP_LO] + 1u;
+  if (lo == 0u) status[ST_STEP_HI] += 1;
+  status[ST_STEP_LO] = (int)lo;
+}
+
+__global__ void k_record_row(int *status, const double *ev, double *rows, int cap) {
+  const int r = status[ST_ROW];
+  if (r < cap) {
+    double *row = rows + 9 * (size_t)r;
+    const long long step = ((long long)(unsigned int)status[ST_STEP_HI] << 32) |
+                           (long long)(unsigned int)status[ST_STEP_LO];
+    row[0] = (double)step;
+    row[1] = ev[7];
+    row[2] = ev[0];
+    for (int k = 0; k < 6; k++) row[3 + k] = ev[1 + k];
+  }
+  status[ST_ROW] = r + 1;
+}
+
+}  // namespace
+
+cudaError_t md_nve_initial(b200_ctx *c, double dtv, double dtf) {
+  const int B = 256;
+  const double triggersq = 0.25 * c->skin * c->skin;  // src/neighbor.cpp:239
+  k_nve_initial<<<md_blocks(c->n, B), B, 0, c->stream>>>(
+      c->n, c->stride, dtv, dtf, c->mass_dev, c->x4, c->v, c->f,
+      c->prec == B200_PREC_MIXED ? c->xr : nullptr, c->cell, c->box,
+      c->check ? c->xhold : nullptr, triggersq, c->status);
+  c->launches++;
+  return cudaGetLastError();
+}
+
+cudaError_t md_nve_final(b200_ctx *c, double dtf, bool ke) {
+  const int B = 256;
+  if (ke)
+    k_nve_final<true><<<md_blocks(c->n, B), B, 0, c->stream>>>(
+        c->n, c->stride, dtf, c->mass_dev, c->x4, c->v, c->f, c->partial, c->counter, c->ev + 7);
+  else
+    k_nve_final<false><<<md_blocks(c->n, B), B, 0, c->stream>>>(
+        c->n, c->stride, dtf, c->mass_dev, c->x4, c->v, c->f, c->partial, c->counter, c->ev + 7);
+  c->launches++;
+  return cudaGetLastError();
+}
+
+cudaError_t md_ke(b200_ctx *c) {
+  const int B = 256;
+  k_ke<<<md_blocks(c->n, B), B, 0, c->stream>>>(c->n, c->stride, c->mass_dev, c->x4, c->v,
+                                                c->partial, c->counter, c->ev + 7);
+  c->launches++;
+  return cudaGetLastError();
+}
+
+cudaError_t md_decide(b200_ctx *c) {
+  k_decide<<<1, 1, 0, c->stream>>>(c->status, c->every, c->delay, c->check);
+  c->launches++;
+  return cudaGetLastError();
+}
+
+cudaError_t md_record_row(b200_ctx *c) {
+  k_record_row<<<1, 1, 0, c->stream>>>(c->status, c->ev, c->rows, c->rows_cap);
+  c->launches++;
+  return cudaGetLastError();
+}
+
+cudaError_t md_zero_ev(b200_ctx *c) {
+  return cudaMemsetAsync(c->ev, 0, 8 * sizeof(double), c->stream);
+}

@@ -1,0 +1,119 @@
+// md_state.h -- host-side state of one b200_ctx and the launchers shared by
+// the engine's translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "md_common.cuh"
+#include "../../include/b200md.h"
+
+struct EAMDev {
+  int nrho = 0, nr = 0, nfrho = 0, nrhor = 0, nz2r = 0;
+  double drho = 0, dr = 0, rdr = 0, rdrho = 0, rhomax = 0, cutmax = 0, cutforcesq = 0;
+  // spline tables, 8 coefficients per knot (7 used): [table][knot][8]
+  double *frho = nullptr, *rhor = nullptr, *z2r = nullptr;
+  float *frho_f = nullptr, *rhor_f = nullptr, *z2r_f = nullptr;
+  int type2frho[MD_MAXTYPES + 1];
+  int type2rhor[(MD_MAXTYPES + 1) * (MD_MAXTYPES + 1)];
+  int type2z2r[(MD_MAXTYPES + 1) * (MD_MAXTYPES + 1)];
+};
+
+// blocks of tables_dev, each TABSZ doubles
+enum { TAB_CUTNEIGHSQ = 0, TAB_CUTSQ, TAB_LJ1, TAB_LJ2, TAB_LJ3, TAB_LJ4, TAB_OFFSET, TAB_COUNT };
+constexpr int TABSZ = (MD_MAXTYPES + 1) * (MD_MAXTYPES + 1);
+
+struct b200_ctx {
+  int device = 0;
+  int prec = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  long long launches = 0;
+
+  // box and cells
+  bool box_set = false;
+  BoxGeom box{};
+  int ncells = 0;
+
+  // settings
+  double skin = 0.3;
+  int every = 1, delay = 10, check = 1, one_user = 0;
+  int ntypes = 0;
+  double mass[MD_MAXTYPES + 1] = {0};
+  bool mass_set = false;
+  int pstyle = 0;
+  LJParamsDev lj{};
+  double cutforce_max = 0.0;  // largest force cutoff
+  double cutneighsq[(MD_MAXTYPES + 1) * (MD_MAXTYPES + 1)] = {0};
+  double cutneighmax = 0.0;
+  EAMDev eam;
+  // device copy of the per-type tables, TAB_* blocks of (ntypes+1)^2 doubles
+  double *tables_dev = nullptr;
+  double *cutneighsq_dev = nullptr;  // = tables_dev + TAB_CUTNEIGHSQ*TABSZ
+
+  // atoms (device, cell-sorted order)
+  int n = 0, nalloc = 0, stride = 0;
+  double4 *x4 = nullptr, *x4b = nullptr;
+  double *v = nullptr, *vb = nullptr;  // 3 SoA planes of `stride`
+  double *f = nullptr;                 // 3 SoA planes of `stride`
+  int *orig = nullptr, *origb = nullptr;
+  int *image = nullptr, *imageb = nullptr;
+  int *cell = nullptr;        // packed cell of each sorted atom
+  float4 *xr = nullptr;       // mixed: cell-relative coordinates
+  double4 *xhold = nullptr;   // positions at the last build (check yes)
+  double *rho = nullptr, *fp = nullptr;
+  float *fpf = nullptr;
+  double *mass_dev = nullptr; // per-type masses (device)
+  bool have_atoms = false, sorted_once = false;
+
+  // binning scratch
+  int ncell_alloc = 0;
+  int *cell_count = nullptr, *cell_start = nullptr, *scan_tmp = nullptr;
+  int *slot = nullptr, *perm = nullptr, *cell_tmp = nullptr;
+
+  // neighbor list
+  int *nlist = nullptr, *numneigh = nullptr;
+  int capacity = 0;     // entries per atom
+  long long nlist_alloc = 0;
+
+  // reductions and status
+  double *partial = nullptr;     // per-block partial sums
+  int partial_blocks = 0;
+  unsigned int *counter = nullptr;
+  double *ev = nullptr;          // [0] eng, [1..6] virial, [7] sum m v^2
+  int *status = nullptr;         // ST_* words
+  int *status_host = nullptr;    // pinned mirror
+  double *rows = nullptr;        // device thermo rows (9 doubles each)
+  int rows_cap = 0;
+
+  // launch shape of the pair kernels
+  int tpa = 0, block = 128;
+  bool tuned = false;
+
+  // CUDA graph of one MD step (captured lazily by b200_run)
+  cudaGraphExec_t step_exec[2] = {nullptr, nullptr};  // [0] no output, [1] output
+  bool graph_valid = false;
+  double graph_dt = 0, graph_ftm2v = 0;
+  int graph_tpa = 0;
+};
+
+// ---- launchers (neigh.cu) -------------------------------------------------
+// full rebuild: wrap, cell counting sort, permute, neighbor list
+cudaError_t md_rebuild(b200_ctx *c, const int *d_flag);
+// LAMMPS half list derived from the full list; returns entry count via *total
+cudaError_t md_half_list(b200_ctx *c, int *d_num, int *d_jowner, int *d_jimage, long long cap,
+                         long long *total);
+// ---- pair kernels (pair_lj.cu, pair_eam.cu) --------------------------------
+cudaError_t md_lj_compute(b200_ctx *c, bool ev, bool atom_ev, double *eatom, double *vatom);
+cudaError_t md_eam_compute(b200_ctx *c, bool ev, bool atom_ev, double *eatom, double *vatom);
+// ---- integration (integrate.cu) --------------------------------------------
+cudaError_t md_nve_initial(b200_ctx *c, double dtv, double dtf);
+cudaError_t md_nve_final(b200_ctx *c, double dtf, bool ke);
+cudaError_t md_ke(b200_ctx *c);
+cudaError_t md_decide(b200_ctx *c);
+cudaError_t md_record_row(b200_ctx *c);
+cudaError_t md_zero_ev(b200_ctx *c);
+
+inline int md_blocks(long long work, int block) {
+  return (int)((work + block - 1) / block);
+}

@@ -1,0 +1,502 @@
+// neigh.cu -- device rebuild of the cell-sorted atom order and the full
+// neighbor list, plus export of the reference's half list.
+//
+// Rebuild (every `every` steps, or when an atom moved more than half the
+// skin) replaces Domain::pbc (src/domain.cpp:478-560), Atom::sort
+// (src/atom.cpp:1575-1700), CommBrick::borders (src/comm_brick.cpp:696-864)
+// and Neighbor::build -> half_bin_newton (src/neigh_half_bin.cpp:285-419):
+//   1 k_wrap_bin    wrap into the box (image flags), count atoms per cell
+//   2 k_scan_*      exclusive scan of the counts -> cell_start
+//   3 k_scatter     counting-sort scatter of atom indices
+//   4 k_sort_cells  order each cell by caller index (deterministic order)
+//   5 k_gather      permute x, v, ids; cell-relative FP32 copy; xhold
+//   6 k_copyback    permuted arrays back into the primary buffers
+//   7 k_neigh_full  full list over the 27 neighbor cells (cell >= rc+skin)
+// The pair test is the reference's, bit for bit: the periodic image is
+// formed as x_j + s*L in FP64 and rsq = dx*dx + dy*dy + dz*dz is rounded
+// after every operation, then compared with `<=` to (rc+skin)^2
+// (src/neigh_half_bin.cpp:355-360, src/atom_vec_atomic.cpp:297-299).
+#include <cstdio>
+
+#include "md_state.h"
+
+namespace {
+
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ bool rebuild_on(const int *flag) { return flag == nullptr || *flag != 0; }
+
+__global__ void k_wrap_bin(int n, BoxGeom box, double4 *__restrict__ x4, int *__restrict__ image,
+                           int *__restrict__ cell_count, int *__restrict__ slot,
+                           int *__restrict__ cell_tmp, int *__restrict__ status, const int *flag) {
+  if (!rebuild_on(flag)) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double4 p = x4[i];
+  double xs[3] = {p.x, p.y, p.z};
+  int img = image[i];
+  int im[3] = {(img & MD_IMGMASK) - MD_IMGMAX, ((img >> 10) & MD_IMGMASK) - MD_IMGMAX,
+               ((img >> 20) & MD_IMGMASK) - MD_IMGMAX};
+  int cc[3];
+  bool bad = false;
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    double x = xs[d];
+    if (!isfinite(x)) {
+      bad = true;
+      x = box.lo[d];
+    }
+    // Domain::pbc: x < lo -> x += prd; x >= hi -> x -= prd, x = max(x, lo)
+    if (x < box.lo[d]) {
+      x = __dadd_rn(x, box.prd[d]);
+      im[d]--;
+    }
+    if (x >= box.hi[d]) {
+      x = __dsub_rn(x, box.prd[d]);
+      x = fmax(x, box.lo[d]);
+      im[d]++;
+    }
+    if (x < box.lo[d] || x >= box.hi[d]) bad = true;
+    xs[d] = x;
+    int c = (int)((x - box.lo[d]) * box.cinv[d]);
+    c = c < 0 ? 0 : (c >= box.ncell[d] ? box.ncell[d] - 1 : c);
+    cc[d] = c;
+  }
+  if (bad) atomicExch(&status[ST_LOST], 1);
+  x4[i] = make_double4(xs[0], xs[1], xs[2], p.w);
+  image[i] = md_img_pack(im[0], im[1], im[2]);
+  int c = cc[0] + box.ncell[0] * (cc[1] + box.ncell[1] * cc[2]);
+  slot[i] = atomicAdd(&cell_count[c], 1);
+  cell_tmp[i] = c;
+}
+
+// block-wide exclusive scan of kScanTile ints; block sums to `sums`
+__global__ void k_scan_tiles(int m, const int *__restrict__ in, int *__restrict__ out,
+                             int *__restrict__ sums, const int *flag) {
+  if (!rebuild_on(flag)) return;
+  __shared__ int warp_tot[kScanThreads / 32];
+  int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+  int v[kScanItems];
+  int run = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; k++) {
+    int idx = base + k;
+    int a = idx < m ? in[idx] : 0;
+    v[k] = run;
+    run += a;
+  }
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int incl = run;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) warp_tot[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    int t = warp_tot[lane];
+    int s = t;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int u = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += u;
+    }
+    warp_tot[lane] = s - t;  // exclusive prefix of warp totals
+    if (lane == 31 && sums) sums[blockIdx.x] = s;
+  }
+  __syncthreads();
+  int excl = incl - run + warp_tot[warp];
+#pragma unroll
+  for (int k = 0; k < kScanItems; k++) {
+    int idx = base + k;
+    if (idx < m) out[idx] = v[k] + excl;
+  }
+}
+
+__global__ void k_scan_add(int m, int *__restrict__ out, const int *__restrict__ sums,
+                           const int *flag) {
+  if (!rebuild_on(flag)) return;
+  int b = blockIdx.x;
+  if (b == 0) return;
+  int add = sums[b];
+  int base = b * kScanTile;
+  for (int k = threadIdx.x; k < kScanTile; k += blockDim.x) {
+    int idx = base + k;
+    if (idx < m) out[idx] += add;
+  }
+}
+
+__global__ void k_scatter(int n, const int *__restrict__ cell_tmp, const int *__restrict__ slot,
+                          const int *__restrict__ cell_start, int *__restrict__ perm,
+                          const int *flag) {
+  if (!rebuild_on(flag)) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  perm[cell_start[cell_tmp[i]] + slot[i]] = i;
+}
+
+// One warp per cell: rank the cell's atoms by caller index so that the
+// sorted order (and with it every summation order) is reproducible.
+constexpr int kSortWarps = 8;
+constexpr int kSortSmall = 64;
+
+__global__ void k_sort_cells(int ncells, const int *__restrict__ cell_start, int *__restrict__ perm,
+                             int *__restrict__ tmp, const int *__restrict__ orig, const int *flag) {
+  if (!rebuild_on(flag)) return;
+  __shared__ int skey[kSortWarps][kSortSmall];
+  __shared__ int sval[kSortWarps][kSortSmall];
+  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int c = blockIdx.x * kSortWarps + w;
+  if (c >= ncells) return;
+  int s = cell_start[c], e = cell_start[c + 1], cnt = e - s;
+  if (cnt <= 1) return;
+  if (cnt <= kSortSmall) {
+    for (int k = lane; k < cnt; k += 32) {
+      int val = perm[s + k];
+      sval[w][k] = val;
+      skey[w][k] = orig[val];
+    }
+    __syncwarp();
+    for (int k = lane; k < cnt; k += 32) {
+      int key = skey[w][k], r = 0;
+      for (int m = 0; m < cnt; m++) r += skey[w][m] < key;
+      perm[s + r] = sval[w][k];
+    }
+  } else {
+    for (int k = lane; k < cnt; k += 32) tmp[s + k] = perm[s + k];
+    __threadfence_block();
+    __syncwarp();
+    for (int k = lane; k < cnt; k += 32) {
+      int val = tmp[s + k], key = orig[val], r = 0;
+      for (int m = 0; m < cnt; m++) r += orig[tmp[s + m]] < key;
+      perm[s + r] = val;
+    }
+  }
+}
+
+__global__ void k_gather(int n, int stride, BoxGeom box, const int *__restrict__ perm,
+                         const double4 *__restrict__ x4, double4 *__restrict__ x4b,
+                         const double *__restrict__ v, double *__restrict__ vb,
+                         const int *__restrict__ orig, int *__restrict__ origb,
+                         const int *__restrict__ image, int *__restrict__ imageb,
+                         const int *__restrict__ cell_tmp, int *__restrict__ cell,
+                         float4 *__restrict__ xr, double4 *__restrict__ xhold, const int *flag) {
+  if (!rebuild_on(flag)) return;
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  int old = perm[k];
+  double4 p = x4[old];
+  x4b[k] = p;
+  vb[k] = v[old];
+  vb[stride + k] = v[stride + old];
+  vb[2 * stride + k] = v[2 * stride + old];
+  origb[k] = orig[old];
+  imageb[k] = image[old];
+  int c = cell_tmp[old];
+  int cx = c % box.ncell[0];
+  int cy = (c / box.ncell[0]) % box.ncell[1];
+  int cz = c / (box.ncell[0] * box.ncell[1]);
+  cell[k] = md_cell_pack(cx, cy, cz);
+  if (xhold) xhold[k] = p;
+  if (xr) {
+    double ox = box.lo[0] + (cx + 0.5) * box.cs[0];
+    double oy = box.lo[1] + (cy + 0.5) * box.cs[1];
+    double oz = box.lo[2] + (cz + 0.5) * box.cs[2];
+    xr[k] = make_float4((float)(p.x - ox), (float)(p.y - oy), (float)(p.z - oz),
+                        __int_as_float((int)p.w));
+  }
+}
+
+__global__ void k_copyback(int n, int stride, const double4 *__restrict__ x4b,
+                           double4 *__restrict__ x4, const double *__restrict__ vb,
+                           double *__restrict__ v, const int *__restrict__ origb,
+                           int *__restrict__ orig, const int *__restrict__ imageb,
+                           int *__restrict__ image, const int *flag) {
+  if (!rebuild_on(flag)) return;
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  x4[k] = x4b[k];
+  v[k] = vb[k];
+  v[stride + k] = vb[stride + k];
+  v[2 * stride + k] = vb[2 * stride + k];
+  orig[k] = origb[k];
+  image[k] = imageb[k];
+}
+
+// Full neighbor list, one thread per atom.  Candidates come from the 27
+// cells around the atom's cell (cell edge >= rc + skin); a wrapped cell
+// carries the box shift of its periodic image.
+__global__ void __launch_bounds__(128) k_neigh_full(
+    int n, int stride, int capacity, BoxGeom box, int ntp1, const double *__restrict__ cutneighsq_g,
+    const double4 *__restrict__ x4, const int *__restrict__ cell, const int *__restrict__ cell_start,
+    int *__restrict__ nlist, int *__restrict__ numneigh, int *__restrict__ status, const int *flag) {
+  if (!rebuild_on(flag)) return;
+  __shared__ double cns[(MD_MAXTYPES + 1) * (MD_MAXTYPES + 1)];
+  for (int k = threadIdx.x; k < ntp1 * ntp1; k += blockDim.x) cns[k] = cutneighsq_g[k];
+  __syncthreads();
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double4 xi = x4[i];
+  int ti = (int)xi.w;
+  int cx, cy, cz;
+  md_cell_unpack(cell[i], cx, cy, cz);
+  const int ncx = box.ncell[0], ncy = box.ncell[1], ncz = box.ncell[2];
+  int count = 0;
+  for (int dz = -1; dz <= 1; dz++) {
+    int czj = cz + dz, sz = 0;
+    if (czj < 0) { czj += ncz; sz = -1; } else if (czj >= ncz) { czj -= ncz; sz = 1; }
+    double shz = sz * box.prd[2];
+    for (int dy = -1; dy <= 1; dy++) {
+      int cyj = cy + dy, sy = 0;
+      if (cyj < 0) { cyj += ncy; sy = -1; } else if (cyj >= ncy) { cyj -= ncy; sy = 1; }
+      double shy = sy * box.prd[1];
+      for (int dx = -1; dx <= 1; dx++) {
+        int cxj = cx + dx, sx = 0;
+        if (cxj < 0) { cxj += ncx; sx = -1; } else if (cxj >= ncx) { cxj -= ncx; sx = 1; }
+        double shx = sx * box.prd[0];
+        int code = (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1);
+        int cj = cxj + ncx * (cyj + ncy * czj);
+        int j0 = cell_start[cj], j1 = cell_start[cj + 1];
+        for (int j = j0; j < j1; j++) {
+          if (code == 13 && j == i) continue;
+          double4 xj = x4[j];
+          double delx = __dsub_rn(xi.x, __dadd_rn(xj.x, shx));
+          double dely = __dsub_rn(xi.y, __dadd_rn(xj.y, shy));
+          double delz = __dsub_rn(xi.z, __dadd_rn(xj.z, shz));
+          double rsq = dsq3(delx, dely, delz);
+          if (rsq <= cns[ti * ntp1 + (int)xj.w]) {
+            if (count < capacity) nlist[(size_t)count * stride + i] = j | (code << MD_JBITS);
+            count++;
+          }
+        }
+      }
+    }
+  }
+  // the stored count never exceeds the capacity, so readers stay in bounds;
+  // an overflow is reported through the status word
+  numneigh[i] = count < capacity ? count : capacity;
+  atomicMax(&status[ST_MAXNEIGH], count);
+  if (count > capacity) atomicExch(&status[ST_OVERFLOW], 1);
+}
+
+__global__ void k_build_done(int *status, int check, const int *flag) {
+  if (!rebuild_on(flag)) return;
+  // Neighbor::build bookkeeping: ago = 0, ncalls++ (src/neighbor.cpp:1384-1386)
+  status[ST_AGO] = 0;
+  status[ST_NCALLS] += 1;
+}
+
+// ---------------------------------------------------------------------------
+// Export of Neighbor::half_bin_newton's half list from the full list.
+struct HalfBins {
+  double lo[3], hi[3], bininv[3], binsize[3];
+  int nbin[3], mbinlo[3];
+  int sx, sy, sz;
+  double cutneighmaxsq;
+};
+
+__device__ __forceinline__ int coord2bin_dim(double x, double lo, double hi, double inv, int nbin) {
+  // Neighbor::coord2bin for one dimension (src/neighbor.cpp:1918-1947)
+  int ix;
+  if (x >= hi) ix = (int)((x - hi) * inv) + nbin;
+  else if (x >= lo) {
+    ix = (int)((x - lo) * inv);
+    ix = ix < nbin - 1 ? ix : nbin - 1;
+  } else ix = (int)((x - lo) * inv) - 1;
+  return ix;
+}
+
+__device__ __forceinline__ double bin_distance(const HalfBins &b, int i, int j, int k) {
+  double dx = i > 0 ? (i - 1) * b.binsize[0] : (i == 0 ? 0.0 : (i + 1) * b.binsize[0]);
+  double dy = j > 0 ? (j - 1) * b.binsize[1] : (j == 0 ? 0.0 : (j + 1) * b.binsize[1]);
+  double dz = k > 0 ? (k - 1) * b.binsize[2] : (k == 0 ? 0.0 : (k + 1) * b.binsize[2]);
+  return dx * dx + dy * dy + dz * dz;
+}
+
+template <bool WRITE>
+__global__ void k_half(int n, int stride, BoxGeom box, HalfBins hb, const double4 *__restrict__ x4,
+                       const int *__restrict__ cell, const int *__restrict__ orig,
+                       const int *__restrict__ nlist, const int *__restrict__ numneigh,
+                       int *__restrict__ count_out, const long long *__restrict__ offset,
+                       int *__restrict__ jowner, int *__restrict__ jimage, long long cap) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double4 xi = x4[i];
+  int bi[3] = {coord2bin_dim(xi.x, hb.lo[0], hb.hi[0], hb.bininv[0], hb.nbin[0]),
+               coord2bin_dim(xi.y, hb.lo[1], hb.hi[1], hb.bininv[1], hb.nbin[1]),
+               coord2bin_dim(xi.z, hb.lo[2], hb.hi[2], hb.bininv[2], hb.nbin[2])};
+  int cx, cy, cz;
+  md_cell_unpack(cell[i], cx, cy, cz);
+  int ci[3] = {cx, cy, cz};
+  int oi = orig[i];
+  int num = numneigh[i];
+  long long out = WRITE ? offset[oi] : 0;
+  int cnt = 0;
+  for (int k = 0; k < num; k++) {
+    unsigned int e = (unsigned int)nlist[(size_t)k * stride + i];
+    int j = (int)(e & MD_JMASK), code = (int)(e >> MD_JBITS);
+    int dc[3] = {code % 3 - 1, (code / 3) % 3 - 1, code / 9 - 1};
+    int s[3];
+    double g[3];
+    double4 xj = x4[j];
+    double xjv[3] = {xj.x, xj.y, xj.z};
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      int c = ci[d] + dc[d];
+      s[d] = c < 0 ? -1 : (c >= box.ncell[d] ? 1 : 0);
+      g[d] = __dadd_rn(xjv[d], s[d] * box.prd[d]);
+    }
+    int bj[3] = {coord2bin_dim(g[0], hb.lo[0], hb.hi[0], hb.bininv[0], hb.nbin[0]),
+                 coord2bin_dim(g[1], hb.lo[1], hb.hi[1], hb.bininv[1], hb.nbin[1]),
+                 coord2bin_dim(g[2], hb.lo[2], hb.hi[2], hb.bininv[2], hb.nbin[2])};
+    int ox = bj[0] - bi[0], oy = bj[1] - bi[1], oz = bj[2] - bi[2];
+    bool ghost = (s[0] | s[1] | s[2]) != 0;
+    bool own;
+    if (ox == 0 && oy == 0 && oz == 0) {
+      if (!ghost) own = orig[j] > oi;  // j beyond i in the bin's linked list
+      else {                            // ghost "above and to the right"
+        own = !(g[2] < xi.z) &&
+              !(g[2] == xi.z && (g[1] < xi.y || (g[1] == xi.y && g[0] < xi.x)));
+      }
+    } else {
+      own = (oz > 0 || oy > 0 || (oy == 0 && ox > 0)) && oz >= 0 && oz <= hb.sz &&
+            ox >= -hb.sx && ox <= hb.sx && oy >= -hb.sy && oy <= hb.sy &&
+            bin_distance(hb, ox, oy, oz) < hb.cutneighmaxsq;
+    }
+    if (own) {
+      if (WRITE && out + cnt < cap) {
+        jowner[out + cnt] = orig[j];
+        jimage[out + cnt] = (s[0] + 1) + 3 * (s[1] + 1) + 9 * (s[2] + 1);
+      }
+      cnt++;
+    }
+  }
+  if (!WRITE) count_out[oi] = cnt;
+}
+
+__global__ void k_prefix_ll(int n, const int *__restrict__ cnt, long long *__restrict__ off,
+                            long long *__restrict__ total) {
+  // single-thread prefix over atoms (export path only, not per step)
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  long long s = 0;
+  for (int i = 0; i < n; i++) {
+    off[i] = s;
+    s += cnt[i];
+  }
+  *total = s;
+}
+
+}  // namespace
+
+static cudaError_t launch_scan(b200_ctx *c, int m, const int *in, int *out, const int *flag) {
+  int tiles = (m + kScanTile - 1) / kScanTile;
+  if (tiles > kScanTile) return cudaErrorInvalidValue;
+  int *sums = c->scan_tmp;
+  k_scan_tiles<<<tiles, kScanThreads, 0, c->stream>>>(m, in, out, sums, flag);
+  c->launches++;
+  if (tiles > 1) {
+    k_scan_tiles<<<1, kScanThreads, 0, c->stream>>>(tiles, sums, sums, nullptr, flag);
+    k_scan_add<<<tiles, 256, 0, c->stream>>>(m, out, sums, flag);
+    c->launches += 2;
+  }
+  return cudaGetLastError();
+}
+
+__global__ void k_zero_counts(int m, int *cnt, const int *flag) {
+  if (flag && !*flag) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m) cnt[i] = 0;
+}
+
+cudaError_t md_rebuild(b200_ctx *c, const int *d_flag) {
+  const int n = c->n, B = 256;
+  const int m = c->ncells + 1;
+  k_zero_counts<<<md_blocks(m, B), B, 0, c->stream>>>(m, c->cell_count, d_flag);
+  k_wrap_bin<<<md_blocks(n, B), B, 0, c->stream>>>(n, c->box, c->x4, c->image, c->cell_count,
+                                                   c->slot, c->cell_tmp, c->status, d_flag);
+  c->launches += 2;
+  cudaError_t e = launch_scan(c, m, c->cell_count, c->cell_start, d_flag);
+  if (e != cudaSuccess) return e;
+  k_scatter<<<md_blocks(n, B), B, 0, c->stream>>>(n, c->cell_tmp, c->slot, c->cell_start, c->perm,
+                                                  d_flag);
+  k_sort_cells<<<md_blocks(c->ncells, kSortWarps), kSortWarps * 32, 0, c->stream>>>(
+      c->ncells, c->cell_start, c->perm, c->slot, c->orig, d_flag);
+  k_gather<<<md_blocks(n, B), B, 0, c->stream>>>(
+      n, c->stride, c->box, c->perm, c->x4, c->x4b, c->v, c->vb, c->orig, c->origb, c->image,
+      c->imageb, c->cell_tmp, c->cell, c->prec == 1 ? c->xr : nullptr,
+      c->check ? c->xhold : nullptr, d_flag);
+  k_copyback<<<md_blocks(n, B), B, 0, c->stream>>>(n, c->stride, c->x4b, c->x4, c->vb, c->v,
+                                                   c->origb, c->orig, c->imageb, c->image, d_flag);
+  k_neigh_full<<<md_blocks(n, 128), 128, 0, c->stream>>>(
+      n, c->stride, c->capacity, c->box, c->ntypes + 1, c->cutneighsq_dev, c->x4, c->cell, c->cell_start, c->nlist, c->numneigh, c->status, d_flag);
+  k_build_done<<<1, 1, 0, c->stream>>>(c->status, c->check, d_flag);
+  c->launches += 5;
+  return cudaGetLastError();
+}
+
+// LAMMPS bins of Neighbor::setup_bins (src/neighbor.cpp:1538-1702) for a
+// single periodic process: binsize = cutneighmax/2, bounding box extended by
+// the ghost cutoff, half stencil extents sx, sy, sz.
+static HalfBins half_bins(const b200_ctx *c) {
+  HalfBins hb{};
+  const double SMALL = 1.0e-6;
+  double cutghost = c->cutneighmax;
+  double binsize_optimal = 0.5 * c->cutneighmax;
+  double bbox[3];
+  for (int d = 0; d < 3; d++) bbox[d] = c->box.hi[d] - c->box.lo[d];
+  if (binsize_optimal == 0.0) binsize_optimal = bbox[0];
+  double binsizeinv = 1.0 / binsize_optimal;
+  for (int d = 0; d < 3; d++) {
+    hb.lo[d] = c->box.lo[d];
+    hb.hi[d] = c->box.hi[d];
+    int nb = (int)(bbox[d] * binsizeinv);
+    if (nb == 0) nb = 1;
+    hb.nbin[d] = nb;
+    hb.binsize[d] = bbox[d] / nb;
+    hb.bininv[d] = 1.0 / hb.binsize[d];
+    double coord = (c->box.lo[d] - cutghost) - SMALL * bbox[d];
+    int lo = (int)((coord - c->box.lo[d]) * hb.bininv[d]);
+    if (coord < c->box.lo[d]) lo = lo - 1;
+    hb.mbinlo[d] = lo - 1;
+  }
+  int s[3];
+  for (int d = 0; d < 3; d++) {
+    s[d] = (int)(c->cutneighmax * hb.bininv[d]);
+    if (s[d] * hb.binsize[d] < c->cutneighmax) s[d]++;
+  }
+  hb.sx = s[0];
+  hb.sy = s[1];
+  hb.sz = s[2];
+  hb.cutneighmaxsq = c->cutneighmax * c->cutneighmax;
+  return hb;
+}
+
+cudaError_t md_half_list(b200_ctx *c, int *d_num, int *d_jowner, int *d_jimage, long long cap,
+                         long long *total) {
+  const int n = c->n, B = 128;
+  HalfBins hb = half_bins(c);
+  long long *d_off = nullptr, *d_total = nullptr;
+  cudaError_t e = cudaMallocAsync((void **)&d_off, sizeof(long long) * (size_t)(n + 1), c->stream);
+  if (e != cudaSuccess) return e;
+  e = cudaMallocAsync((void **)&d_total, sizeof(long long), c->stream);
+  if (e != cudaSuccess) return e;
+  k_half<false><<<md_blocks(n, B), B, 0, c->stream>>>(n, c->stride, c->box, hb, c->x4, c->cell,
+                                                      c->orig, c->nlist, c->numneigh, d_num,
+                                                      nullptr, nullptr, nullptr, 0);
+  k_prefix_ll<<<1, 1, 0, c->stream>>>(n, d_num, d_off, d_total);
+  if (d_jowner && cap > 0)
+    k_half<true><<<md_blocks(n, B), B, 0, c->stream>>>(n, c->stride, c->box, hb, c->x4, c->cell,
+                                                       c->orig, c->nlist, c->numneigh, nullptr,
+                                                       d_off, d_jowner, d_jimage, cap);
+  c->launches += d_jowner && cap > 0 ? 3 : 2;
+  e = cudaMemcpyAsync(total, d_total, sizeof(long long), cudaMemcpyDeviceToHost, c->stream);
+  if (e != cudaSuccess) return e;
+  cudaFreeAsync(d_off, c->stream);
+  cudaFreeAsync(d_total, c->stream);
+  e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return e;
+  return cudaGetLastError();
+}

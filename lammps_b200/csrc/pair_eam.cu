@@ -1,0 +1,378 @@
+// pair_eam.cu -- pair_style eam / eam/alloy / eam/fs over the full list.
+//
+// Replaces PairEAM::compute (src/MANYBODY/pair_eam.cpp:125-306), whose three
+// passes become two kernels:
+//   k_eam_rho    density rho_i over the full list (no ghost densities, so the
+//                reverse_comm_pair of rho disappears) and, in the same
+//                kernel, the embedding derivative fp_i = F'(rho_i) and energy
+//                F(rho_i) (+ linear term above rhomax)            (:160-228)
+//   k_eam_force  pair force psi'/r using fp_i and the neighbor's own fp_j
+//                (the forward_comm_pair of fp disappears)         (:237-303)
+// Splines are the reference's 7-coefficient cubic tables
+// (PairEAM::interpolate, :723-751), stored 8 doubles per knot; the index
+// clamps are the reference's: m = min(m, nr-1), p = min(p, 1) for r and
+// m = max(1, min(m, nrho-1)) for rho.
+// Mixed form: FP32 tables reordered per knot as [c3 c4 c5 c6 | c0 c1 c2 -]
+// so one float4 load gives a value and one a derivative; distances from the
+// FP32 cell-relative coordinates; fp_j gathered as FP32; sums in FP64.  The
+// embedding step F(rho) stays FP64 in both forms.
+#include "md_state.h"
+
+namespace {
+
+struct EamArgs {
+  int n, stride, ntp1;
+  BoxGeom box;
+  const int *cell, *nlist, *numneigh, *orig;
+  int nrho, nr;
+  double rdr, rdrho, rhomax, cutforcesq;
+  const double *frho, *rhor, *z2r;
+  const float *rhor_f, *z2r_f;
+  const int *t2frho, *t2rhor, *t2z2r;  // device copies of the type maps
+  double *rho, *fp;
+  float *fpf;
+  double *f;
+  double *partial;
+  unsigned int *counter;
+  double *ev;
+  double *eatom, *vatom;
+};
+
+struct Shift3 {
+  double m, p;
+};
+__device__ __forceinline__ Shift3 shifts(int c, int nc, double prd) {
+  Shift3 s;
+  s.m = (c - 1 < 0) ? -prd : 0.0;
+  s.p = (c + 1 >= nc) ? prd : 0.0;
+  return s;
+}
+__device__ __forceinline__ double pick(const Shift3 &s, int d) {
+  return d < 0 ? s.m : (d > 0 ? s.p : 0.0);
+}
+__device__ __forceinline__ void decode(unsigned int e, int &j, int &dx, int &dy, int &dz) {
+  j = (int)(e & MD_JMASK);
+  const int code = (int)(e >> MD_JBITS);
+  dz = code / 9 - 1;
+  const int rem = code - 9 * (dz + 1);
+  dy = rem / 3 - 1;
+  dx = rem - 3 * (dy + 1) - 1;
+}
+
+// Embedding F(rho) and F'(rho) of one atom, FP64, reference clamps.
+__device__ __forceinline__ void embed(const EamArgs &a, int itype_frho, double rho, double &fp,
+                                      double &phi) {
+  double p = __dadd_rn(__dmul_rn(rho, a.rdrho), 1.0);
+  int m = (int)p;
+  m = max(1, min(m, a.nrho - 1));
+  p -= m;
+  p = fmin(p, 1.0);
+  const double *c = a.frho + ((size_t)itype_frho * (a.nrho + 1) + m) * 8;
+  fp = (c[0] * p + c[1]) * p + c[2];
+  phi = ((c[3] * p + c[4]) * p + c[5]) * p + c[6];
+  if (rho > a.rhomax) phi += fp * (rho - a.rhomax);
+}
+
+template <int TPA, bool EV, bool ATOM, bool MIXED>
+__global__ void __launch_bounds__(128) k_eam_rho(EamArgs a, const double4 *__restrict__ x4,
+                                                 const float4 *__restrict__ xr) {
+  __shared__ int s_t2rhor[TABSZ];
+  __shared__ int s_t2frho[MD_MAXTYPES + 1];
+  __shared__ double red[7 * 4];
+  const int nt2 = a.ntp1 * a.ntp1;
+  for (int k = threadIdx.x; k < nt2; k += blockDim.x) s_t2rhor[k] = a.t2rhor[k];
+  for (int k = threadIdx.x; k < a.ntp1; k += blockDim.x) s_t2frho[k] = a.t2frho[k];
+  __syncthreads();
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = t / TPA, lane = t % TPA;
+  const bool active = i < a.n;
+  double rho = 0.0;
+  int ti = 1;
+  if (active) {
+    const int num = a.numneigh[i];
+    if (!MIXED) {
+      const double4 xi = x4[i];
+      ti = (int)xi.w;
+      int cx, cy, cz;
+      md_cell_unpack(a.cell[i], cx, cy, cz);
+      const Shift3 sx = shifts(cx, a.box.ncell[0], a.box.prd[0]);
+      const Shift3 sy = shifts(cy, a.box.ncell[1], a.box.prd[1]);
+      const Shift3 sz = shifts(cz, a.box.ncell[2], a.box.prd[2]);
+      for (int k = lane; k < num; k += TPA) {
+        int j, dx, dy, dz;
+        decode((unsigned int)a.nlist[(size_t)k * a.stride + i], j, dx, dy, dz);
+        const double4 xj = x4[j];
+        const double delx = __dsub_rn(xi.x, __dadd_rn(xj.x, pick(sx, dx)));
+        const double dely = __dsub_rn(xi.y, __dadd_rn(xj.y, pick(sy, dy)));
+        const double delz = __dsub_rn(xi.z, __dadd_rn(xj.z, pick(sz, dz)));
+        const double rsq = dsq3(delx, dely, delz);
+        if (rsq < a.cutforcesq) {
+          double p = __dadd_rn(__dmul_rn(sqrt(rsq), a.rdr), 1.0);
+          int m = (int)p;
+          m = min(m, a.nr - 1);
+          p -= m;
+          p = fmin(p, 1.0);
+          const int tab = s_t2rhor[(int)xj.w * a.ntp1 + ti];
+          const double *c = a.rhor + ((size_t)tab * (a.nr + 1) + m) * 8;
+          rho += ((c[3] * p + c[4]) * p + c[5]) * p + c[6];
+        }
+      }
+    } else {
+      const float4 xi = xr[i];
+      ti = __float_as_int(xi.w);
+      const float csx = (float)a.box.cs[0], csy = (float)a.box.cs[1], csz = (float)a.box.cs[2];
+      const float cutf = (float)a.cutforcesq, rdrf = (float)a.rdr;
+      for (int k = lane; k < num; k += TPA) {
+        int j, dx, dy, dz;
+        decode((unsigned int)a.nlist[(size_t)k * a.stride + i], j, dx, dy, dz);
+        const float4 xj = xr[j];
+        const float delx = (xi.x - xj.x) - (float)dx * csx;
+        const float dely = (xi.y - xj.y) - (float)dy * csy;
+        const float delz = (xi.z - xj.z) - (float)dz * csz;
+        const float rsq = delx * delx + dely * dely + delz * delz;
+        if (rsq < cutf) {
+          float p = sqrtf(rsq) * rdrf + 1.0f;
+          int m = (int)p;
+          m = min(m, a.nr - 1);
+          p -= (float)m;
+          p = fminf(p, 1.0f);
+          const int tab = s_t2rhor[__float_as_int(xj.w) * a.ntp1 + ti];
+          const float4 c = *reinterpret_cast<const float4 *>(a.rhor_f + ((size_t)tab * (a.nr + 1) + m) * 8);
+          rho += (double)(((c.x * p + c.y) * p + c.z) * p + c.w);
+        }
+      }
+    }
+  }
+  rho = lane_sum<TPA>(rho);
+  double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+  if (active && lane == 0) {
+    double fpi, phi;
+    embed(a, s_t2frho[ti], rho, fpi, phi);
+    a.rho[i] = rho;
+    a.fp[i] = fpi;
+    if (MIXED) a.fpf[i] = (float)fpi;
+    if (EV) {
+      acc[0] = phi;
+      if (ATOM && a.eatom) a.eatom[a.orig[i]] = phi;
+    }
+  }
+  if (EV) block_partials_finish<7>(acc, red, a.partial, a.counter, a.ev, false);
+}
+
+template <int TPA, bool EV, bool ATOM, bool MIXED>
+__global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__restrict__ x4,
+                                                   const float4 *__restrict__ xr) {
+  __shared__ int s_t2rhor[TABSZ];
+  __shared__ int s_t2z2r[TABSZ];
+  __shared__ double red[7 * 4];
+  const int nt2 = a.ntp1 * a.ntp1;
+  for (int k = threadIdx.x; k < nt2; k += blockDim.x) {
+    s_t2rhor[k] = a.t2rhor[k];
+    s_t2z2r[k] = a.t2z2r[k];
+  }
+  __syncthreads();
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = t / TPA, lane = t % TPA;
+  const bool active = i < a.n;
+  double fx = 0.0, fy = 0.0, fz = 0.0;
+  double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+  if (active) {
+    const int num = a.numneigh[i];
+    if (!MIXED) {
+      const double4 xi = x4[i];
+      const int ti = (int)xi.w;
+      const double fpi = a.fp[i];
+      int cx, cy, cz;
+      md_cell_unpack(a.cell[i], cx, cy, cz);
+      const Shift3 sx = shifts(cx, a.box.ncell[0], a.box.prd[0]);
+      const Shift3 sy = shifts(cy, a.box.ncell[1], a.box.prd[1]);
+      const Shift3 sz = shifts(cz, a.box.ncell[2], a.box.prd[2]);
+      for (int k = lane; k < num; k += TPA) {
+        int j, dx, dy, dz;
+        decode((unsigned int)a.nlist[(size_t)k * a.stride + i], j, dx, dy, dz);
+        const double4 xj = x4[j];
+        const double delx = __dsub_rn(xi.x, __dadd_rn(xj.x, pick(sx, dx)));
+        const double dely = __dsub_rn(xi.y, __dadd_rn(xj.y, pick(sy, dy)));
+        const double delz = __dsub_rn(xi.z, __dadd_rn(xj.z, pick(sz, dz)));
+        const double rsq = dsq3(delx, dely, delz);
+        if (rsq < a.cutforcesq) {
+          const int tj = (int)xj.w;
+          const double r = sqrt(rsq);
+          double p = __dadd_rn(__dmul_rn(r, a.rdr), 1.0);
+          int m = (int)p;
+          m = min(m, a.nr - 1);
+          p -= m;
+          p = fmin(p, 1.0);
+          const double *ci = a.rhor + ((size_t)s_t2rhor[ti * a.ntp1 + tj] * (a.nr + 1) + m) * 8;
+          const double rhoip = (ci[0] * p + ci[1]) * p + ci[2];
+          const double *cj = a.rhor + ((size_t)s_t2rhor[tj * a.ntp1 + ti] * (a.nr + 1) + m) * 8;
+          const double rhojp = (cj[0] * p + cj[1]) * p + cj[2];
+          const double *cz2 = a.z2r + ((size_t)s_t2z2r[ti * a.ntp1 + tj] * (a.nr + 1) + m) * 8;
+          const double z2p = (cz2[0] * p + cz2[1]) * p + cz2[2];
+          const double z2 = ((cz2[3] * p + cz2[4]) * p + cz2[5]) * p + cz2[6];
+          const double recip = 1.0 / r;
+          const double phi = z2 * recip;
+          const double phip = z2p * recip - phi * recip;
+          const double psip = fpi * rhojp + a.fp[j] * rhoip + phip;
+          const double fpair = -psip * recip;
+          fx += delx * fpair;
+          fy += dely * fpair;
+          fz += delz * fpair;
+          if (EV) {
+            acc[0] += 0.5 * phi;
+            const double hf = 0.5 * fpair;
+            acc[1] += delx * delx * hf;
+            acc[2] += dely * dely * hf;
+            acc[3] += delz * delz * hf;
+            acc[4] += delx * dely * hf;
+            acc[5] += delx * delz * hf;
+            acc[6] += dely * delz * hf;
+          }
+        }
+      }
+    } else {
+      const float4 xi = xr[i];
+      const int ti = __float_as_int(xi.w);
+      const float fpi = a.fpf[i];
+      const float csx = (float)a.box.cs[0], csy = (float)a.box.cs[1], csz = (float)a.box.cs[2];
+      const float cutf = (float)a.cutforcesq, rdrf = (float)a.rdr;
+      for (int k = lane; k < num; k += TPA) {
+        int j, dx, dy, dz;
+        decode((unsigned int)a.nlist[(size_t)k * a.stride + i], j, dx, dy, dz);
+        const float4 xj = xr[j];
+        const float delx = (xi.x - xj.x) - (float)dx * csx;
+        const float dely = (xi.y - xj.y) - (float)dy * csy;
+        const float delz = (xi.z - xj.z) - (float)dz * csz;
+        const float rsq = delx * delx + dely * dely + delz * delz;
+        if (rsq < cutf) {
+          const int tj = __float_as_int(xj.w);
+          const float recip = rsqrtf(rsq);
+          const float r = rsq * recip;
+          float p = r * rdrf + 1.0f;
+          int m = (int)p;
+          m = min(m, a.nr - 1);
+          p -= (float)m;
+          p = fminf(p, 1.0f);
+          const float4 ci = *reinterpret_cast<const float4 *>(
+              a.rhor_f + ((size_t)s_t2rhor[ti * a.ntp1 + tj] * (a.nr + 1) + m) * 8 + 4);
+          const float rhoip = (ci.x * p + ci.y) * p + ci.z;
+          const float4 cj = *reinterpret_cast<const float4 *>(
+              a.rhor_f + ((size_t)s_t2rhor[tj * a.ntp1 + ti] * (a.nr + 1) + m) * 8 + 4);
+          const float rhojp = (cj.x * p + cj.y) * p + cj.z;
+          const float *zb = a.z2r_f + ((size_t)s_t2z2r[ti * a.ntp1 + tj] * (a.nr + 1) + m) * 8;
+          const float4 zv = *reinterpret_cast<const float4 *>(zb);
+          const float4 zd = *reinterpret_cast<const float4 *>(zb + 4);
+          const float z2p = (zd.x * p + zd.y) * p + zd.z;
+          const float z2 = ((zv.x * p + zv.y) * p + zv.z) * p + zv.w;
+          const float phi = z2 * recip;
+          const float phip = z2p * recip - phi * recip;
+          const float psip = fpi * rhojp + a.fpf[j] * rhoip + phip;
+          const float fpair = -psip * recip;
+          fx += (double)(delx * fpair);
+          fy += (double)(dely * fpair);
+          fz += (double)(delz * fpair);
+          if (EV) {
+            acc[0] += 0.5 * (double)phi;
+            const float hf = 0.5f * fpair;
+            acc[1] += (double)(delx * delx * hf);
+            acc[2] += (double)(dely * dely * hf);
+            acc[3] += (double)(delz * delz * hf);
+            acc[4] += (double)(delx * dely * hf);
+            acc[5] += (double)(delx * delz * hf);
+            acc[6] += (double)(dely * delz * hf);
+          }
+        }
+      }
+    }
+  }
+  fx = lane_sum<TPA>(fx);
+  fy = lane_sum<TPA>(fy);
+  fz = lane_sum<TPA>(fz);
+  if (active && lane == 0) {
+    a.f[i] = fx;
+    a.f[a.stride + i] = fy;
+    a.f[2 * a.stride + i] = fz;
+  }
+  if (EV) {
+    if (ATOM) {
+      double e[7];
+#pragma unroll
+      for (int k = 0; k < 7; k++) e[k] = lane_sum<TPA>(acc[k]);
+      if (active && lane == 0) {
+        const int o = a.orig[i];
+        if (a.eatom) a.eatom[o] += e[0];
+        if (a.vatom)
+#pragma unroll
+          for (int k = 0; k < 6; k++) a.vatom[6 * (size_t)o + k] = e[1 + k];
+      }
+    }
+    block_partials_finish<7>(acc, red, a.partial, a.counter, a.ev, true);
+  }
+}
+
+template <int TPA, bool EV, bool ATOM>
+void launch_t(b200_ctx *c, const EamArgs &a) {
+  const int B = 128;
+  const int grid = md_blocks((long long)a.n * TPA, B);
+  if (c->prec == B200_PREC_MIXED) {
+    k_eam_rho<TPA, EV, ATOM, true><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
+    k_eam_force<TPA, EV, ATOM, true><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
+  } else {
+    k_eam_rho<TPA, EV, ATOM, false><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
+    k_eam_force<TPA, EV, ATOM, false><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
+  }
+  c->launches += 2;
+}
+
+template <int TPA>
+void launch_tpa(b200_ctx *c, const EamArgs &a, bool ev, bool atom) {
+  if (!ev) launch_t<TPA, false, false>(c, a);
+  else if (!atom) launch_t<TPA, true, false>(c, a);
+  else launch_t<TPA, true, true>(c, a);
+}
+
+}  // namespace
+
+cudaError_t md_eam_compute(b200_ctx *c, bool ev, bool atom_ev, double *eatom, double *vatom) {
+  EamArgs a;
+  a.n = c->n;
+  a.stride = c->stride;
+  a.ntp1 = c->ntypes + 1;
+  a.box = c->box;
+  a.cell = c->cell;
+  a.nlist = c->nlist;
+  a.numneigh = c->numneigh;
+  a.orig = c->orig;
+  a.nrho = c->eam.nrho;
+  a.nr = c->eam.nr;
+  a.rdr = c->eam.rdr;
+  a.rdrho = c->eam.rdrho;
+  a.rhomax = c->eam.rhomax;
+  a.cutforcesq = c->eam.cutforcesq;
+  a.frho = c->eam.frho;
+  a.rhor = c->eam.rhor;
+  a.z2r = c->eam.z2r;
+  a.rhor_f = c->eam.rhor_f;
+  a.z2r_f = c->eam.z2r_f;
+  // type maps live right after the TAB_* tables in tables_dev (as ints)
+  const int *maps = reinterpret_cast<const int *>(c->tables_dev + TAB_COUNT * TABSZ);
+  a.t2frho = maps;
+  a.t2rhor = maps + (MD_MAXTYPES + 1);
+  a.t2z2r = maps + (MD_MAXTYPES + 1) + TABSZ;
+  a.rho = c->rho;
+  a.fp = c->fp;
+  a.fpf = c->fpf;
+  a.f = c->f;
+  a.partial = c->partial;
+  a.counter = c->counter;
+  a.ev = c->ev;
+  a.eatom = eatom;
+  a.vatom = vatom;
+  switch (c->tpa) {
+    case 1: launch_tpa<1>(c, a, ev, atom_ev); break;
+    case 2: launch_tpa<2>(c, a, ev, atom_ev); break;
+    case 4: launch_tpa<4>(c, a, ev, atom_ev); break;
+    default: launch_tpa<8>(c, a, ev, atom_ev); break;
+  }
+  return cudaGetLastError();
+}

@@ -1,0 +1,294 @@
+// pair_lj.cu -- pair_style lj/cut force kernels over the full neighbor list.
+//
+// Replaces PairLJCut::compute (src/pair_lj_cut.cpp:68-141).  With a full
+// list each atom sums its own force, so no atomics, no ghost forces and no
+// reverse communication are needed; energy and virial are accumulated as
+// half of every pair term (the reference's ev_tally with newton on gives the
+// same totals, src/pair.cpp:769-855) and reduced deterministically.
+//
+// FP64 form: arithmetic identical to the reference per pair; the periodic
+// image is x_j + s*L and rsq is rounded after every operation, so the
+// rsq < cutsq decision is the reference's.
+// Mixed form: positions are read as FP32 offsets from the centre of the
+// atom's cell (float4, 16 B per gather); the pair force is FP32 and each
+// atom's force, energy and virial are summed in FP64.
+#include "md_state.h"
+
+namespace {
+
+struct PairArgs {
+  int n, stride, ntp1;
+  BoxGeom box;
+  const double *tables;
+  const int *cell, *nlist, *numneigh, *orig;
+  double *f;
+  double *partial;
+  unsigned int *counter;
+  double *ev;
+  double *eatom, *vatom;
+};
+
+// per-atom periodic shifts for cell offsets -1, 0, +1 along one dimension
+struct Shift3 {
+  double m, p;
+};
+__device__ __forceinline__ Shift3 shifts(int c, int nc, double prd) {
+  Shift3 s;
+  s.m = (c - 1 < 0) ? -prd : 0.0;
+  s.p = (c + 1 >= nc) ? prd : 0.0;
+  return s;
+}
+__device__ __forceinline__ double pick(const Shift3 &s, int d) {
+  return d < 0 ? s.m : (d > 0 ? s.p : 0.0);
+}
+
+template <int TPA, bool EV, bool ATOM, bool SINGLE>
+__global__ void __launch_bounds__(128) k_lj_fp64(PairArgs a, const double4 *__restrict__ x4) {
+  __shared__ double tab[6 * TABSZ];
+  __shared__ double red[7 * 4];
+  const int nt2 = a.ntp1 * a.ntp1;
+  if (!SINGLE) {
+    for (int k = threadIdx.x; k < 6 * nt2; k += blockDim.x)
+      tab[k] = a.tables[(TAB_CUTSQ + k / nt2) * TABSZ + k % nt2];
+    __syncthreads();
+  }
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = t / TPA, lane = t % TPA;
+  const bool active = i < a.n;
+  double fx = 0.0, fy = 0.0, fz = 0.0;
+  double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+  if (active) {
+    double cutsq1 = 0, lj1 = 0, lj2 = 0, lj3 = 0, lj4 = 0, off = 0;
+    if (SINGLE) {
+      const int k11 = a.ntp1 + 1;
+      cutsq1 = __ldg(&a.tables[TAB_CUTSQ * TABSZ + k11]);
+      lj1 = __ldg(&a.tables[TAB_LJ1 * TABSZ + k11]);
+      lj2 = __ldg(&a.tables[TAB_LJ2 * TABSZ + k11]);
+      lj3 = __ldg(&a.tables[TAB_LJ3 * TABSZ + k11]);
+      lj4 = __ldg(&a.tables[TAB_LJ4 * TABSZ + k11]);
+      off = __ldg(&a.tables[TAB_OFFSET * TABSZ + k11]);
+    }
+    const double4 xi = x4[i];
+    const int ti = (int)xi.w;
+    int cx, cy, cz;
+    md_cell_unpack(a.cell[i], cx, cy, cz);
+    const Shift3 sx = shifts(cx, a.box.ncell[0], a.box.prd[0]);
+    const Shift3 sy = shifts(cy, a.box.ncell[1], a.box.prd[1]);
+    const Shift3 sz = shifts(cz, a.box.ncell[2], a.box.prd[2]);
+    const int num = a.numneigh[i];
+    for (int k = lane; k < num; k += TPA) {
+      const unsigned int e = (unsigned int)__ldcs(&a.nlist[(size_t)k * a.stride + i]);
+      const int j = (int)(e & MD_JMASK);
+      const int code = (int)(e >> MD_JBITS);
+      const int dz = code / 9 - 1, rem = code - 9 * (dz + 1);
+      const int dy = rem / 3 - 1, dx = rem - 3 * (dy + 1) - 1;
+      const double4 xj = x4[j];
+      const double delx = __dsub_rn(xi.x, __dadd_rn(xj.x, pick(sx, dx)));
+      const double dely = __dsub_rn(xi.y, __dadd_rn(xj.y, pick(sy, dy)));
+      const double delz = __dsub_rn(xi.z, __dadd_rn(xj.z, pick(sz, dz)));
+      const double rsq = dsq3(delx, dely, delz);
+      const int tj = (int)xj.w;
+      const int tt = ti * a.ntp1 + tj;
+      const double cs = SINGLE ? cutsq1 : tab[0 * nt2 + tt];
+      if (rsq < cs) {
+        const double c1 = SINGLE ? lj1 : tab[1 * nt2 + tt];
+        const double c2 = SINGLE ? lj2 : tab[2 * nt2 + tt];
+        const double r2inv = 1.0 / rsq;
+        const double r6inv = r2inv * r2inv * r2inv;
+        const double forcelj = r6inv * (c1 * r6inv - c2);
+        const double fpair = forcelj * r2inv;
+        fx += delx * fpair;
+        fy += dely * fpair;
+        fz += delz * fpair;
+        if (EV) {
+          const double c3 = SINGLE ? lj3 : tab[3 * nt2 + tt];
+          const double c4 = SINGLE ? lj4 : tab[4 * nt2 + tt];
+          const double co = SINGLE ? off : tab[5 * nt2 + tt];
+          const double evdwl = r6inv * (c3 * r6inv - c4) - co;
+          acc[0] += 0.5 * evdwl;
+          const double hf = 0.5 * fpair;
+          acc[1] += delx * delx * hf;
+          acc[2] += dely * dely * hf;
+          acc[3] += delz * delz * hf;
+          acc[4] += delx * dely * hf;
+          acc[5] += delx * delz * hf;
+          acc[6] += dely * delz * hf;
+        }
+      }
+    }
+  }
+  fx = lane_sum<TPA>(fx);
+  fy = lane_sum<TPA>(fy);
+  fz = lane_sum<TPA>(fz);
+  if (active && lane == 0) {
+    a.f[i] = fx;
+    a.f[a.stride + i] = fy;
+    a.f[2 * a.stride + i] = fz;
+  }
+  if (EV) {
+    if (ATOM) {
+      double e[7];
+#pragma unroll
+      for (int k = 0; k < 7; k++) e[k] = lane_sum<TPA>(acc[k]);
+      if (active && lane == 0) {
+        const int o = a.orig[i];
+        if (a.eatom) a.eatom[o] = e[0];
+        if (a.vatom)
+#pragma unroll
+          for (int k = 0; k < 6; k++) a.vatom[6 * (size_t)o + k] = e[1 + k];
+      }
+    }
+    block_partials_finish<7>(acc, red, a.partial, a.counter, a.ev, false);
+  }
+}
+
+template <int TPA, bool EV, bool ATOM, bool SINGLE>
+__global__ void __launch_bounds__(128) k_lj_mixed(PairArgs a, const float4 *__restrict__ xr) {
+  __shared__ float tabf[6 * TABSZ];
+  __shared__ double red[7 * 4];
+  const int nt2 = a.ntp1 * a.ntp1;
+  if (!SINGLE) {
+    for (int k = threadIdx.x; k < 6 * nt2; k += blockDim.x)
+      tabf[k] = (float)a.tables[(TAB_CUTSQ + k / nt2) * TABSZ + k % nt2];
+    __syncthreads();
+  }
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = t / TPA, lane = t % TPA;
+  const bool active = i < a.n;
+  double fx = 0.0, fy = 0.0, fz = 0.0;
+  double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+  if (active) {
+    float cutsq1 = 0, lj1 = 0, lj2 = 0, lj3 = 0, lj4 = 0, off = 0;
+    if (SINGLE) {
+      const int k11 = a.ntp1 + 1;
+      cutsq1 = (float)__ldg(&a.tables[TAB_CUTSQ * TABSZ + k11]);
+      lj1 = (float)__ldg(&a.tables[TAB_LJ1 * TABSZ + k11]);
+      lj2 = (float)__ldg(&a.tables[TAB_LJ2 * TABSZ + k11]);
+      lj3 = (float)__ldg(&a.tables[TAB_LJ3 * TABSZ + k11]);
+      lj4 = (float)__ldg(&a.tables[TAB_LJ4 * TABSZ + k11]);
+      off = (float)__ldg(&a.tables[TAB_OFFSET * TABSZ + k11]);
+    }
+    const float4 xi = xr[i];
+    const int ti = __float_as_int(xi.w);
+    const float csx = (float)a.box.cs[0], csy = (float)a.box.cs[1], csz = (float)a.box.cs[2];
+    const int num = a.numneigh[i];
+    for (int k = lane; k < num; k += TPA) {
+      const unsigned int e = (unsigned int)__ldcs(&a.nlist[(size_t)k * a.stride + i]);
+      const int j = (int)(e & MD_JMASK);
+      const int code = (int)(e >> MD_JBITS);
+      const int dz = code / 9 - 1, rem = code - 9 * (dz + 1);
+      const int dy = rem / 3 - 1, dx = rem - 3 * (dy + 1) - 1;
+      const float4 xj = xr[j];
+      // x_i - (x_j + image shift) = (xr_i - xr_j) - (neighbour cell centre - own cell centre)
+      const float delx = (xi.x - xj.x) - (float)dx * csx;
+      const float dely = (xi.y - xj.y) - (float)dy * csy;
+      const float delz = (xi.z - xj.z) - (float)dz * csz;
+      const float rsq = delx * delx + dely * dely + delz * delz;
+      const int tj = __float_as_int(xj.w);
+      const int tt = ti * a.ntp1 + tj;
+      const float cs = SINGLE ? cutsq1 : tabf[0 * nt2 + tt];
+      if (rsq < cs) {
+        const float c1 = SINGLE ? lj1 : tabf[1 * nt2 + tt];
+        const float c2 = SINGLE ? lj2 : tabf[2 * nt2 + tt];
+        const float r2inv = __frcp_rn(rsq);
+        const float r6inv = r2inv * r2inv * r2inv;
+        const float forcelj = r6inv * (c1 * r6inv - c2);
+        const float fpair = forcelj * r2inv;
+        fx += (double)(delx * fpair);
+        fy += (double)(dely * fpair);
+        fz += (double)(delz * fpair);
+        if (EV) {
+          const float c3 = SINGLE ? lj3 : tabf[3 * nt2 + tt];
+          const float c4 = SINGLE ? lj4 : tabf[4 * nt2 + tt];
+          const float co = SINGLE ? off : tabf[5 * nt2 + tt];
+          const float evdwl = r6inv * (c3 * r6inv - c4) - co;
+          acc[0] += 0.5 * (double)evdwl;
+          const float hf = 0.5f * fpair;
+          acc[1] += (double)(delx * delx * hf);
+          acc[2] += (double)(dely * dely * hf);
+          acc[3] += (double)(delz * delz * hf);
+          acc[4] += (double)(delx * dely * hf);
+          acc[5] += (double)(delx * delz * hf);
+          acc[6] += (double)(dely * delz * hf);
+        }
+      }
+    }
+  }
+  fx = lane_sum<TPA>(fx);
+  fy = lane_sum<TPA>(fy);
+  fz = lane_sum<TPA>(fz);
+  if (active && lane == 0) {
+    a.f[i] = fx;
+    a.f[a.stride + i] = fy;
+    a.f[2 * a.stride + i] = fz;
+  }
+  if (EV) {
+    if (ATOM) {
+      double e[7];
+#pragma unroll
+      for (int k = 0; k < 7; k++) e[k] = lane_sum<TPA>(acc[k]);
+      if (active && lane == 0) {
+        const int o = a.orig[i];
+        if (a.eatom) a.eatom[o] = e[0];
+        if (a.vatom)
+#pragma unroll
+          for (int k = 0; k < 6; k++) a.vatom[6 * (size_t)o + k] = e[1 + k];
+      }
+    }
+    block_partials_finish<7>(acc, red, a.partial, a.counter, a.ev, false);
+  }
+}
+
+template <int TPA, bool EV, bool ATOM, bool SINGLE>
+void launch_t(b200_ctx *c, const PairArgs &a) {
+  const int B = 128;
+  const int grid = md_blocks((long long)a.n * TPA, B);
+  if (c->prec == B200_PREC_MIXED)
+    k_lj_mixed<TPA, EV, ATOM, SINGLE><<<grid, B, 0, c->stream>>>(a, c->xr);
+  else
+    k_lj_fp64<TPA, EV, ATOM, SINGLE><<<grid, B, 0, c->stream>>>(a, c->x4);
+  c->launches++;
+}
+
+template <int TPA>
+void launch_tpa(b200_ctx *c, const PairArgs &a, bool ev, bool atom, bool single) {
+  if (!ev) {
+    if (single) launch_t<TPA, false, false, true>(c, a);
+    else launch_t<TPA, false, false, false>(c, a);
+  } else if (!atom) {
+    if (single) launch_t<TPA, true, false, true>(c, a);
+    else launch_t<TPA, true, false, false>(c, a);
+  } else {
+    if (single) launch_t<TPA, true, true, true>(c, a);
+    else launch_t<TPA, true, true, false>(c, a);
+  }
+}
+
+}  // namespace
+
+cudaError_t md_lj_compute(b200_ctx *c, bool ev, bool atom_ev, double *eatom, double *vatom) {
+  PairArgs a;
+  a.n = c->n;
+  a.stride = c->stride;
+  a.ntp1 = c->ntypes + 1;
+  a.box = c->box;
+  a.tables = c->tables_dev;
+  a.cell = c->cell;
+  a.nlist = c->nlist;
+  a.numneigh = c->numneigh;
+  a.orig = c->orig;
+  a.f = c->f;
+  a.partial = c->partial;
+  a.counter = c->counter;
+  a.ev = c->ev;
+  a.eatom = eatom;
+  a.vatom = vatom;
+  const bool single = c->ntypes == 1;
+  switch (c->tpa) {
+    case 1: launch_tpa<1>(c, a, ev, atom_ev, single); break;
+    case 2: launch_tpa<2>(c, a, ev, atom_ev, single); break;
+    case 4: launch_tpa<4>(c, a, ev, atom_ev, single); break;
+    default: launch_tpa<8>(c, a, ev, atom_ev, single); break;
+  }
+  return cudaGetLastError();
+}

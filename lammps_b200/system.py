@@ -1,0 +1,229 @@
+"""`System`: a host-side driver of one device-resident box.
+
+It plays the role of the reference's Verlet/Thermo plumbing around the
+engine: it pushes the pair tables, masses, box and atoms through the C ABI,
+runs `setup` + `run N` on the device (CUDA graph per step) and turns the
+device's thermo rows into the reference's thermo columns
+(ComputeTemp, ComputePE, ComputePressure, Thermo; src/compute_temp.cpp:59-89,
+src/compute_pressure.cpp:177-207, src/thermo.cpp:1581-1619).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from .inputs import UNITS, velocity_create
+from .pair import PairEAM, PairLJCut
+
+
+class System:
+    def __init__(self, units: str = "lj", precision: str = "fp64", device: int = 0):
+        if units not in UNITS:
+            raise ValueError(f"unknown units {units}")
+        self._L = _abi.load()
+        self.units = units
+        self.u = UNITS[units]
+        self.precision = precision
+        h = C.c_void_p()
+        rc = self._L.b200_create(device, _abi.PREC[precision], C.byref(h))
+        self._h = h
+        if rc != 0:
+            msg = self._L.b200_last_error(h).decode() if h.value else "b200_create failed"
+            raise _abi.B200Error(rc, msg)
+        self.dt = self.u["dt"]
+        self.thermo_every = 0
+        self.n = 0
+        self.ntypes = 0
+        self.mass = None
+        self.pair = None
+        self.box_lo = self.box_hi = None
+        self.ntimestep = 0
+        self.thermo_rows = []
+
+    def __del__(self):
+        try:
+            if self._h:
+                self._L.b200_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+    def close(self):
+        self.__del__()
+
+    def _ck(self, rc):
+        if rc != 0:
+            raise _abi.B200Error(rc, self._L.b200_last_error(self._h).decode())
+
+    # ---- settings --------------------------------------------------------
+    def set_box(self, lo, hi):
+        self.box_lo = np.ascontiguousarray(lo, dtype=np.float64)
+        self.box_hi = np.ascontiguousarray(hi, dtype=np.float64)
+        self._ck(self._L.b200_set_box(self._h, _abi.dptr(self.box_lo), _abi.dptr(self.box_hi)))
+
+    def set_neighbor(self, skin=None, every=1, delay=10, check=True, one=0):
+        skin = self.u["skin"] if skin is None else skin
+        self.skin = skin
+        self._ck(self._L.b200_set_neighbor(self._h, skin, every, delay, int(check), one))
+
+    def set_pair(self, pair):
+        self.pair = pair
+        self.ntypes = pair.ntypes
+        t = pair.tables()
+        if isinstance(pair, PairLJCut):
+            self._ck(self._L.b200_set_lj(self._h, pair.ntypes, *(_abi.dptr(t[k]) for k in
+                                                                ("cutsq", "lj1", "lj2", "lj3", "lj4", "offset"))))
+        elif isinstance(pair, PairEAM):
+            fr = np.ascontiguousarray(t["frho_spline"])
+            rr = np.ascontiguousarray(t["rhor_spline"])
+            zr = np.ascontiguousarray(t["z2r_spline"])
+            self._keep = (fr, rr, zr)
+            self._ck(self._L.b200_set_eam(
+                self._h, pair.ntypes, t["nrho"], t["drho"], t["nr"], t["dr"], t["rhomax"], t["cutmax"],
+                fr.shape[0], _abi.dptr(fr), rr.shape[0], _abi.dptr(rr), zr.shape[0], _abi.dptr(zr),
+                _abi.iptr(np.ascontiguousarray(t["type2frho"], dtype=np.int32)),
+                _abi.iptr(np.ascontiguousarray(t["type2rhor"], dtype=np.int32)),
+                _abi.iptr(np.ascontiguousarray(t["type2z2r"], dtype=np.int32))))
+            if self.mass is None:
+                self.set_mass([m if m > 0 else 1.0 for m in pair.mass[1:]])
+        else:
+            raise TypeError("unsupported pair style")
+        self.tables = t
+
+    def set_mass(self, masses):
+        """masses for types 1..ntypes."""
+        m = np.zeros(len(masses) + 1)
+        m[1:] = masses
+        self.mass = m
+        self._ck(self._L.b200_set_mass(self._h, len(masses), _abi.dptr(m)))
+
+    def set_timestep(self, dt):
+        self.dt = dt
+
+    def set_thermo(self, every):
+        self.thermo_every = every
+
+    def set_launch(self, threads_per_atom=0, block=128):
+        self._ck(self._L.b200_set_launch(self._h, threads_per_atom, block))
+
+    def launch(self):
+        t, b = C.c_int(), C.c_int()
+        self._ck(self._L.b200_get_launch(self._h, C.byref(t), C.byref(b)))
+        return t.value, b.value
+
+    # ---- atoms -----------------------------------------------------------
+    def set_atoms(self, x, type_=None, v=None):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        self.n = x.shape[0]
+        t = np.ones(self.n, np.int32) if type_ is None else np.ascontiguousarray(type_, dtype=np.int32)
+        vv = None if v is None else np.ascontiguousarray(v, dtype=np.float64)
+        self.type = t
+        self._ck(self._L.b200_upload_atoms(self._h, self.n, _abi.dptr(x), _abi.dptr(vv),
+                                           _abi.iptr(t), None))
+
+    def create_velocity(self, x, t, seed, gaussian=False, loop="geom", mom=True, type_=None):
+        type_ = np.ones(x.shape[0], np.int32) if type_ is None else type_
+        return velocity_create(x, type_, self.mass, t, seed, self.units, gaussian, loop, mom)
+
+    def download(self):
+        n = self.n
+        x = np.zeros((n, 3))
+        v = np.zeros((n, 3))
+        f = np.zeros((n, 3))
+        img = np.zeros((n, 3), np.int32)
+        self._ck(self._L.b200_download_atoms(self._h, _abi.dptr(x), _abi.dptr(v), _abi.dptr(f),
+                                             _abi.iptr(img)))
+        return dict(x=x, v=v, f=f, image=img)
+
+    # ---- actions ---------------------------------------------------------
+    def neigh_build(self):
+        self._ck(self._L.b200_neigh_build(self._h))
+
+    def compute(self, eflag=1, vflag=1, per_atom=False):
+        """Pair::compute on the current atoms (lists must be built)."""
+        eng = C.c_double(0.0)
+        vir = np.zeros(6)
+        n = self.n
+        ea = np.zeros(n) if per_atom else None
+        va = np.zeros((n, 6)) if per_atom else None
+        ef = eflag | (2 if per_atom else 0)
+        vf = vflag | (4 if per_atom else 0)
+        self._ck(self._L.b200_pair_compute(self._h, ef, vf, C.byref(eng), _abi.dptr(vir),
+                                           _abi.dptr(ea), _abi.dptr(va)))
+        out = dict(eng=eng.value, virial=vir)
+        if per_atom:
+            out.update(eatom=ea, vatom=va)
+        return out
+
+    def _row_to_thermo(self, row):
+        u = self.u
+        n = self.n
+        dof = 3.0 * n - 3.0
+        tfactor = u["mvv2e"] / (dof * u["boltz"]) if dof > 0 else 0.0
+        temp = row[1] * tfactor
+        pe = row[2]
+        epair = pe / n if u["normflag"] else pe
+        ke = temp * 0.5 * dof * u["boltz"]
+        if u["normflag"]:
+            ke /= n
+        vol = float(np.prod(self.box_hi - self.box_lo))
+        press = (dof * u["boltz"] * temp + row[3] + row[4] + row[5]) / 3.0 * (1.0 / vol) * u["nktv2p"]
+        return dict(Step=int(round(row[0])), Temp=temp, E_pair=epair, E_mol=0.0,
+                    TotEng=epair + ke, Press=press, eng=pe, virial=np.array(row[3:9]), ke2=row[1])
+
+    def setup(self):
+        row = np.zeros(9)
+        self._ck(self._L.b200_setup(self._h, _abi.dptr(row)))
+        row[0] = self.ntimestep
+        r = self._row_to_thermo(row)
+        self.thermo_rows = [r]
+        return r
+
+    def run(self, nsteps):
+        ftm2v = self.u["ftm2v"]
+        nout = 1 + (nsteps // self.thermo_every if self.thermo_every > 0 else 0)
+        rows = np.zeros((nout, 9))
+        nr = C.c_int(0)
+        self._ck(self._L.b200_run(self._h, nsteps, self.dt, ftm2v, self.thermo_every,
+                                  _abi.dptr(rows), nout, C.byref(nr)))
+        self.ntimestep += nsteps
+        out = [self._row_to_thermo(rows[k]) for k in range(min(nr.value, nout))]
+        self.thermo_rows.extend(out)
+        return out
+
+    # ---- diagnostics -----------------------------------------------------
+    def neigh_stats(self):
+        tot = C.c_longlong()
+        nc, nd, mx, cap = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        self._ck(self._L.b200_neigh_stats(self._h, C.byref(tot), C.byref(nc), C.byref(nd),
+                                          C.byref(mx), C.byref(cap)))
+        return dict(full_total=tot.value, ncalls=nc.value, ndanger=nd.value, maxneigh=mx.value,
+                    capacity=cap.value)
+
+    def half_list(self):
+        n = self.n
+        num = np.zeros(n, np.int32)
+        tot = C.c_longlong()
+        self._ck(self._L.b200_neigh_half(self._h, _abi.iptr(num), None, None, 0, C.byref(tot)))
+        m = tot.value
+        jo = np.zeros(max(m, 1), np.int32)
+        ji = np.zeros(max(m, 1), np.int32)
+        self._ck(self._L.b200_neigh_half(self._h, _abi.iptr(num), _abi.iptr(jo), _abi.iptr(ji), m,
+                                         C.byref(tot)))
+        return num, jo[:m], ji[:m]
+
+    def rho_fp(self):
+        rho = np.zeros(self.n)
+        fp = np.zeros(self.n)
+        self._ck(self._L.b200_get_rho_fp(self._h, _abi.dptr(rho), _abi.dptr(fp)))
+        return rho, fp
+
+    @property
+    def kernel_launches(self):
+        return self._L.b200_kernel_launches(self._h)
+
+    @property
+    def stream(self):
+        return self._L.b200_stream(self._h)
