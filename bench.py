@@ -1,0 +1,437 @@
+#!/usr/bin/env python
+"""Throughput of the short-range MD step on B200, in Matom-steps/s.
+
+Workload (one bench step = 100 NVE timesteps of the box, continuing the
+trajectory): the EAM configuration -- 32,000 atoms, fcc 20^3, a = 3.615 A,
+synthetic 5000-point setfl tables (lammps_b200/eam_synth.py), Gaussian
+velocities at 1600 K (seed 376847), dt = 5 fs, skin 1.0 A,
+`neigh_modify every 1 delay 5 check yes`, FP32-mixed precision.  The FP64
+form of the same workload and the 4,000,000-atom LJ configuration (fcc 100^3,
+rho* 0.8442, T* 1.44, rc 2.5, skin 0.3, rebuild every 20) in both precisions
+are reported beside it.  Inputs are seeded synthetic data of the reference's
+benchmark shapes.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Timing: W untimed bench steps, then K bench steps bracketed by a barrier and
+torch.cuda.synchronize(); each bench step is timed with CUDA events on the
+engine's stream, after an L2 flush (a 256 MB write) that is outside the
+events.  `value` is the aggregate over ranks (max time over ranks).  `e2e` is
+the same metric through the public API with host buffers: upload of x, v,
+type, setup, 100 steps, download of x, v, f, image -- wall clock around
+synchronised calls.  Under torchrun each rank runs its own replica (weak
+scaling, no data-path collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "Matom-steps/s LJ+EAM: FP32-mixed vs FP64 on 1 B200 at ≤1e-5 rel force error"
+MD_STEPS = 100          # NVE timesteps per bench step
+DEVICE = 0              # CUDA device of this rank
+FLUSH_BYTES = 256 << 20  # > 126 MB L2
+
+
+# ---------------------------------------------------------------------------
+# workloads
+
+def eam32k_inputs():
+    from lammps_b200 import inputs
+    x = inputs.lattice("fcc", 20, 20, 20, 3.615)
+    v = inputs.velocity_create(x, np.ones(len(x), np.int32), np.array([0.0, 63.55]), 1600.0,
+                               376847, "metal", gaussian=True, loop="geom")
+    return x, v, np.array([20 * 3.615] * 3)
+
+
+def make_eam32k(precision, setfl, x, v, hi):
+    from lammps_b200 import PairEAMAlloy, System
+    s = System("metal", precision, device=DEVICE)
+    s.set_box([0.0, 0.0, 0.0], hi)
+    p = PairEAMAlloy(1)
+    p.coeff(setfl, ["Cu"])
+    s.set_pair(p)
+    s.set_neighbor(1.0, every=1, delay=5, check=True)
+    s.set_timestep(0.005)
+    s.set_thermo(0)
+    s.set_atoms(x, None, v)
+    return s
+
+
+def lj4m_inputs():
+    from lammps_b200 import inputs
+    a = inputs.lj_lattice_constant("fcc", 0.8442)
+    x = inputs.lattice("fcc", 100, 100, 100, a)
+    v = inputs.velocity_create(x, np.ones(len(x), np.int32), np.array([0.0, 1.0]), 1.44, 87287,
+                               "lj", gaussian=True, loop="geom")
+    return x, v, np.array([100 * a] * 3)
+
+
+def make_lj(precision, x, v, hi):
+    from lammps_b200 import PairLJCut, System
+    s = System("lj", precision, device=DEVICE)
+    s.set_box([0.0, 0.0, 0.0], hi)
+    p = PairLJCut(2.5)
+    p.coeff(1, 1, 1.0, 1.0, 2.5)
+    s.set_pair(p)
+    s.set_mass([1.0])
+    s.set_neighbor(0.3, every=20, delay=0, check=False)
+    s.set_timestep(0.005)
+    s.set_thermo(0)
+    s.set_atoms(x, None, v)
+    return s
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.device)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def load_traffic():
+    """dram bytes per launch of the profiled kernels, from the committed ncu summary."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as fh:
+            return json.load(fh)
+    except Exception:
+        return {}
+
+
+def device_time_run(sysm, torch, ext, flush, nsteps):
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(ext):
+        flush.zero_()
+    e0.record(ext)
+    sysm.run(nsteps)
+    e1.record(ext)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def time_form(sysm, torch, flush, K, W, timing=False):
+    """Warm up, then K timed bench steps; returns (total ms, per-step ms list)."""
+    ext = torch.cuda.ExternalStream(sysm.stream)
+    sysm.setup()
+    sysm.set_timing(timing)
+    for _ in range(W):
+        device_time_run(sysm, torch, ext, flush, MD_STEPS)
+    sysm.timing(reset=True)
+    ms = [device_time_run(sysm, torch, ext, flush, MD_STEPS) for _ in range(K)]
+    return sum(ms), ms
+
+
+def e2e_run(sysm, x_pin, v_pin, K):
+    """Public-API end to end: host buffers in, host results out, per bench step."""
+    n = x_pin.shape[0]
+    t0 = time.perf_counter()
+    for _ in range(K):
+        sysm.set_atoms(x_pin, None, v_pin)
+        sysm.setup()
+        sysm.run(MD_STEPS)
+        out = sysm.download()
+    t1 = time.perf_counter()
+    h2d = x_pin.nbytes + v_pin.nbytes + n * 4
+    d2h = out["x"].nbytes + out["v"].nbytes + out["f"].nbytes + out["image"].nbytes
+    return (t1 - t0) * 1e3, h2d, d2h
+
+
+def cpu_reference(setfl, x, v, hi, seconds=10.0, threads=None):
+    """The oracle port (reference CPU algorithm) on the host cores."""
+    import oracle
+    threads = threads or os.cpu_count() or 1
+    s = oracle.OracleSim("metal", threads=threads)
+    s.box([0.0, 0.0, 0.0], hi)
+    s.atoms(x, v)
+    s.eam_setfl(setfl, [0])
+    s.neighbor(1.0, 1, 5, True, 1000)
+    s.timestep(0.005)
+    s.setup()
+    t0 = time.perf_counter()
+    s.run(5)
+    dt5 = time.perf_counter() - t0
+    nsteps = max(5, min(200, int(seconds / max(dt5 / 5, 1e-6))))
+    t0 = time.perf_counter()
+    s.run(nsteps)
+    dt = time.perf_counter() - t0
+    return dict(value=len(x) * nsteps / dt / 1e6, unit="Matom-steps/s", cores=threads, kind="port",
+                sample=f"EAM 32,000 atoms x {nsteps} NVE steps (oracle port, OpenMP {threads} threads), "
+                       f"{dt:.1f} s")
+
+
+def dist_setup():
+    import torch
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+        dist.init_process_group("nccl" if torch.cuda.is_available() else "gloo",
+                                timeout=datetime.timedelta(seconds=300))
+    return ws, rank, local
+
+
+def allmax(val, ws, torch):
+    if ws == 1:
+        return val
+    import torch.distributed as dist
+    t = torch.tensor([val], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def profile_case(args):
+    """One form of one workload, W warm-up + K bench steps, for ncu captures."""
+    import torch
+    torch.cuda.set_device(0)
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    work, prec = args.case.split("-")
+    if work == "eam32k":
+        tmp = tempfile.mkdtemp(prefix="b200prof_")
+        from lammps_b200.eam_synth import write_setfl
+        setfl = write_setfl(os.path.join(tmp, "Cu_synth.eam.alloy"))
+        x, v, hi = eam32k_inputs()
+        s = make_eam32k(prec, setfl, x, v, hi)
+    elif work == "lj4m":
+        x, v, hi = lj4m_inputs()
+        s = make_lj(prec, x, v, hi)
+    else:
+        raise SystemExit(f"unknown case {args.case}")
+    total, per = time_form(s, torch, flush, args.steps, max(args.warmup, 1))
+    print(json.dumps({"case": args.case, "atoms": s.n, "steps": args.steps,
+                      "matom_steps_per_s": s.n * MD_STEPS * args.steps / (total * 1e3),
+                      "launch": s.launch()}))
+    s.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-extras", action="store_true", help="skip the FP64 and 4M-atom LJ lines")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--case", default=None,
+                    help="profile one form only: eam32k-mixed, eam32k-fp64, lj4m-mixed, lj4m-fp64")
+    args = ap.parse_args()
+    if args.case:
+        return profile_case(args)
+    K, W = args.steps, max(args.warmup, 3)
+    ws, rank, local = dist_setup()
+    config = {"workload": "eam-32k fcc 20^3 synthetic setfl, 100 NVE steps per bench step "
+                          "(configs[1]); also lj-4M fcc 100^3 (configs[4])",
+              "atoms": 32000, "md_steps_per_step": MD_STEPS, "precision": "mixed",
+              "l2": "flushed (256 MB write) before every timed bench step",
+              "parallelism": f"replicas x{ws}"}
+    tmp = tempfile.mkdtemp(prefix="b200bench_")
+    from lammps_b200.eam_synth import write_setfl
+    setfl = write_setfl(os.path.join(tmp, "Cu_synth.eam.alloy"))
+    x, v, hi = eam32k_inputs()
+
+    if args.impl == "reference":
+        if rank == 0:
+            cpu = cpu_reference(setfl, x, v, hi, seconds=max(5.0, 2.0 * (K + W) / 3))
+            line = {"metric": METRIC, "value": cpu["value"], "unit": "Matom-steps/s", "n_gpus": ws,
+                    "steps": K, "warmup": W, "ms_per_step": 32000 * MD_STEPS / (cpu["value"] * 1e3),
+                    "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                    "dtype": "f64", "data": "synthetic (seeded lattice + velocities, synthetic setfl)",
+                    "config": config, "impl": "reference", "cpu_baseline": cpu,
+                    "e2e": {"value": cpu["value"], "unit": "Matom-steps/s", "h2d_bytes_per_step": 0,
+                            "d2h_bytes_per_step": 0}}
+            print(json.dumps(line))
+        return
+
+    import torch
+    global DEVICE
+    dev = local if torch.cuda.device_count() > 1 else 0
+    DEVICE = dev
+    torch.cuda.set_device(dev)
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    sysm = make_eam32k("mixed", setfl, x, v, hi)
+    n = sysm.n
+    ext = torch.cuda.ExternalStream(sysm.stream)
+
+    # ---- headline: mixed precision EAM, device-timed -----------------------
+    launches0 = None
+    sysm.setup()
+    for _ in range(W):
+        device_time_run(sysm, torch, ext, flush, MD_STEPS)
+    barrier(ws)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    launches0 = sysm.kernel_launches
+    per = [device_time_run(sysm, torch, ext, flush, MD_STEPS) for _ in range(K)]
+    torch.cuda.synchronize()
+    launches = sysm.kernel_launches - launches0
+    barrier(ws)
+    clk = clocks.stop()
+    total_ms = allmax(sum(per), ws, torch)
+    value = ws * n * MD_STEPS * K / (total_ms * 1e3)
+
+    # ---- per-phase device timers over the same number of bench steps ------
+    sysm.set_timing(True)
+    for _ in range(2):
+        device_time_run(sysm, torch, ext, flush, MD_STEPS)
+    sysm.timing(reset=True)
+    per_t = [device_time_run(sysm, torch, ext, flush, MD_STEPS) for _ in range(K)]
+    ph = sysm.timing(reset=True)
+    sysm.set_timing(False)
+    steps_t = max(ph["steps"], 1)
+    phases = {k: ph[k] / steps_t for k in sysm.PHASES}
+    dom = max(("pair1", "pair2"), key=lambda k: phases[k])
+    # algorithmic bytes per atom of the dominant EAM kernel: force pass reads
+    # x (24 B) and fp (8 B) and writes f (24 B); density pass reads x (24 B)
+    # and writes rho, fp (16 B)
+    bytes_per_atom = 56.0 if dom == "pair2" else 40.0
+    peak, peak_kind = load_peaks()
+    achieved = bytes_per_atom * n / (phases[dom] * 1e-3) / 1e9
+    traffic = load_traffic().get(f"eam32k_mixed_{dom}")
+    step_ms = sum(per_t) / (K * MD_STEPS)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic,
+                "kernel": "k_eam_force (mixed)" if dom == "pair2" else "k_eam_rho (mixed)",
+                "kernel_ms": phases[dom], "peak_source": f"{peak_kind} hbm_gbs",
+                "step": {"alg_bytes_per_atom_step": 200.0,
+                         "achieved_gbs": 200.0 * n / (step_ms * 1e-3) / 1e9}}
+
+    # ---- end to end through the public API --------------------------------
+    x_pin = np.ascontiguousarray(x)
+    v_pin = np.ascontiguousarray(v)
+    e2e_run(sysm, x_pin, v_pin, 1)
+    e_ms, h2d, d2h = e2e_run(sysm, x_pin, v_pin, K)
+    e_ms = allmax(e_ms, ws, torch)
+    e2e = {"value": ws * n * MD_STEPS * K / (e_ms * 1e3), "unit": "Matom-steps/s",
+           "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+
+    extras = {}
+    if not args.no_extras:
+        s64 = make_eam32k("fp64", setfl, x, v, hi)
+        t64, _ = time_form(s64, torch, flush, K, W)
+        extras["eam_32k"] = {"mixed": value / ws, "fp64": n * MD_STEPS * K / (t64 * 1e3)}
+        extras["eam_32k"]["mixed_over_fp64"] = extras["eam_32k"]["mixed"] / extras["eam_32k"]["fp64"]
+        s64.close()
+        x4, v4, hi4 = lj4m_inputs()
+        lj = {}
+        for prec in ("mixed", "fp64"):
+            s = make_lj(prec, x4, v4, hi4)
+            k4 = max(2, K // 3)
+            t, _ = time_form(s, torch, flush, k4, 2)
+            s.set_timing(True)
+            ext4 = torch.cuda.ExternalStream(s.stream)
+            device_time_run(s, torch, ext4, flush, MD_STEPS)
+            s.timing(reset=True)
+            device_time_run(s, torch, ext4, flush, MD_STEPS)
+            ph4 = s.timing(reset=True)
+            lj[prec] = len(x4) * MD_STEPS * k4 / (t * 1e3)
+            lj[prec + "_phases_ms_per_step"] = {k: ph4[k] / max(ph4["steps"], 1) for k in s.PHASES}
+            s.close()
+        lj["mixed_over_fp64"] = lj["mixed"] / lj["fp64"]
+        f_ms = lj["mixed_phases_ms_per_step"]["pair1"]
+        lj["force_kernel_gbs"] = 48.0 * len(x4) / (f_ms * 1e-3) / 1e9
+        extras["lj_4M"] = lj
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cpu = cpu_reference(setfl, x, v, hi, seconds=10.0)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "Matom-steps/s", "n_gpus": ws, "steps": K,
+                "warmup": W, "ms_per_step": total_ms / K, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32-mixed (f64 positions/sums)",
+                "data": "synthetic (seeded fcc lattice + Gaussian velocities, synthetic setfl EAM)",
+                "config": config, "clocks": clk, "e2e": e2e, "gpu_launches": int(launches),
+                "roofline": roofline, "phases_ms_per_md_step": phases, "cpu_baseline": cpu}
+        line.update(extras)
+        print(json.dumps(line))
+    sysm.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

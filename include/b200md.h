@@ -82,7 +82,11 @@ long long b200_bytes(const b200_ctx *ctx);
    src/domain.cpp:213-217). */
 int b200_set_box(b200_ctx *ctx, const double lo[3], const double hi[3]);
 /* `neighbor skin bin` + `neigh_modify every/delay/check/one`
-   (src/neighbor.cpp:1731-1790).  one <= 0 picks a capacity from the density. */
+   (src/neighbor.cpp:1731-1790).  one > 0 is a hard per-atom limit: a list
+   longer than that fails with B200_ERR_NEIGH_OVERFLOW, as the reference's
+   "Neighbor list overflow, boost neigh_modify one".  one == 0 sizes the list
+   from the density, one < 0 starts at -one entries per atom; in both cases
+   the list grows when needed (b200_run replays a chunk that overflowed). */
 int b200_set_neighbor(b200_ctx *ctx, double skin, int every, int delay, int check, int one);
 /* Per-type masses, mass[1..ntypes] (Atom::mass). */
 int b200_set_mass(b200_ctx *ctx, int ntypes, const double *mass);
@@ -165,7 +169,19 @@ int b200_get_rho_fp(b200_ctx *ctx, double *rho, double *fp);
    the autotuner on the next b200_setup) and threads per block. */
 int b200_set_launch(b200_ctx *ctx, int threads_per_atom, int block_size);
 int b200_get_launch(const b200_ctx *ctx, int *threads_per_atom, int *block_size);
-/* Kernel launches issued by the context since creation (for accounting). */
+/* Phase timers of b200_run (the Timer categories of Verlet::run,
+   src/timer.h:19-20, src/verlet.cpp:237-306), measured on the device with
+   CUDA events recorded inside each step's graph.  Phases:
+     0 fix nve initial half-step + rebuild decision
+     1 neighbor rebuild (wrap, cell sort, list) -- near zero on steps without
+     2 pair pass 1 (LJ force; EAM density + embedding)
+     3 pair pass 2 (EAM force; zero for LJ)
+     4 fix nve final half-step (+ kinetic energy and thermo row on output steps)
+   b200_get_timing returns milliseconds summed over the timed steps. */
+int b200_set_timing(b200_ctx *ctx, int on);
+int b200_get_timing(b200_ctx *ctx, double phase_ms[5], long long *steps, int reset);
+/* Kernel launches issued by the context since creation (for accounting);
+   kernels replayed inside step graphs are counted per replay. */
 long long b200_kernel_launches(const b200_ctx *ctx);
 /* CUDA stream of the context, as a void* (cudaStream_t). */
 void *b200_stream(const b200_ctx *ctx);

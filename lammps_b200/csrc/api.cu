@@ -47,11 +47,14 @@ void dfree(T *&p) {
 }
 
 void invalidate_graphs(b200_ctx *c) {
-  for (auto &g : c->step_exec)
-    if (g) {
-      cudaGraphExecDestroy(g);
-      g = nullptr;
-    }
+  for (int k = 0; k < 2; k++) {
+    if (c->step_exec[k]) cudaGraphExecDestroy(c->step_exec[k]);
+    if (c->step_graph[k]) cudaGraphDestroy(c->step_graph[k]);
+    c->step_exec[k] = nullptr;
+    c->step_graph[k] = nullptr;
+    c->ev_nodes[k].clear();
+    c->step_kernels[k] = 0;
+  }
   c->graph_valid = false;
 }
 
@@ -171,6 +174,7 @@ int init_cutoffs_and_cells(b200_ctx *c) {
   }
   if (ncells > (long long)4096 * 4096 - 1)
     return set_err(c, B200_ERR_ARG, "too many cells (%lld)", ncells);
+  if ((int)ncells != c->ncells) invalidate_graphs(c);  // scan launch shape changes
   c->ncells = (int)ncells;
   return B200_OK;
 }
@@ -213,6 +217,7 @@ int upload_tables(b200_ctx *c) {
 
 int alloc_cells(b200_ctx *c) {
   if (c->ncells + 1 > c->ncell_alloc) {
+    invalidate_graphs(c);
     int m = c->ncells + 1;
     CK(dalloc(&c->cell_count, (size_t)m));
     CK(dalloc(&c->cell_start, (size_t)m));
@@ -224,7 +229,9 @@ int alloc_cells(b200_ctx *c) {
 
 int alloc_list(b200_ctx *c, int capacity) {
   long long need = (long long)capacity * c->stride;
+  if (capacity != c->capacity) invalidate_graphs(c);  // capacity is a kernel argument
   if (need > c->nlist_alloc) {
+    invalidate_graphs(c);
     CK(dalloc(&c->nlist, (size_t)need));
     c->nlist_alloc = need;
   }
@@ -237,7 +244,7 @@ int default_capacity(const b200_ctx *c) {
   const double dens = c->n / vol;
   const double pi = 3.14159265358979323846;
   const double expect = 4.0 / 3.0 * pi * c->cutneighmax * c->cutneighmax * c->cutneighmax * dens;
-  int cap = (int)(1.4 * expect + 32.0);
+  int cap = (int)(2.0 * expect + 64.0);
   cap = (cap + 7) & ~7;
   return cap;
 }
@@ -323,27 +330,143 @@ int autotune(b200_ctx *c) {
   return B200_OK;
 }
 
-int capture_step(b200_ctx *c, bool out, double dtv, double dtf, cudaGraphExec_t *exec) {
+int capture_step(b200_ctx *c, bool out, double dtv, double dtf, int slot) {
+  // One MD step (Verlet::run body, src/verlet.cpp:223-308) as a CUDA graph.
+  // With timing on, event-record nodes mark the phase boundaries; their
+  // events are swapped per replay so every step's phases can be read back.
   cudaGraph_t g = nullptr;
+  const bool tm = c->timing;
+  const long long launches0 = c->launches;
   CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-  cudaError_t e = md_nve_initial(c, dtv, dtf);
+  cudaError_t e = cudaSuccess;
+  if (tm) e = cudaEventRecord(c->ph_event[0], c->stream);
+  if (e == cudaSuccess) e = md_nve_initial(c, dtv, dtf);
   if (e == cudaSuccess) e = md_decide(c);
+  if (e == cudaSuccess && tm) e = cudaEventRecord(c->ph_event[1], c->stream);
   if (e == cudaSuccess) e = md_rebuild(c, c->status + ST_REBUILD);
+  if (e == cudaSuccess && tm) e = cudaEventRecord(c->ph_event[2], c->stream);
   if (e == cudaSuccess) {
-    if (c->pstyle == B200_PAIR_LJ_CUT) e = md_lj_compute(c, out, false, nullptr, nullptr);
-    else e = md_eam_compute(c, out, false, nullptr, nullptr);
+    if (c->pstyle == B200_PAIR_LJ_CUT) {
+      e = md_lj_compute(c, out, false, nullptr, nullptr);
+      if (e == cudaSuccess && tm) e = cudaEventRecord(c->ph_event[3], c->stream);
+    } else {
+      e = md_eam_compute(c, out, false, nullptr, nullptr, tm ? c->ph_event[3] : nullptr);
+    }
   }
+  if (e == cudaSuccess && tm) e = cudaEventRecord(c->ph_event[4], c->stream);
   if (e == cudaSuccess) e = md_nve_final(c, dtf, out);
   if (e == cudaSuccess && out) e = md_record_row(c);
+  if (e == cudaSuccess && tm) e = cudaEventRecord(c->ph_event[5], c->stream);
   cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
+  c->launches = launches0;
   if (e != cudaSuccess || e2 != cudaSuccess) {
     if (g) cudaGraphDestroy(g);
     return set_err(c, B200_ERR_CUDA, "graph capture: %s / %s", cudaGetErrorString(e),
                    cudaGetErrorString(e2));
   }
-  e = cudaGraphInstantiate(exec, g, 0);
-  cudaGraphDestroy(g);
-  if (e != cudaSuccess) return set_err(c, B200_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+  // kernel nodes (for launch accounting) and event-record nodes in capture order
+  size_t nn = 0;
+  CK(cudaGraphGetNodes(g, nullptr, &nn));
+  std::vector<cudaGraphNode_t> nodes(nn);
+  CK(cudaGraphGetNodes(g, nodes.data(), &nn));
+  int kernels = 0;
+  c->ev_nodes[slot].clear();
+  for (auto nd : nodes) {
+    cudaGraphNodeType t;
+    CK(cudaGraphNodeGetType(nd, &t));
+    if (t == cudaGraphNodeTypeKernel) kernels++;
+    if (t == cudaGraphNodeTypeEventRecord) c->ev_nodes[slot].push_back(nd);
+  }
+  if (tm && c->ev_nodes[slot].size() != MD_NPHASE + 1) {
+    cudaGraphDestroy(g);
+    return set_err(c, B200_ERR_CUDA, "graph capture: expected %d event nodes, found %zu",
+                   MD_NPHASE + 1, c->ev_nodes[slot].size());
+  }
+  e = cudaGraphInstantiate(&c->step_exec[slot], g, 0);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return set_err(c, B200_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+  }
+  c->step_graph[slot] = g;
+  c->step_kernels[slot] = kernels;
+  return B200_OK;
+}
+
+int ensure_graphs(b200_ctx *c, double dtv, double dtf, double ftm2v) {
+  if (c->graph_valid) return B200_OK;
+  int rc = capture_step(c, false, dtv, dtf, 0);
+  if (!rc) rc = capture_step(c, true, dtv, dtf, 1);
+  if (rc) return rc;
+  c->graph_valid = true;
+  c->graph_dt = dtv;
+  c->graph_ftm2v = ftm2v;
+  c->graph_tpa = c->tpa;
+  c->graph_timing = c->timing;
+  return B200_OK;
+}
+
+// Larger neighbor-list capacity.  keep = true copies the current entries
+// (entry k of atom i sits at k*stride + i, so the old list is a prefix).
+int grow_list(b200_ctx *c, int capacity, bool keep) {
+  if (capacity <= c->capacity) return B200_OK;
+  long long need = (long long)capacity * c->stride;
+  if (need > c->nlist_alloc) {
+    int *nl = nullptr;
+    CK(cudaMalloc((void **)&nl, (size_t)need * sizeof(int)));
+    if (keep && c->nlist)
+      CK(cudaMemcpyAsync(nl, c->nlist, (size_t)c->capacity * c->stride * sizeof(int),
+                         cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (c->nlist) cudaFree(c->nlist);
+    c->nlist = nl;
+    c->nlist_alloc = need;
+  }
+  c->capacity = capacity;
+  invalidate_graphs(c);
+  return B200_OK;
+}
+
+// Save (save = true) or restore the per-atom state and status words that a
+// run chunk changes.
+int snapshot(b200_ctx *c, bool save) {
+  const size_t s = (size_t)c->stride;
+  if (c->snap_alloc < c->stride) {
+    CK(dalloc(&c->snap_x4, s));
+    CK(dalloc(&c->snap_xhold, s));
+    CK(dalloc(&c->snap_v, 3 * s));
+    CK(dalloc(&c->snap_f, 3 * s));
+    CK(dalloc(&c->snap_orig, s));
+    CK(dalloc(&c->snap_image, s));
+    CK(dalloc(&c->snap_cell, s));
+    CK(dalloc(&c->snap_xr, s));
+    if (!c->snap_status) CK(cudaMalloc((void **)&c->snap_status, ST_COUNT * sizeof(int)));
+    c->snap_alloc = c->stride;
+  }
+  auto cp = [&](void *a, void *b, size_t bytes) -> cudaError_t {
+    return save ? cudaMemcpyAsync(b, a, bytes, cudaMemcpyDeviceToDevice, c->stream)
+                : cudaMemcpyAsync(a, b, bytes, cudaMemcpyDeviceToDevice, c->stream);
+  };
+  const size_t n = (size_t)c->n;
+  CK(cp(c->x4, c->snap_x4, n * sizeof(double4)));
+  CK(cp(c->v, c->snap_v, 3 * s * sizeof(double)));
+  CK(cp(c->f, c->snap_f, 3 * s * sizeof(double)));
+  CK(cp(c->orig, c->snap_orig, n * sizeof(int)));
+  CK(cp(c->image, c->snap_image, n * sizeof(int)));
+  CK(cp(c->cell, c->snap_cell, n * sizeof(int)));
+  if (c->check) CK(cp(c->xhold, c->snap_xhold, n * sizeof(double4)));
+  if (c->prec == B200_PREC_MIXED) CK(cp(c->xr, c->snap_xr, n * sizeof(float4)));
+  CK(cp(c->status, c->snap_status, ST_COUNT * sizeof(int)));
+  return B200_OK;
+}
+
+int ensure_events(b200_ctx *c, size_t count) {
+  for (int k = 0; k <= MD_NPHASE; k++)
+    if (!c->ph_event[k]) CK(cudaEventCreate(&c->ph_event[k]));
+  while (c->ev_pool.size() < count) {
+    cudaEvent_t ev;
+    CK(cudaEventCreate(&ev));
+    c->ev_pool.push_back(ev);
+  }
   return B200_OK;
 }
 
@@ -396,8 +519,14 @@ int b200_destroy(b200_ctx *c) {
   dfree(c->slot); dfree(c->perm); dfree(c->cell_tmp);
   dfree(c->nlist); dfree(c->numneigh); dfree(c->partial); dfree(c->counter); dfree(c->ev);
   dfree(c->status); dfree(c->rows); dfree(c->tables_dev);
+  dfree(c->snap_x4); dfree(c->snap_xhold); dfree(c->snap_v); dfree(c->snap_f);
+  dfree(c->snap_orig); dfree(c->snap_image); dfree(c->snap_cell); dfree(c->snap_xr);
+  dfree(c->snap_status);
   dfree(c->eam.frho); dfree(c->eam.rhor); dfree(c->eam.z2r);
   dfree(c->eam.frho_f); dfree(c->eam.rhor_f); dfree(c->eam.z2r_f);
+  for (auto &ev : c->ph_event)
+    if (ev) cudaEventDestroy(ev);
+  for (auto ev : c->ev_pool) cudaEventDestroy(ev);
   if (c->status_host) cudaFreeHost(c->status_host);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -436,7 +565,8 @@ int b200_set_neighbor(b200_ctx *c, double skin, int every, int delay, int check,
   c->every = every;
   c->delay = delay;
   c->check = check ? 1 : 0;
-  c->one_user = one > 0 ? one : 0;
+  if (one != c->one_user) c->capacity = 0;  // re-size the list at the next setup
+  c->one_user = one;
   invalidate_graphs(c);
   return B200_OK;
 }
@@ -551,7 +681,8 @@ int b200_upload_atoms(b200_ctx *c, int n, const double *x, const double *v, cons
     if (type[i] < 1 || type[i] > c->ntypes)
       return set_err(c, B200_ERR_ARG, "Invalid atom type %d of atom %d", type[i], i);
   CK(cudaSetDevice(c->device));
-  invalidate_graphs(c);
+  // step graphs bake the atom count and the buffer addresses
+  if (n != c->n || n > c->nalloc) invalidate_graphs(c);
   if (n > c->nalloc) {
     const int stride = (n + 31) & ~31;
     CK(dalloc(&c->x4, stride));
@@ -640,7 +771,9 @@ static int prepare(b200_ctx *c) {
   if (!rc) rc = upload_tables(c);
   if (!rc) rc = alloc_cells(c);
   if (!rc && (c->capacity == 0 || c->one_user > 0 || !c->nlist)) {
-    int cap = c->one_user > 0 ? c->one_user : (c->capacity > 0 ? c->capacity : default_capacity(c));
+    int cap = c->one_user > 0   ? c->one_user
+              : c->one_user < 0 ? (c->capacity > 0 ? c->capacity : -c->one_user)
+              : (c->capacity > 0 ? c->capacity : default_capacity(c));
     rc = alloc_list(c, cap);
   }
   return rc;
@@ -754,19 +887,21 @@ int b200_run(b200_ctx *c, int nsteps, double dt, double ftm2v, int thermo_every,
     c->rows_cap = nout;
     invalidate_graphs(c);
   }
-  if (c->graph_valid && (c->graph_dt != dtv || c->graph_ftm2v != ftm2v || c->graph_tpa != c->tpa))
+  if (c->graph_valid && (c->graph_dt != dtv || c->graph_ftm2v != ftm2v || c->graph_tpa != c->tpa ||
+                         c->graph_timing != c->timing))
     invalidate_graphs(c);
-  if (!c->graph_valid) {
-    int rc = capture_step(c, false, dtv, dtf, &c->step_exec[0]);
-    if (!rc) rc = capture_step(c, true, dtv, dtf, &c->step_exec[1]);
+  const int chunk = 256;  // steps per timing read-back
+  if (c->timing) {
+    int rc = ensure_events(c, (size_t)(MD_NPHASE + 1) * chunk);
     if (rc) return rc;
-    c->graph_valid = true;
-    c->graph_dt = dtv;
-    c->graph_ftm2v = ftm2v;
-    c->graph_tpa = c->tpa;
+  }
+  {
+    int rc = ensure_graphs(c, dtv, dtf, ftm2v);
+    if (rc) return rc;
   }
   CK(cudaMemsetAsync(c->status + ST_ROW, 0, sizeof(int), c->stream));
   CK(cudaMemsetAsync(c->status + ST_OVERFLOW, 0, sizeof(int), c->stream));
+  CK(cudaMemsetAsync(c->status + ST_MAXNEIGH, 0, sizeof(int), c->stream));
   // host view of the current step for the output schedule
   CK(cudaMemcpyAsync(c->status_host, c->status, ST_COUNT * sizeof(int), cudaMemcpyDeviceToHost,
                      c->stream));
@@ -774,11 +909,68 @@ int b200_run(b200_ctx *c, int nsteps, double dt, double ftm2v, int thermo_every,
   long long step0 = ((long long)(unsigned int)c->status_host[ST_STEP_HI] << 32) |
                     (long long)(unsigned int)c->status_host[ST_STEP_LO];
   const long long last = step0 + nsteps;
-  for (long long s = step0 + 1; s <= last; s++) {
-    const bool out = (s == last) || (thermo_every > 0 && s % thermo_every == 0);
-    CK(cudaGraphLaunch(c->step_exec[out ? 1 : 0], c->stream));
+  long long s = step0 + 1;
+  int replays = 0;
+  while (s <= last) {
+    const long long s_end = (last - s + 1) > chunk ? s + chunk - 1 : last;
+    // A list that outgrows its capacity during a chunk is recovered by
+    // replaying the chunk from this snapshot with a larger list, starting
+    // with a forced rebuild (the reference instead stops with "Neighbor list
+    // overflow, boost neigh_modify one", src/neigh_half_bin.cpp:414-415).
+    int rc = snapshot(c, true);
+    if (rc) return rc;
+    for (long long t = s; t <= s_end; t++) {
+      const bool out = (t == last) || (thermo_every > 0 && t % thermo_every == 0);
+      const int g = out ? 1 : 0;
+      if (c->timing) {
+        const size_t base = (size_t)(t - s) * (MD_NPHASE + 1);
+        for (int k = 0; k <= MD_NPHASE; k++)
+          CK(cudaGraphExecEventRecordNodeSetEvent(c->step_exec[g], c->ev_nodes[g][k],
+                                                  c->ev_pool[base + k]));
+      }
+      CK(cudaGraphLaunch(c->step_exec[g], c->stream));
+      c->launches += c->step_kernels[g];
+    }
+    rc = read_status(c);
+    if (rc) return rc;
+    if (c->status_host[ST_LOST]) return status_errors(c);
+    if (c->status_host[ST_OVERFLOW]) {
+      if (c->one_user > 0 || ++replays > 4) return status_errors(c);
+      const int need = c->status_host[ST_MAXNEIGH];
+      int cap = (int)(need * 1.25) + 32;
+      if (cap < c->capacity * 3 / 2) cap = c->capacity * 3 / 2;
+      rc = grow_list(c, (cap + 7) & ~7, false);
+      if (!rc) rc = snapshot(c, false);
+      if (!rc) rc = ensure_graphs(c, dtv, dtf, ftm2v);
+      if (rc) return rc;
+      int one = 1;
+      CK(cudaMemcpyAsync(c->status + ST_FORCE_BUILD, &one, sizeof(int), cudaMemcpyHostToDevice,
+                         c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      c->overflow_replays++;
+      continue;
+    }
+    if (c->one_user <= 0 && c->status_host[ST_MAXNEIGH] * 20 > c->capacity * 17) {
+      // within 15% of the capacity: widen the list for the next builds,
+      // keeping the current entries (same stride, longer slab)
+      int cap = ((int)(c->status_host[ST_MAXNEIGH] * 1.5) + 32 + 7) & ~7;
+      rc = grow_list(c, cap, true);
+      if (!rc) rc = ensure_graphs(c, dtv, dtf, ftm2v);
+      if (rc) return rc;
+    }
+    if (c->timing) {
+      for (long long t = s; t <= s_end; t++) {
+        const size_t base = (size_t)(t - s) * (MD_NPHASE + 1);
+        for (int k = 0; k < MD_NPHASE; k++) {
+          float ms = 0.f;
+          CK(cudaEventElapsedTime(&ms, c->ev_pool[base + k], c->ev_pool[base + k + 1]));
+          c->phase_ms[k] += ms;
+        }
+      }
+      c->phase_steps += s_end - s + 1;
+    }
+    s = s_end + 1;
   }
-  c->launches += 0;  // kernel launches inside graphs are counted at capture
   int rc = read_status(c);
   if (rc) return rc;
   int nr = c->status_host[ST_ROW];
@@ -883,6 +1075,25 @@ int b200_get_launch(const b200_ctx *c, int *tpa, int *block) {
 }
 
 long long b200_kernel_launches(const b200_ctx *c) { return c ? c->launches : 0; }
+
+int b200_set_timing(b200_ctx *c, int on) {
+  if (!c) return B200_ERR_ARG;
+  c->timing = on != 0;
+  invalidate_graphs(c);
+  return B200_OK;
+}
+
+int b200_get_timing(b200_ctx *c, double *phase_ms, long long *steps, int reset) {
+  if (!c) return B200_ERR_ARG;
+  if (phase_ms)
+    for (int k = 0; k < MD_NPHASE; k++) phase_ms[k] = c->phase_ms[k];
+  if (steps) *steps = c->phase_steps;
+  if (reset) {
+    for (int k = 0; k < MD_NPHASE; k++) c->phase_ms[k] = 0.0;
+    c->phase_steps = 0;
+  }
+  return B200_OK;
+}
 
 void *b200_stream(const b200_ctx *c) { return c ? (void *)c->stream : nullptr; }
 

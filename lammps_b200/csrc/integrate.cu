@@ -107,6 +107,10 @@ __global__ void k_decide(int *status, int every, int delay, int check) {
       if (rebuild && ago == (every > delay ? every : delay)) status[ST_NDANGER] += 1;
     }
   }
+  if (status[ST_FORCE_BUILD]) {  // replay after a list overflow: lists are stale
+    rebuild = 1;
+    status[ST_FORCE_BUILD] = 0;
+  }
   status[ST_MOVED] = 0;
   status[ST_REBUILD] = rebuild;
   unsigned int lo = (unsigned int)status[ST_STEP_LO] + 1u;

@@ -36,6 +36,7 @@ enum {
   ST_ROW = 8,        // thermo rows written by the device in this run
   ST_STEP_LO = 9,    // current timestep (low/high 32 bits)
   ST_STEP_HI = 10,
+  ST_FORCE_BUILD = 11,  // rebuild on the next step regardless of the schedule
   ST_COUNT = 16
 };
 

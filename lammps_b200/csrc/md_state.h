@@ -4,9 +4,20 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <vector>
 
 #include "md_common.cuh"
 #include "../../include/b200md.h"
+
+// timer phases of one step
+enum {
+  PH_INITIAL = 0,  // fix nve initial_integrate + rebuild decision
+  PH_NEIGH = 1,    // wrap, cell sort, neighbor list (when taken)
+  PH_PAIR1 = 2,    // LJ force, or EAM density + embedding
+  PH_PAIR2 = 3,    // EAM force (empty for LJ)
+  PH_FINAL = 4,    // fix nve final_integrate (+ kinetic energy, thermo row)
+  MD_NPHASE = 5
+};
 
 struct EAMDev {
   int nrho = 0, nr = 0, nfrho = 0, nrhor = 0, nz2r = 0;
@@ -76,6 +87,15 @@ struct b200_ctx {
   int capacity = 0;     // entries per atom
   long long nlist_alloc = 0;
 
+  // run-chunk snapshot for overflow replay (x4, v, f, xhold planes + ids)
+  double4 *snap_x4 = nullptr, *snap_xhold = nullptr;
+  double *snap_v = nullptr, *snap_f = nullptr;
+  int *snap_orig = nullptr, *snap_image = nullptr, *snap_cell = nullptr;
+  float4 *snap_xr = nullptr;
+  int *snap_status = nullptr;
+  int snap_alloc = 0;
+  int overflow_replays = 0;
+
   // reductions and status
   double *partial = nullptr;     // per-block partial sums
   int partial_blocks = 0;
@@ -92,9 +112,21 @@ struct b200_ctx {
 
   // CUDA graph of one MD step (captured lazily by b200_run)
   cudaGraphExec_t step_exec[2] = {nullptr, nullptr};  // [0] no output, [1] output
+  cudaGraph_t step_graph[2] = {nullptr, nullptr};
+  int step_kernels[2] = {0, 0};                         // kernel nodes per graph
   bool graph_valid = false;
   double graph_dt = 0, graph_ftm2v = 0;
   int graph_tpa = 0;
+  bool graph_timing = false;
+
+  // phase timers (Timer categories of the reference, src/timer.h:19-20):
+  // event-record nodes at the phase boundaries of every step graph
+  bool timing = false;
+  cudaEvent_t ph_event[MD_NPHASE + 1] = {};           // placeholders used at capture
+  std::vector<cudaGraphNode_t> ev_nodes[2];            // event-record nodes per graph
+  std::vector<cudaEvent_t> ev_pool;                    // per-step events of a chunk
+  double phase_ms[MD_NPHASE] = {0};
+  long long phase_steps = 0;
 };
 
 // ---- launchers (neigh.cu) -------------------------------------------------
@@ -105,7 +137,9 @@ cudaError_t md_half_list(b200_ctx *c, int *d_num, int *d_jowner, int *d_jimage, 
                          long long *total);
 // ---- pair kernels (pair_lj.cu, pair_eam.cu) --------------------------------
 cudaError_t md_lj_compute(b200_ctx *c, bool ev, bool atom_ev, double *eatom, double *vatom);
-cudaError_t md_eam_compute(b200_ctx *c, bool ev, bool atom_ev, double *eatom, double *vatom);
+// `mid`, when given, is recorded between the density and the force kernel
+cudaError_t md_eam_compute(b200_ctx *c, bool ev, bool atom_ev, double *eatom, double *vatom,
+                           cudaEvent_t mid = nullptr);
 // ---- integration (integrate.cu) --------------------------------------------
 cudaError_t md_nve_initial(b200_ctx *c, double dtv, double dtf);
 cudaError_t md_nve_final(b200_ctx *c, double dtf, bool ke);

@@ -311,29 +311,32 @@ __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__r
 }
 
 template <int TPA, bool EV, bool ATOM>
-void launch_t(b200_ctx *c, const EamArgs &a) {
+void launch_t(b200_ctx *c, const EamArgs &a, cudaEvent_t mid) {
   const int B = 128;
   const int grid = md_blocks((long long)a.n * TPA, B);
   if (c->prec == B200_PREC_MIXED) {
     k_eam_rho<TPA, EV, ATOM, true><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
+    if (mid) cudaEventRecord(mid, c->stream);
     k_eam_force<TPA, EV, ATOM, true><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
   } else {
     k_eam_rho<TPA, EV, ATOM, false><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
+    if (mid) cudaEventRecord(mid, c->stream);
     k_eam_force<TPA, EV, ATOM, false><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
   }
   c->launches += 2;
 }
 
 template <int TPA>
-void launch_tpa(b200_ctx *c, const EamArgs &a, bool ev, bool atom) {
-  if (!ev) launch_t<TPA, false, false>(c, a);
-  else if (!atom) launch_t<TPA, true, false>(c, a);
-  else launch_t<TPA, true, true>(c, a);
+void launch_tpa(b200_ctx *c, const EamArgs &a, bool ev, bool atom, cudaEvent_t mid) {
+  if (!ev) launch_t<TPA, false, false>(c, a, mid);
+  else if (!atom) launch_t<TPA, true, false>(c, a, mid);
+  else launch_t<TPA, true, true>(c, a, mid);
 }
 
 }  // namespace
 
-cudaError_t md_eam_compute(b200_ctx *c, bool ev, bool atom_ev, double *eatom, double *vatom) {
+cudaError_t md_eam_compute(b200_ctx *c, bool ev, bool atom_ev, double *eatom, double *vatom,
+                           cudaEvent_t mid) {
   EamArgs a;
   a.n = c->n;
   a.stride = c->stride;
@@ -369,10 +372,10 @@ cudaError_t md_eam_compute(b200_ctx *c, bool ev, bool atom_ev, double *eatom, do
   a.eatom = eatom;
   a.vatom = vatom;
   switch (c->tpa) {
-    case 1: launch_tpa<1>(c, a, ev, atom_ev); break;
-    case 2: launch_tpa<2>(c, a, ev, atom_ev); break;
-    case 4: launch_tpa<4>(c, a, ev, atom_ev); break;
-    default: launch_tpa<8>(c, a, ev, atom_ev); break;
+    case 1: launch_tpa<1>(c, a, ev, atom_ev, mid); break;
+    case 2: launch_tpa<2>(c, a, ev, atom_ev, mid); break;
+    case 4: launch_tpa<4>(c, a, ev, atom_ev, mid); break;
+    default: launch_tpa<8>(c, a, ev, atom_ev, mid); break;
   }
   return cudaGetLastError();
 }

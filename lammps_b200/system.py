@@ -220,6 +220,17 @@ class System:
         self._ck(self._L.b200_get_rho_fp(self._h, _abi.dptr(rho), _abi.dptr(fp)))
         return rho, fp
 
+    PHASES = ("initial", "neigh", "pair1", "pair2", "final")
+
+    def set_timing(self, on=True):
+        self._ck(self._L.b200_set_timing(self._h, int(on)))
+
+    def timing(self, reset=False):
+        ms = np.zeros(5)
+        steps = C.c_longlong()
+        self._ck(self._L.b200_get_timing(self._h, _abi.dptr(ms), C.byref(steps), int(reset)))
+        return dict(zip(self.PHASES, ms.tolist()), steps=steps.value)
+
     @property
     def kernel_launches(self):
         return self._L.b200_kernel_launches(self._h)
