@@ -209,6 +209,29 @@ def e2e_run(sysm, x_pin, v_pin, K):
     return (t1 - t0) * 1e3, h2d, d2h
 
 
+def mixed_error(make):
+    """Norm-wise relative force error of the mixed form against the FP64
+    form on the same positions (taken after 100 FP64 steps, off-lattice)."""
+    s64 = make("fp64")
+    s64.setup()
+    s64.run(MD_STEPS)
+    st = s64.download()
+    s64.neigh_build()
+    f64 = s64.compute(1, 1)
+    F64 = s64.download()["f"]
+    s64.close()
+    smx = make("mixed")
+    smx.set_atoms(st["x"], None, st["v"])
+    smx.neigh_build()
+    fmx = smx.compute(1, 1)
+    Fmx = smx.download()["f"]
+    smx.close()
+    return {"force": float(np.linalg.norm(Fmx - F64) / np.linalg.norm(F64)),
+            "energy": abs(fmx["eng"] - f64["eng"]) / abs(f64["eng"]),
+            "virial_diag": float(np.max(np.abs(fmx["virial"][:3] - f64["virial"][:3]) /
+                                        np.abs(f64["virial"][:3])))}
+
+
 def cpu_reference(setfl, x, v, hi, seconds=10.0, threads=None):
     """The oracle port (reference CPU algorithm) on the host cores."""
     import oracle
@@ -279,10 +302,17 @@ def profile_case(args):
         s = make_lj(prec, x, v, hi)
     else:
         raise SystemExit(f"unknown case {args.case}")
+    if args.eager:
+        s.set_graphs(False)
     total, per = time_form(s, torch, flush, args.steps, max(args.warmup, 1))
+    s.set_timing(True)
+    ext = torch.cuda.ExternalStream(s.stream)
+    device_time_run(s, torch, ext, flush, MD_STEPS)
+    ph = s.timing(reset=True)
     print(json.dumps({"case": args.case, "atoms": s.n, "steps": args.steps,
                       "matom_steps_per_s": s.n * MD_STEPS * args.steps / (total * 1e3),
-                      "launch": s.launch()}))
+                      "launch": s.launch(), "neigh": s.neigh_stats(),
+                      "phases_ms_per_md_step": {k: ph[k] / max(ph["steps"], 1) for k in s.PHASES}}))
     s.close()
 
 
@@ -294,6 +324,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip the FP64 and 4M-atom LJ lines")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--eager", action="store_true",
+                    help="with --case: launch kernels one by one (for profilers)")
     ap.add_argument("--case", default=None,
                     help="profile one form only: eam32k-mixed, eam32k-fp64, lj4m-mixed, lj4m-fp64")
     args = ap.parse_args()
@@ -413,6 +445,12 @@ def main():
         f_ms = lj["mixed_phases_ms_per_step"]["pair1"]
         lj["force_kernel_gbs"] = 48.0 * len(x4) / (f_ms * 1e-3) / 1e9
         extras["lj_4M"] = lj
+
+    if not args.no_extras:
+        extras["mixed_force_error"] = {
+            "eam_32k": mixed_error(lambda prec: make_eam32k(prec, setfl, x, v, hi)),
+            "lj_4M": mixed_error(lambda prec: make_lj(prec, x4, v4, hi4)),
+            "metric": "||F_mixed - F_fp64|| / ||F_fp64|| over all atoms, after 100 steps"}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:

@@ -179,6 +179,11 @@ int b200_get_launch(const b200_ctx *ctx, int *threads_per_atom, int *block_size)
      4 fix nve final half-step (+ kinetic energy and thermo row on output steps)
    b200_get_timing returns milliseconds summed over the timed steps. */
 int b200_set_timing(b200_ctx *ctx, int on);
+/* on = 1 (default): b200_run replays one CUDA graph per step, the rebuild
+   held in a device-conditional IF node.  on = 0: the same kernels launched
+   one by one with the rebuild decision read back each step (for profilers,
+   which cannot look inside graphs with conditional nodes). */
+int b200_set_graphs(b200_ctx *ctx, int on);
 int b200_get_timing(b200_ctx *ctx, double phase_ms[5], long long *steps, int reset);
 /* Kernel launches issued by the context since creation (for accounting);
    kernels replayed inside step graphs are counted per replay. */

@@ -52,6 +52,7 @@ SIGNATURES = {
     "b200_get_launch": (C.c_int, [_vp, _ip, _ip]),
     "b200_kernel_launches": (C.c_longlong, [_vp]),
     "b200_set_timing": (C.c_int, [_vp, C.c_int]),
+    "b200_set_graphs": (C.c_int, [_vp, C.c_int]),
     "b200_get_timing": (C.c_int, [_vp, _dp, C.POINTER(C.c_longlong), C.c_int]),
     "b200_stream": (_vp, [_vp]),
 }

@@ -228,6 +228,7 @@ int alloc_cells(b200_ctx *c) {
 }
 
 int alloc_list(b200_ctx *c, int capacity) {
+  capacity = (capacity + 3) & ~3;  // whole int4 slabs
   long long need = (long long)capacity * c->stride;
   if (capacity != c->capacity) invalidate_graphs(c);  // capacity is a kernel argument
   if (need > c->nlist_alloc) {
@@ -330,52 +331,124 @@ int autotune(b200_ctx *c) {
   return B200_OK;
 }
 
-int capture_step(b200_ctx *c, bool out, double dtv, double dtf, int slot) {
-  // One MD step (Verlet::run body, src/verlet.cpp:223-308) as a CUDA graph.
-  // With timing on, event-record nodes mark the phase boundaries; their
-  // events are swapped per replay so every step's phases can be read back.
-  cudaGraph_t g = nullptr;
-  const bool tm = c->timing;
-  const long long launches0 = c->launches;
-  CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-  cudaError_t e = cudaSuccess;
-  if (tm) e = cudaEventRecord(c->ph_event[0], c->stream);
-  if (e == cudaSuccess) e = md_nve_initial(c, dtv, dtf);
-  if (e == cudaSuccess) e = md_decide(c);
-  if (e == cudaSuccess && tm) e = cudaEventRecord(c->ph_event[1], c->stream);
-  if (e == cudaSuccess) e = md_rebuild(c, c->status + ST_REBUILD);
-  if (e == cudaSuccess && tm) e = cudaEventRecord(c->ph_event[2], c->stream);
-  if (e == cudaSuccess) {
-    if (c->pstyle == B200_PAIR_LJ_CUT) {
-      e = md_lj_compute(c, out, false, nullptr, nullptr);
-      if (e == cudaSuccess && tm) e = cudaEventRecord(c->ph_event[3], c->stream);
-    } else {
-      e = md_eam_compute(c, out, false, nullptr, nullptr, tm ? c->ph_event[3] : nullptr);
-    }
-  }
-  if (e == cudaSuccess && tm) e = cudaEventRecord(c->ph_event[4], c->stream);
-  if (e == cudaSuccess) e = md_nve_final(c, dtf, out);
-  if (e == cudaSuccess && out) e = md_record_row(c);
-  if (e == cudaSuccess && tm) e = cudaEventRecord(c->ph_event[5], c->stream);
-  cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
-  c->launches = launches0;
-  if (e != cudaSuccess || e2 != cudaSuccess) {
-    if (g) cudaGraphDestroy(g);
-    return set_err(c, B200_ERR_CUDA, "graph capture: %s / %s", cudaGetErrorString(e),
-                   cudaGetErrorString(e2));
-  }
-  // kernel nodes (for launch accounting) and event-record nodes in capture order
+int count_kernels(b200_ctx *c, cudaGraph_t g, int *kernels, std::vector<cudaGraphNode_t> *events) {
   size_t nn = 0;
   CK(cudaGraphGetNodes(g, nullptr, &nn));
   std::vector<cudaGraphNode_t> nodes(nn);
   CK(cudaGraphGetNodes(g, nodes.data(), &nn));
-  int kernels = 0;
-  c->ev_nodes[slot].clear();
+  *kernels = 0;
   for (auto nd : nodes) {
     cudaGraphNodeType t;
-    CK(cudaGraphNodeGetType(nd, &t));
-    if (t == cudaGraphNodeTypeKernel) kernels++;
-    if (t == cudaGraphNodeTypeEventRecord) c->ev_nodes[slot].push_back(nd);
+    // this runtime reports the conditional node's type as an error: such a
+    // node is neither a kernel nor an event record, so it is skipped
+    if (cudaGraphNodeGetType(nd, &t) != cudaSuccess) {
+      (void)cudaGetLastError();
+      continue;
+    }
+    if (t == cudaGraphNodeTypeKernel) (*kernels)++;
+    if (events && t == cudaGraphNodeTypeEventRecord) events->push_back(nd);
+  }
+  return B200_OK;
+}
+
+int capture_step(b200_ctx *c, bool out, double dtv, double dtf, int slot) {
+  // One MD step (Verlet::run body, src/verlet.cpp:223-308) as a CUDA graph:
+  //   [nve initial, decide] -> IF(rebuild){wrap, sort, list} -> [pair, nve final, row]
+  // The decide kernel sets the IF node's condition on the device, so a step
+  // without a rebuild launches none of the rebuild kernels.  With timing on,
+  // event-record nodes mark the phase boundaries; their events are swapped
+  // per replay so every step's phases can be read back.
+  const bool tm = c->timing;
+  const long long launches0 = c->launches;
+  const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
+  cudaGraph_t g = nullptr;
+  CK(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle cond;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault);
+  // part 1
+  if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(c->stream, g, nullptr, nullptr, 0, mode);
+  if (e == cudaSuccess) {
+    cudaError_t ek = cudaSuccess;
+    if (tm) ek = cudaEventRecordWithFlags(c->ph_event[0], c->stream, cudaEventRecordExternal);
+    if (ek == cudaSuccess) ek = md_nve_initial(c, dtv, dtf);
+    if (ek == cudaSuccess) ek = md_decide(c, cond);
+    if (ek == cudaSuccess && tm)
+      ek = cudaEventRecordWithFlags(c->ph_event[1], c->stream, cudaEventRecordExternal);
+    std::vector<cudaGraphNode_t> tail;
+    if (ek == cudaSuccess) {
+      cudaStreamCaptureStatus st;
+      const cudaGraphNode_t *deps = nullptr;
+      size_t nd = 0;
+      ek = cudaStreamGetCaptureInfo(c->stream, &st, nullptr, nullptr, &deps, &nd);
+      if (ek == cudaSuccess) tail.assign(deps, deps + nd);
+    }
+    cudaGraph_t gout = nullptr;
+    e = cudaStreamEndCapture(c->stream, &gout);
+    if (e == cudaSuccess) e = ek;
+    // IF node holding the rebuild
+    cudaGraphNode_t cnode = nullptr;
+    cudaGraph_t body = nullptr;
+    if (e == cudaSuccess) {
+      cudaGraphNodeParams cp = {};
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = cond;
+      cp.conditional.type = cudaGraphCondTypeIf;
+      cp.conditional.size = 1;
+      e = cudaGraphAddNode(&cnode, g, tail.data(), tail.size(), &cp);
+      if (e == cudaSuccess) body = cp.conditional.phGraph_out[0];
+    }
+    if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(c->stream, body, nullptr, nullptr, 0, mode);
+    if (e == cudaSuccess) {
+      cudaError_t ek2 = md_rebuild(c, nullptr);
+      cudaGraph_t bout = nullptr;
+      e = cudaStreamEndCapture(c->stream, &bout);
+      if (e == cudaSuccess) e = ek2;
+    }
+    // part 2, after the IF node
+    if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(c->stream, g, &cnode, nullptr, 1, mode);
+    if (e == cudaSuccess) {
+      cudaError_t ek3 = cudaSuccess;
+      if (tm) ek3 = cudaEventRecordWithFlags(c->ph_event[2], c->stream, cudaEventRecordExternal);
+      if (ek3 == cudaSuccess) {
+        if (c->pstyle == B200_PAIR_LJ_CUT) {
+          ek3 = md_lj_compute(c, out, false, nullptr, nullptr);
+          if (ek3 == cudaSuccess && tm)
+            ek3 = cudaEventRecordWithFlags(c->ph_event[3], c->stream, cudaEventRecordExternal);
+        } else {
+          ek3 = md_eam_compute(c, out, false, nullptr, nullptr, tm ? c->ph_event[3] : nullptr);
+        }
+      }
+      if (ek3 == cudaSuccess && tm)
+        ek3 = cudaEventRecordWithFlags(c->ph_event[4], c->stream, cudaEventRecordExternal);
+      if (ek3 == cudaSuccess) ek3 = md_nve_final(c, dtf, out);
+      if (ek3 == cudaSuccess && out) ek3 = md_record_row(c);
+      if (ek3 == cudaSuccess && tm)
+        ek3 = cudaEventRecordWithFlags(c->ph_event[5], c->stream, cudaEventRecordExternal);
+      cudaGraph_t gout2 = nullptr;
+      e = cudaStreamEndCapture(c->stream, &gout2);
+      if (e == cudaSuccess) e = ek3;
+    }
+    if (e == cudaSuccess) {
+      int bk = 0;
+      int rc = count_kernels(c, body, &bk, nullptr);
+      if (rc) {
+        cudaGraphDestroy(g);
+        return rc;
+      }
+      c->rebuild_kernels = bk;
+    }
+  }
+  c->launches = launches0;
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return set_err(c, B200_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+  }
+  int kernels = 0;
+  c->ev_nodes[slot].clear();
+  int rc = count_kernels(c, g, &kernels, &c->ev_nodes[slot]);
+  if (rc) {
+    cudaGraphDestroy(g);
+    return rc;
   }
   if (tm && c->ev_nodes[slot].size() != MD_NPHASE + 1) {
     cudaGraphDestroy(g);
@@ -392,7 +465,37 @@ int capture_step(b200_ctx *c, bool out, double dtv, double dtf, int slot) {
   return B200_OK;
 }
 
+// The same step as the graph, launched kernel by kernel; the rebuild
+// decision is read back to the host (one synchronisation per step).  Used
+// for profiling (tools cannot look inside graphs with conditional nodes) and
+// as a path without graphs.  `ev`, when given, receives the phase events.
+int eager_step(b200_ctx *c, bool out, double dtv, double dtf, cudaEvent_t *ev) {
+  if (ev) CK(cudaEventRecord(ev[0], c->stream));
+  CK(md_nve_initial(c, dtv, dtf));
+  CK(md_decide(c, 0));
+  if (ev) CK(cudaEventRecord(ev[1], c->stream));
+  int rebuild = 0;
+  CK(cudaMemcpyAsync(&c->status_host[ST_REBUILD], c->status + ST_REBUILD, sizeof(int),
+                     cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  rebuild = c->status_host[ST_REBUILD];
+  if (rebuild) CK(md_rebuild(c, nullptr));
+  if (ev) CK(cudaEventRecord(ev[2], c->stream));
+  if (c->pstyle == B200_PAIR_LJ_CUT) {
+    CK(md_lj_compute(c, out, false, nullptr, nullptr));
+    if (ev) CK(cudaEventRecord(ev[3], c->stream));
+  } else {
+    CK(md_eam_compute(c, out, false, nullptr, nullptr, ev ? ev[3] : nullptr));
+  }
+  if (ev) CK(cudaEventRecord(ev[4], c->stream));
+  CK(md_nve_final(c, dtf, out));
+  if (out) CK(md_record_row(c));
+  if (ev) CK(cudaEventRecord(ev[5], c->stream));
+  return B200_OK;
+}
+
 int ensure_graphs(b200_ctx *c, double dtv, double dtf, double ftm2v) {
+  if (!c->use_graphs) return B200_OK;
   if (c->graph_valid) return B200_OK;
   int rc = capture_step(c, false, dtv, dtf, 0);
   if (!rc) rc = capture_step(c, true, dtv, dtf, 1);
@@ -408,6 +511,7 @@ int ensure_graphs(b200_ctx *c, double dtv, double dtf, double ftm2v) {
 // Larger neighbor-list capacity.  keep = true copies the current entries
 // (entry k of atom i sits at k*stride + i, so the old list is a prefix).
 int grow_list(b200_ctx *c, int capacity, bool keep) {
+  capacity = (capacity + 3) & ~3;  // whole int4 slabs
   if (capacity <= c->capacity) return B200_OK;
   long long need = (long long)capacity * c->stride;
   if (need > c->nlist_alloc) {
@@ -919,11 +1023,17 @@ int b200_run(b200_ctx *c, int nsteps, double dt, double ftm2v, int thermo_every,
     // overflow, boost neigh_modify one", src/neigh_half_bin.cpp:414-415).
     int rc = snapshot(c, true);
     if (rc) return rc;
+    const int ncalls0 = c->status_host[ST_NCALLS];
     for (long long t = s; t <= s_end; t++) {
       const bool out = (t == last) || (thermo_every > 0 && t % thermo_every == 0);
       const int g = out ? 1 : 0;
+      const size_t base = (size_t)(t - s) * (MD_NPHASE + 1);
+      if (!c->use_graphs) {
+        rc = eager_step(c, out, dtv, dtf, c->timing ? &c->ev_pool[base] : nullptr);
+        if (rc) return rc;
+        continue;
+      }
       if (c->timing) {
-        const size_t base = (size_t)(t - s) * (MD_NPHASE + 1);
         for (int k = 0; k <= MD_NPHASE; k++)
           CK(cudaGraphExecEventRecordNodeSetEvent(c->step_exec[g], c->ev_nodes[g][k],
                                                   c->ev_pool[base + k]));
@@ -933,6 +1043,9 @@ int b200_run(b200_ctx *c, int nsteps, double dt, double ftm2v, int thermo_every,
     }
     rc = read_status(c);
     if (rc) return rc;
+    // kernels of the rebuild body ran once per build taken in this chunk
+    if (c->use_graphs)
+      c->launches += (long long)c->rebuild_kernels * (c->status_host[ST_NCALLS] - ncalls0);
     if (c->status_host[ST_LOST]) return status_errors(c);
     if (c->status_host[ST_OVERFLOW]) {
       if (c->one_user > 0 || ++replays > 4) return status_errors(c);
@@ -1079,6 +1192,13 @@ long long b200_kernel_launches(const b200_ctx *c) { return c ? c->launches : 0; 
 int b200_set_timing(b200_ctx *c, int on) {
   if (!c) return B200_ERR_ARG;
   c->timing = on != 0;
+  invalidate_graphs(c);
+  return B200_OK;
+}
+
+int b200_set_graphs(b200_ctx *c, int on) {
+  if (!c) return B200_ERR_ARG;
+  c->use_graphs = on != 0;
   invalidate_graphs(c);
   return B200_OK;
 }

@@ -6,9 +6,9 @@
 //   f[3][n]    double SoA                     -- forces (owner-summed; no ghosts)
 //   xr[i]      float4 (cell-relative x,y,z, type bits) -- mixed precision only
 //   cell[i]    packed cell coordinates cx | cy<<10 | cz<<20 of the last build
-//   nlist      ELL neighbor list, entry k of atom i at nlist[k*stride + i]:
-//              bits 0..26 = neighbor atom index, bits 27..31 = cell offset
-//              code (dcx+1) + 3(dcy+1) + 9(dcz+1) of the neighbor's cell.
+//   nlist      neighbor list in int4 slabs (md_slab): bits 0..25 = neighbor
+//              atom index, bits 26..31 = offset of the neighbor's cell from
+//              the atom's cell, two bits per dimension (d+1 for d = -1,0,1).
 // Periodic images are never stored: a neighbor in a wrapped cell is the owner
 // atom plus the box shift implied by the offset code, so the reference's
 // ghost atoms, forward_comm and reverse_comm disappear.
@@ -17,7 +17,7 @@
 #include <stdint.h>
 
 #define MD_MAXTYPES 8
-#define MD_JBITS 27
+#define MD_JBITS 26
 #define MD_JMASK ((1u << MD_JBITS) - 1u)
 #define MD_MAX_ATOMS ((int)MD_JMASK)
 #define MD_CELLBITS 10
@@ -66,6 +66,26 @@ __host__ __device__ inline void md_cell_unpack(int c, int &cx, int &cy, int &cz)
   cz = c >> (2 * MD_CELLBITS);
 }
 
+// neighbor-cell offset code of a list entry: (dx+1) | (dy+1)<<2 | (dz+1)<<4
+__host__ __device__ inline int md_code(int dx, int dy, int dz) {
+  return (dx + 1) | ((dy + 1) << 2) | ((dz + 1) << 4);
+}
+#define MD_CODE_SELF 21  // md_code(0, 0, 0)
+__host__ __device__ inline void md_entry(unsigned int e, int &j, int &dx, int &dy, int &dz) {
+  j = (int)(e & MD_JMASK);
+  dx = (int)((e >> MD_JBITS) & 3u) - 1;
+  dy = (int)((e >> (MD_JBITS + 2)) & 3u) - 1;
+  dz = (int)(e >> (MD_JBITS + 4)) - 1;
+}
+
+// Slab layout of the neighbor list: entry k of atom i is at
+//   nlist[((k >> 2) * stride + i) * 4 + (k & 3)]
+// so that one int4 load returns four consecutive entries of an atom and the
+// 32 atoms of a warp read 512 contiguous bytes per slab.
+__host__ __device__ inline size_t md_slab(int k, int i, int stride) {
+  return ((size_t)(k >> 2) * stride + i) * 4 + (k & 3);
+}
+
 // image flags packed as LAMMPS imageint: 10 bits per dimension, offset 512
 // (src/lmptype.h IMGMAX/IMGBITS)
 #define MD_IMGMAX 512
@@ -73,6 +93,20 @@ __host__ __device__ inline void md_cell_unpack(int c, int &cx, int &cy, int &cz)
 __host__ __device__ inline int md_img_pack(int ix, int iy, int iz) {
   return ((iz + MD_IMGMAX) & MD_IMGMASK) << 20 | ((iy + MD_IMGMAX) & MD_IMGMASK) << 10 |
          ((ix + MD_IMGMAX) & MD_IMGMASK);
+}
+
+// 1/x in FP64: Newton's method on f(y) = 1/y - x, i.e. the iteration
+// y <- y + y (1 - x y), started from the hardware reciprocal approximation
+// (rcp.approx.ftz.f64) and applied twice.  For the normal, positive x used
+// here the result is within two ulp of the correctly rounded quotient; the
+// FP64 parity tests bound its effect on forces.
+__device__ __forceinline__ double rcp_nr(double x) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  double e = fma(-x, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-x, y, 1.0);
+  return fma(y, e, y);
 }
 
 // FP64 helpers that keep a*b+c rounded twice, as the reference's x86-64
@@ -137,12 +171,21 @@ __device__ __forceinline__ void block_partials_finish(double (&v)[NV], double *s
   __syncthreads();
   if (last) {
     __threadfence();
-    // threads of the last block sum one component each, in block order
-    for (int k = threadIdx.x; k < NV; k += blockDim.x) {
-      double s = 0.0;
-      for (unsigned int b = 0; b < gridDim.x; b++) s += __ldcg(&partial[(size_t)b * NV + k]);
-      out[k] = accumulate ? out[k] + s : s;
+    // every thread of the last block sums a fixed strided subset of the
+    // block partials, then the block tree-reduces them: a fixed order, so
+    // the result is reproducible run to run
+    double s[NV];
+#pragma unroll
+    for (int k = 0; k < NV; k++) s[k] = 0.0;
+    for (unsigned int b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+#pragma unroll
+      for (int k = 0; k < NV; k++) s[k] += __ldcg(&partial[(size_t)b * NV + k]);
+    __syncthreads();
+    block_sum<NV>(s, smem);
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int k = 0; k < NV; k++) out[k] = accumulate ? out[k] + s[k] : s[k];
+      *counter = 0u;
     }
-    if (threadIdx.x == 0) *counter = 0u;
   }
 }

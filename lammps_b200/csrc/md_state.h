@@ -114,10 +114,12 @@ struct b200_ctx {
   cudaGraphExec_t step_exec[2] = {nullptr, nullptr};  // [0] no output, [1] output
   cudaGraph_t step_graph[2] = {nullptr, nullptr};
   int step_kernels[2] = {0, 0};                         // kernel nodes per graph
+  int rebuild_kernels = 0;                              // kernel nodes of the rebuild body
   bool graph_valid = false;
   double graph_dt = 0, graph_ftm2v = 0;
   int graph_tpa = 0;
   bool graph_timing = false;
+  bool use_graphs = true;   // false: eager launches, host-side rebuild decision
 
   // phase timers (Timer categories of the reference, src/timer.h:19-20):
   // event-record nodes at the phase boundaries of every step graph
@@ -144,7 +146,8 @@ cudaError_t md_eam_compute(b200_ctx *c, bool ev, bool atom_ev, double *eatom, do
 cudaError_t md_nve_initial(b200_ctx *c, double dtv, double dtf);
 cudaError_t md_nve_final(b200_ctx *c, double dtf, bool ke);
 cudaError_t md_ke(b200_ctx *c);
-cudaError_t md_decide(b200_ctx *c);
+// `cond` (0 outside graphs) receives the rebuild decision as an IF condition
+cudaError_t md_decide(b200_ctx *c, cudaGraphConditionalHandle cond);
 cudaError_t md_record_row(b200_ctx *c);
 cudaError_t md_zero_ev(b200_ctx *c);
 

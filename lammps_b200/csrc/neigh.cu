@@ -226,60 +226,243 @@ __global__ void k_copyback(int n, int stride, const double4 *__restrict__ x4b,
   image[k] = imageb[k];
 }
 
-// Full neighbor list, one thread per atom.  Candidates come from the 27
-// cells around the atom's cell (cell edge >= rc + skin); a wrapped cell
-// carries the box shift of its periodic image.
-__global__ void __launch_bounds__(128) k_neigh_full(
+// Full neighbor list with shared-memory staging of neighbor-cell tiles.
+// A CTA owns kTileCells consecutive cells along x; the 3 x 3 x (kTileCells+2)
+// block of cells around them is staged in shared memory as 9 contiguous
+// ranges of the cell-sorted atom arrays (positions as FP32 offsets from the
+// CTA's reference point, with the periodic image already applied).  Each
+// thread takes one atom of the owned cells and scans its 27 neighbor cells
+// from shared memory.  The FP32 distance decides every pair whose rsq lies
+// outside a relative band of 1e-5 around (rc+skin)^2; pairs inside the band
+// are decided by the reference's FP64 arithmetic on the global FP64
+// positions, so the list is bit-identical to the FP64 criterion.
+constexpr int kTileCells = 4;
+constexpr int kStageCap = 2048;
+constexpr int kStageCells = 3 * 3 * (kTileCells + 2);
+constexpr int kNeighThreads = 32 * kTileCells;  // one warp per owned cell
+
+// The last four list entries of a thread rotate through an int4 register
+// buffer; every fourth append stores the slab with one 16-byte write.
+__device__ __forceinline__ void append_entry(int *__restrict__ nlist, int stride, int i,
+                                             int &count, int capacity, int e, int4 &buf) {
+  buf.x = buf.y;
+  buf.y = buf.z;
+  buf.z = buf.w;
+  buf.w = e;
+  if ((count & 3) == 3 && count < capacity)
+    reinterpret_cast<int4 *>(nlist)[(size_t)(count >> 2) * stride + i] = buf;
+  count++;
+}
+
+// store the last, partly filled slab (its r entries sit at the end of buf)
+__device__ __forceinline__ void flush_entries(int *__restrict__ nlist, int stride, int i,
+                                              int count, int capacity, const int4 &buf) {
+  const int r = count & 3;
+  if (r == 0 || count - 1 >= capacity) return;
+  int4 o = make_int4(0, 0, 0, 0);
+  if (r == 1) o.x = buf.w;
+  else if (r == 2) { o.x = buf.z; o.y = buf.w; }
+  else { o.x = buf.y; o.y = buf.z; o.z = buf.w; }
+  reinterpret_cast<int4 *>(nlist)[(size_t)(count >> 2) * stride + i] = o;
+}
+
+// exact reference criterion for one candidate (FP64, no contraction)
+__device__ __forceinline__ bool exact_pair(const double4 &xi, const double4 &xj, double shx,
+                                           double shy, double shz, double cutsq) {
+  const double delx = __dsub_rn(xi.x, __dadd_rn(xj.x, shx));
+  const double dely = __dsub_rn(xi.y, __dadd_rn(xj.y, shy));
+  const double delz = __dsub_rn(xi.z, __dadd_rn(xj.z, shz));
+  return dsq3(delx, dely, delz) <= cutsq;
+}
+
+template <bool SINGLE>
+__global__ void __launch_bounds__(kNeighThreads) k_neigh_tiles(
     int n, int stride, int capacity, BoxGeom box, int ntp1, const double *__restrict__ cutneighsq_g,
-    const double4 *__restrict__ x4, const int *__restrict__ cell, const int *__restrict__ cell_start,
-    int *__restrict__ nlist, int *__restrict__ numneigh, int *__restrict__ status, const int *flag) {
+    const double4 *__restrict__ x4, const int *__restrict__ cell_start, int *__restrict__ nlist,
+    int *__restrict__ numneigh, int *__restrict__ status, const int *flag) {
   if (!rebuild_on(flag)) return;
+  __shared__ float4 sp[kStageCap];
+  __shared__ int sj[kStageCap];
+  __shared__ int s_start[kStageCells + 1];
+  __shared__ int s_src[kStageCells];
+  __shared__ double s_sh[kStageCells][3];
   __shared__ double cns[(MD_MAXTYPES + 1) * (MD_MAXTYPES + 1)];
-  for (int k = threadIdx.x; k < ntp1 * ntp1; k += blockDim.x) cns[k] = cutneighsq_g[k];
-  __syncthreads();
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  double4 xi = x4[i];
-  int ti = (int)xi.w;
-  int cx, cy, cz;
-  md_cell_unpack(cell[i], cx, cy, cz);
+  __shared__ float cns_lo[(MD_MAXTYPES + 1) * (MD_MAXTYPES + 1)];
+  __shared__ float cns_hi[(MD_MAXTYPES + 1) * (MD_MAXTYPES + 1)];
   const int ncx = box.ncell[0], ncy = box.ncell[1], ncz = box.ncell[2];
-  int count = 0;
-  for (int dz = -1; dz <= 1; dz++) {
-    int czj = cz + dz, sz = 0;
-    if (czj < 0) { czj += ncz; sz = -1; } else if (czj >= ncz) { czj -= ncz; sz = 1; }
-    double shz = sz * box.prd[2];
-    for (int dy = -1; dy <= 1; dy++) {
-      int cyj = cy + dy, sy = 0;
-      if (cyj < 0) { cyj += ncy; sy = -1; } else if (cyj >= ncy) { cyj -= ncy; sy = 1; }
-      double shy = sy * box.prd[1];
-      for (int dx = -1; dx <= 1; dx++) {
-        int cxj = cx + dx, sx = 0;
-        if (cxj < 0) { cxj += ncx; sx = -1; } else if (cxj >= ncx) { cxj -= ncx; sx = 1; }
-        double shx = sx * box.prd[0];
-        int code = (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1);
-        int cj = cxj + ncx * (cyj + ncy * czj);
-        int j0 = cell_start[cj], j1 = cell_start[cj + 1];
-        for (int j = j0; j < j1; j++) {
-          if (code == 13 && j == i) continue;
-          double4 xj = x4[j];
-          double delx = __dsub_rn(xi.x, __dadd_rn(xj.x, shx));
-          double dely = __dsub_rn(xi.y, __dadd_rn(xj.y, shy));
-          double delz = __dsub_rn(xi.z, __dadd_rn(xj.z, shz));
-          double rsq = dsq3(delx, dely, delz);
-          if (rsq <= cns[ti * ntp1 + (int)xj.w]) {
-            if (count < capacity) nlist[(size_t)count * stride + i] = j | (code << MD_JBITS);
-            count++;
-          }
-        }
+  const int tiles_x = (ncx + kTileCells - 1) / kTileCells;
+  const int bx = blockIdx.x % tiles_x;
+  const int cy = (blockIdx.x / tiles_x) % ncy;
+  const int cz = blockIdx.x / (tiles_x * ncy);
+  const int cx0 = bx * kTileCells;
+  const int ow = min(kTileCells, ncx - cx0);  // owned cells in this tile
+  for (int k = threadIdx.x; k < ntp1 * ntp1; k += blockDim.x) {
+    const double c = cutneighsq_g[k];
+    cns[k] = c;
+    cns_lo[k] = (float)(c * (1.0 - 1.0e-5));
+    cns_hi[k] = (float)(c * (1.0 + 1.0e-5));
+  }
+  // staged cells: id = sx + (kTileCells+2)*(sy + 3*sz) is global cell
+  // (cx0-1+sx, cy-1+sy, cz-1+sz), wrapped, with the shift of its image
+  if (threadIdx.x < kStageCells) {
+    const int id = threadIdx.x;
+    const int sx = id % (kTileCells + 2), sy = (id / (kTileCells + 2)) % 3,
+              sz = id / (3 * (kTileCells + 2));
+    int g = 0, ix = 0, iy = 0, iz = 0, cnt = 0;
+    if (sx <= ow + 1) {  // columns past the box edge are not neighbours of any owned cell
+      int gx = cx0 - 1 + sx, gy = cy - 1 + sy, gz = cz - 1 + sz;
+      if (gx < 0) { gx += ncx; ix = -1; } else if (gx >= ncx) { gx -= ncx; ix = 1; }
+      if (gy < 0) { gy += ncy; iy = -1; } else if (gy >= ncy) { gy -= ncy; iy = 1; }
+      if (gz < 0) { gz += ncz; iz = -1; } else if (gz >= ncz) { gz -= ncz; iz = 1; }
+      g = gx + ncx * (gy + ncy * gz);
+      cnt = cell_start[g + 1] - cell_start[g];
+    }
+    s_src[id] = g;
+    s_sh[id][0] = ix * box.prd[0];
+    s_sh[id][1] = iy * box.prd[1];
+    s_sh[id][2] = iz * box.prd[2];
+    s_start[id + 1] = cnt;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    s_start[0] = 0;
+    for (int id = 0; id < kStageCells; id++) s_start[id + 1] += s_start[id];
+  }
+  __syncthreads();
+  const bool staged = s_start[kStageCells] <= kStageCap;
+  // FP32 reference point: centre of cell (cx0, cy, cz)
+  const double rx = box.lo[0] + (cx0 + 0.5) * box.cs[0];
+  const double ry = box.lo[1] + (cy + 0.5) * box.cs[1];
+  const double rz = box.lo[2] + (cz + 0.5) * box.cs[2];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (staged) {
+    for (int id = warp; id < kStageCells; id += kNeighThreads / 32) {
+      const int g0 = cell_start[s_src[id]];
+      const int cnt = s_start[id + 1] - s_start[id];
+      const double shx = s_sh[id][0], shy = s_sh[id][1], shz = s_sh[id][2];
+      for (int t = lane; t < cnt; t += 32) {
+        const double4 p = x4[g0 + t];
+        const int o = s_start[id] + t;
+        sp[o] = make_float4((float)(__dadd_rn(p.x, shx) - rx), (float)(__dadd_rn(p.y, shy) - ry),
+                            (float)(__dadd_rn(p.z, shz) - rz), __int_as_float((int)p.w));
+        sj[o] = g0 + t;
       }
     }
   }
-  // the stored count never exceeds the capacity, so readers stay in bounds;
-  // an overflow is reported through the status word
-  numneigh[i] = count < capacity ? count : capacity;
-  atomicMax(&status[ST_MAXNEIGH], count);
-  if (count > capacity) atomicExch(&status[ST_OVERFLOW], 1);
+  __syncthreads();
+  // Warp w owns cell (cx0 + w, cy, cz); each lane takes one of its atoms.
+  // The 27 neighbour cells are 9 contiguous staged ranges (3 cells along x
+  // each), scanned 32 candidates at a time: a branch-free test phase builds
+  // a 32-bit acceptance mask per lane (broadcast shared reads), then an
+  // append phase walks the set bits in candidate order.
+  if (warp >= ow) return;
+  const int own_id = (warp + 1) + (kTileCells + 2) * (1 + 3 * 1);
+  const int cown = cx0 + warp + ncx * (cy + ncy * cz);
+  const int a0 = cell_start[cown], a1 = cell_start[cown + 1];
+  const float lo1 = SINGLE ? cns_lo[ntp1 + 1] : 0.f, hi1 = SINGLE ? cns_hi[ntp1 + 1] : 0.f;
+  const double cut1 = SINGLE ? cns[ntp1 + 1] : 0.0;
+  if (staged) {
+    const int o0 = s_start[own_id];
+    for (int base = a0; base < a1; base += 32) {
+      const int i = base + lane;
+      const bool act = i < a1;
+      const double4 xi = x4[act ? i : a0];
+      const int ti = (int)xi.w;
+      const int my_m = act ? o0 + (i - a0) : -1;
+      // an inactive lane sits far away and accepts no candidate
+      const float pix = act ? (float)(xi.x - rx) : 1.0e30f;
+      const float piy = (float)(xi.y - ry), piz = (float)(xi.z - rz);
+      int count = 0;
+      int4 buf = make_int4(0, 0, 0, 0);
+      for (int dz = -1; dz <= 1; dz++)
+        for (int dy = -1; dy <= 1; dy++) {
+          const int idL = warp + (kTileCells + 2) * ((1 + dy) + 3 * (1 + dz));  // dx = -1
+          const int r0 = s_start[idL], r1 = s_start[idL + 3];
+          const int b1 = s_start[idL + 1], b2 = s_start[idL + 2];
+          for (int cb = r0; cb < r1; cb += 32) {
+            const int nc = min(32, r1 - cb);
+            unsigned acc = 0u, band = 0u;
+            if (SINGLE && nc == 32) {
+#pragma unroll
+              for (int t = 0; t < 32; t++) {
+                const float4 pj = sp[cb + t];
+                const float ddx = pix - pj.x, ddy = piy - pj.y, ddz = piz - pj.z;
+                const float r2 = ddx * ddx + ddy * ddy + ddz * ddz;
+                acc |= (r2 <= hi1) ? (1u << t) : 0u;
+                band |= (r2 >= lo1) ? (1u << t) : 0u;
+              }
+            } else {
+              for (int t = 0; t < nc; t++) {
+                const float4 pj = sp[cb + t];
+                const float ddx = pix - pj.x, ddy = piy - pj.y, ddz = piz - pj.z;
+                const float r2 = ddx * ddx + ddy * ddy + ddz * ddz;
+                float lo = lo1, hi = hi1;
+                if (!SINGLE) {
+                  const int tt = ti * ntp1 + __float_as_int(pj.w);
+                  lo = cns_lo[tt];
+                  hi = cns_hi[tt];
+                }
+                acc |= (r2 <= hi) ? (1u << t) : 0u;
+                band |= (r2 >= lo) ? (1u << t) : 0u;
+              }
+            }
+            if (my_m >= cb && my_m < cb + nc) acc &= ~(1u << (my_m - cb));
+            band &= acc;
+            while (acc) {
+              const int t = __ffs(acc) - 1;
+              acc &= acc - 1u;
+              const int m = cb + t;
+              const int j = sj[m];
+              const int dxl = (m >= b1) + (m >= b2);  // staged column of the candidate
+              // inside the FP32 uncertainty band: the reference's FP64 test
+              if (((band >> t) & 1u) &&
+                  !exact_pair(xi, x4[j], s_sh[idL + dxl][0], s_sh[idL + dxl][1],
+                              s_sh[idL + dxl][2],
+                              SINGLE ? cut1 : cns[ti * ntp1 + __float_as_int(sp[m].w)]))
+                continue;
+              append_entry(nlist, stride, i, count, capacity,
+                           j | (md_code(dxl - 1, dy, dz) << MD_JBITS), buf);
+            }
+          }
+        }
+      if (act) {
+        flush_entries(nlist, stride, i, count, capacity, buf);
+        // the stored count never exceeds the capacity, so readers stay in
+        // bounds; an overflow is reported through the status word
+        numneigh[i] = count < capacity ? count : capacity;
+        atomicMax(&status[ST_MAXNEIGH], count);
+        if (count > capacity) atomicExch(&status[ST_OVERFLOW], 1);
+      }
+    }
+    return;
+  }
+  // fallback (a tile or a cell too crowded for shared memory): one thread
+  // per owned atom, candidates read from global memory, FP64 test
+  for (int i = a0 + lane; i < a1; i += 32) {
+    const double4 xi = x4[i];
+    const int ti = (int)xi.w;
+    int count = 0;
+    int4 buf = make_int4(0, 0, 0, 0);
+    for (int dz = -1; dz <= 1; dz++)
+      for (int dy = -1; dy <= 1; dy++)
+        for (int dx = -1; dx <= 1; dx++) {
+          const int id = (warp + 1 + dx) + (kTileCells + 2) * ((1 + dy) + 3 * (1 + dz));
+          const int codebits = md_code(dx, dy, dz) << MD_JBITS;
+          const int g = s_src[id];
+          const int j1 = cell_start[g + 1];
+          for (int j = cell_start[g]; j < j1; j++) {
+            if (codebits == (MD_CODE_SELF << MD_JBITS) && j == i) continue;
+            const double4 xj = x4[j];
+            if (exact_pair(xi, xj, s_sh[id][0], s_sh[id][1], s_sh[id][2],
+                           cns[ti * ntp1 + (int)xj.w]))
+              append_entry(nlist, stride, i, count, capacity, j | codebits, buf);
+          }
+        }
+    flush_entries(nlist, stride, i, count, capacity, buf);
+    numneigh[i] = count < capacity ? count : capacity;
+    atomicMax(&status[ST_MAXNEIGH], count);
+    if (count > capacity) atomicExch(&status[ST_OVERFLOW], 1);
+  }
 }
 
 __global__ void k_build_done(int *status, int check, const int *flag) {
@@ -336,9 +519,9 @@ __global__ void k_half(int n, int stride, BoxGeom box, HalfBins hb, const double
   long long out = WRITE ? offset[oi] : 0;
   int cnt = 0;
   for (int k = 0; k < num; k++) {
-    unsigned int e = (unsigned int)nlist[(size_t)k * stride + i];
-    int j = (int)(e & MD_JMASK), code = (int)(e >> MD_JBITS);
-    int dc[3] = {code % 3 - 1, (code / 3) % 3 - 1, code / 9 - 1};
+    unsigned int e = (unsigned int)nlist[md_slab(k, i, stride)];
+    int j, dc[3];
+    md_entry(e, j, dc[0], dc[1], dc[2]);
     int s[3];
     double g[3];
     double4 xj = x4[j];
@@ -430,8 +613,18 @@ cudaError_t md_rebuild(b200_ctx *c, const int *d_flag) {
       c->check ? c->xhold : nullptr, d_flag);
   k_copyback<<<md_blocks(n, B), B, 0, c->stream>>>(n, c->stride, c->x4b, c->x4, c->vb, c->v,
                                                    c->origb, c->orig, c->imageb, c->image, d_flag);
-  k_neigh_full<<<md_blocks(n, 128), 128, 0, c->stream>>>(
-      n, c->stride, c->capacity, c->box, c->ntypes + 1, c->cutneighsq_dev, c->x4, c->cell, c->cell_start, c->nlist, c->numneigh, c->status, d_flag);
+  {
+    const int tiles = ((c->box.ncell[0] + kTileCells - 1) / kTileCells) * c->box.ncell[1] *
+                      c->box.ncell[2];
+    if (c->ntypes == 1)
+      k_neigh_tiles<true><<<tiles, kNeighThreads, 0, c->stream>>>(
+          n, c->stride, c->capacity, c->box, c->ntypes + 1, c->cutneighsq_dev, c->x4,
+          c->cell_start, c->nlist, c->numneigh, c->status, d_flag);
+    else
+      k_neigh_tiles<false><<<tiles, kNeighThreads, 0, c->stream>>>(
+          n, c->stride, c->capacity, c->box, c->ntypes + 1, c->cutneighsq_dev, c->x4,
+          c->cell_start, c->nlist, c->numneigh, c->status, d_flag);
+  }
   k_build_done<<<1, 1, 0, c->stream>>>(c->status, c->check, d_flag);
   c->launches += 5;
   return cudaGetLastError();

@@ -15,7 +15,8 @@
 // Mixed form: FP32 tables reordered per knot as [c3 c4 c5 c6 | c0 c1 c2 -]
 // so one float4 load gives a value and one a derivative; distances from the
 // FP32 cell-relative coordinates; fp_j gathered as FP32; sums in FP64.  The
-// embedding step F(rho) stays FP64 in both forms.
+// embedding step F(rho) stays FP64 in both forms.  Each thread reads four
+// list entries with one 16-byte load and issues their gathers together.
 #include "md_state.h"
 
 namespace {
@@ -51,13 +52,10 @@ __device__ __forceinline__ double pick(const Shift3 &s, int d) {
   return d < 0 ? s.m : (d > 0 ? s.p : 0.0);
 }
 __device__ __forceinline__ void decode(unsigned int e, int &j, int &dx, int &dy, int &dz) {
-  j = (int)(e & MD_JMASK);
-  const int code = (int)(e >> MD_JBITS);
-  dz = code / 9 - 1;
-  const int rem = code - 9 * (dz + 1);
-  dy = rem / 3 - 1;
-  dx = rem - 3 * (dy + 1) - 1;
+  md_entry(e, j, dx, dy, dz);
 }
+// neighbour-cell centre offset along one dimension (d = -1, 0, +1)
+__device__ __forceinline__ float offf(int d, float cs) { return d < 0 ? -cs : (d > 0 ? cs : 0.f); }
 
 // Embedding F(rho) and F'(rho) of one atom, FP64, reference clamps.
 __device__ __forceinline__ void embed(const EamArgs &a, int itype_frho, double rho, double &fp,
@@ -98,23 +96,35 @@ __global__ void __launch_bounds__(128) k_eam_rho(EamArgs a, const double4 *__res
       const Shift3 sx = shifts(cx, a.box.ncell[0], a.box.prd[0]);
       const Shift3 sy = shifts(cy, a.box.ncell[1], a.box.prd[1]);
       const Shift3 sz = shifts(cz, a.box.ncell[2], a.box.prd[2]);
-      for (int k = lane; k < num; k += TPA) {
-        int j, dx, dy, dz;
-        decode((unsigned int)a.nlist[(size_t)k * a.stride + i], j, dx, dy, dz);
-        const double4 xj = x4[j];
-        const double delx = __dsub_rn(xi.x, __dadd_rn(xj.x, pick(sx, dx)));
-        const double dely = __dsub_rn(xi.y, __dadd_rn(xj.y, pick(sy, dy)));
-        const double delz = __dsub_rn(xi.z, __dadd_rn(xj.z, pick(sz, dz)));
-        const double rsq = dsq3(delx, dely, delz);
-        if (rsq < a.cutforcesq) {
-          double p = __dadd_rn(__dmul_rn(sqrt(rsq), a.rdr), 1.0);
-          int m = (int)p;
-          m = min(m, a.nr - 1);
-          p -= m;
-          p = fmin(p, 1.0);
-          const int tab = s_t2rhor[(int)xj.w * a.ntp1 + ti];
-          const double *c = a.rhor + ((size_t)tab * (a.nr + 1) + m) * 8;
-          rho += ((c[3] * p + c[4]) * p + c[5]) * p + c[6];
+      const int4 *nl4 = reinterpret_cast<const int4 *>(a.nlist);
+      for (int c4 = lane; 4 * c4 < num; c4 += TPA) {
+        const int4 e4 = nl4[(size_t)c4 * a.stride + i];
+        const int mm = min(4, num - 4 * c4);
+        const unsigned int ee[4] = {(unsigned int)e4.x, (unsigned int)e4.y, (unsigned int)e4.z,
+                                    (unsigned int)e4.w};
+        double4 xq[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) xq[u] = x4[u < mm ? (int)(ee[u] & MD_JMASK) : i];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          if (u >= mm) break;
+          int j, dx, dy, dz;
+          decode(ee[u], j, dx, dy, dz);
+          const double4 xj = xq[u];
+          const double delx = __dsub_rn(xi.x, __dadd_rn(xj.x, pick(sx, dx)));
+          const double dely = __dsub_rn(xi.y, __dadd_rn(xj.y, pick(sy, dy)));
+          const double delz = __dsub_rn(xi.z, __dadd_rn(xj.z, pick(sz, dz)));
+          const double rsq = dsq3(delx, dely, delz);
+          if (rsq < a.cutforcesq) {
+            double p = __dadd_rn(__dmul_rn(sqrt(rsq), a.rdr), 1.0);
+            int m = (int)p;
+            m = min(m, a.nr - 1);
+            p -= m;
+            p = fmin(p, 1.0);
+            const int tab = s_t2rhor[(int)xj.w * a.ntp1 + ti];
+            const double *c = a.rhor + ((size_t)tab * (a.nr + 1) + m) * 8;
+            rho += ((c[3] * p + c[4]) * p + c[5]) * p + c[6];
+          }
         }
       }
     } else {
@@ -122,24 +132,39 @@ __global__ void __launch_bounds__(128) k_eam_rho(EamArgs a, const double4 *__res
       ti = __float_as_int(xi.w);
       const float csx = (float)a.box.cs[0], csy = (float)a.box.cs[1], csz = (float)a.box.cs[2];
       const float cutf = (float)a.cutforcesq, rdrf = (float)a.rdr;
-      for (int k = lane; k < num; k += TPA) {
-        int j, dx, dy, dz;
-        decode((unsigned int)a.nlist[(size_t)k * a.stride + i], j, dx, dy, dz);
-        const float4 xj = xr[j];
-        const float delx = (xi.x - xj.x) - (float)dx * csx;
-        const float dely = (xi.y - xj.y) - (float)dy * csy;
-        const float delz = (xi.z - xj.z) - (float)dz * csz;
-        const float rsq = delx * delx + dely * dely + delz * delz;
-        if (rsq < cutf) {
-          float p = sqrtf(rsq) * rdrf + 1.0f;
-          int m = (int)p;
-          m = min(m, a.nr - 1);
-          p -= (float)m;
-          p = fminf(p, 1.0f);
-          const int tab = s_t2rhor[__float_as_int(xj.w) * a.ntp1 + ti];
-          const float4 c = *reinterpret_cast<const float4 *>(a.rhor_f + ((size_t)tab * (a.nr + 1) + m) * 8);
-          rho += (double)(((c.x * p + c.y) * p + c.z) * p + c.w);
+      const int4 *nl4 = reinterpret_cast<const int4 *>(a.nlist);
+      for (int c4 = lane; 4 * c4 < num; c4 += TPA) {
+        const int4 e4 = nl4[(size_t)c4 * a.stride + i];
+        const int mm = min(4, num - 4 * c4);
+        const unsigned int ee[4] = {(unsigned int)e4.x, (unsigned int)e4.y, (unsigned int)e4.z,
+                                    (unsigned int)e4.w};
+        float4 xq[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) xq[u] = xr[u < mm ? (int)(ee[u] & MD_JMASK) : i];
+        float crho = 0.f;  // FP32 slab sum, added to the FP64 density
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          if (u >= mm) break;
+          int j, dx, dy, dz;
+          decode(ee[u], j, dx, dy, dz);
+          const float4 xj = xq[u];
+          const float delx = (xi.x - xj.x) - offf(dx, csx);
+          const float dely = (xi.y - xj.y) - offf(dy, csy);
+          const float delz = (xi.z - xj.z) - offf(dz, csz);
+          const float rsq = delx * delx + dely * dely + delz * delz;
+          if (rsq < cutf) {
+            float p = sqrtf(rsq) * rdrf + 1.0f;
+            int m = (int)p;
+            m = min(m, a.nr - 1);
+            p -= (float)m;
+            p = fminf(p, 1.0f);
+            const int tab = s_t2rhor[__float_as_int(xj.w) * a.ntp1 + ti];
+            const float4 c =
+                *reinterpret_cast<const float4 *>(a.rhor_f + ((size_t)tab * (a.nr + 1) + m) * 8);
+            crho += ((c.x * p + c.y) * p + c.z) * p + c.w;
+          }
         }
+        rho += (double)crho;
       }
     }
   }
@@ -187,10 +212,26 @@ __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__r
       const Shift3 sx = shifts(cx, a.box.ncell[0], a.box.prd[0]);
       const Shift3 sy = shifts(cy, a.box.ncell[1], a.box.prd[1]);
       const Shift3 sz = shifts(cz, a.box.ncell[2], a.box.prd[2]);
-      for (int k = lane; k < num; k += TPA) {
+      const int4 *nl4 = reinterpret_cast<const int4 *>(a.nlist);
+      for (int c4 = lane; 4 * c4 < num; c4 += TPA) {
+       const int4 e4 = nl4[(size_t)c4 * a.stride + i];
+       const int mm = min(4, num - 4 * c4);
+       const unsigned int ee[4] = {(unsigned int)e4.x, (unsigned int)e4.y, (unsigned int)e4.z,
+                                   (unsigned int)e4.w};
+       double4 xq[4];
+       double fpq[4];
+#pragma unroll
+       for (int u = 0; u < 4; u++) {
+         const int jj = u < mm ? (int)(ee[u] & MD_JMASK) : i;
+         xq[u] = x4[jj];
+         fpq[u] = a.fp[jj];
+       }
+#pragma unroll
+       for (int u = 0; u < 4; u++) {
+        if (u >= mm) break;
         int j, dx, dy, dz;
-        decode((unsigned int)a.nlist[(size_t)k * a.stride + i], j, dx, dy, dz);
-        const double4 xj = x4[j];
+        decode(ee[u], j, dx, dy, dz);
+        const double4 xj = xq[u];
         const double delx = __dsub_rn(xi.x, __dadd_rn(xj.x, pick(sx, dx)));
         const double dely = __dsub_rn(xi.y, __dadd_rn(xj.y, pick(sy, dy)));
         const double delz = __dsub_rn(xi.z, __dadd_rn(xj.z, pick(sz, dz)));
@@ -210,10 +251,10 @@ __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__r
           const double *cz2 = a.z2r + ((size_t)s_t2z2r[ti * a.ntp1 + tj] * (a.nr + 1) + m) * 8;
           const double z2p = (cz2[0] * p + cz2[1]) * p + cz2[2];
           const double z2 = ((cz2[3] * p + cz2[4]) * p + cz2[5]) * p + cz2[6];
-          const double recip = 1.0 / r;
+          const double recip = rcp_nr(r);
           const double phi = z2 * recip;
           const double phip = z2p * recip - phi * recip;
-          const double psip = fpi * rhojp + a.fp[j] * rhoip + phip;
+          const double psip = fpi * rhojp + fpq[u] * rhoip + phip;
           const double fpair = -psip * recip;
           fx += delx * fpair;
           fy += dely * fpair;
@@ -229,6 +270,7 @@ __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__r
             acc[6] += dely * delz * hf;
           }
         }
+       }
       }
     } else {
       const float4 xi = xr[i];
@@ -236,13 +278,31 @@ __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__r
       const float fpi = a.fpf[i];
       const float csx = (float)a.box.cs[0], csy = (float)a.box.cs[1], csz = (float)a.box.cs[2];
       const float cutf = (float)a.cutforcesq, rdrf = (float)a.rdr;
-      for (int k = lane; k < num; k += TPA) {
+      const int4 *nl4 = reinterpret_cast<const int4 *>(a.nlist);
+      for (int c4 = lane; 4 * c4 < num; c4 += TPA) {
+       const int4 e4 = nl4[(size_t)c4 * a.stride + i];
+       const int mm = min(4, num - 4 * c4);
+       const unsigned int ee[4] = {(unsigned int)e4.x, (unsigned int)e4.y, (unsigned int)e4.z,
+                                   (unsigned int)e4.w};
+       float4 xq[4];
+       float fpq[4];
+#pragma unroll
+       for (int u = 0; u < 4; u++) {
+         const int jj = u < mm ? (int)(ee[u] & MD_JMASK) : i;
+         xq[u] = xr[jj];
+         fpq[u] = a.fpf[jj];
+       }
+       // FP32 sum of the slab's pair forces, added to the FP64 accumulator
+       float cfx = 0.f, cfy = 0.f, cfz = 0.f;
+#pragma unroll
+       for (int u = 0; u < 4; u++) {
+        if (u >= mm) break;
         int j, dx, dy, dz;
-        decode((unsigned int)a.nlist[(size_t)k * a.stride + i], j, dx, dy, dz);
-        const float4 xj = xr[j];
-        const float delx = (xi.x - xj.x) - (float)dx * csx;
-        const float dely = (xi.y - xj.y) - (float)dy * csy;
-        const float delz = (xi.z - xj.z) - (float)dz * csz;
+        decode(ee[u], j, dx, dy, dz);
+        const float4 xj = xq[u];
+        const float delx = (xi.x - xj.x) - offf(dx, csx);
+        const float dely = (xi.y - xj.y) - offf(dy, csy);
+        const float delz = (xi.z - xj.z) - offf(dz, csz);
         const float rsq = delx * delx + dely * dely + delz * delz;
         if (rsq < cutf) {
           const int tj = __float_as_int(xj.w);
@@ -266,11 +326,11 @@ __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__r
           const float z2 = ((zv.x * p + zv.y) * p + zv.z) * p + zv.w;
           const float phi = z2 * recip;
           const float phip = z2p * recip - phi * recip;
-          const float psip = fpi * rhojp + a.fpf[j] * rhoip + phip;
+          const float psip = fpi * rhojp + fpq[u] * rhoip + phip;
           const float fpair = -psip * recip;
-          fx += (double)(delx * fpair);
-          fy += (double)(dely * fpair);
-          fz += (double)(delz * fpair);
+          cfx += delx * fpair;
+          cfy += dely * fpair;
+          cfz += delz * fpair;
           if (EV) {
             acc[0] += 0.5 * (double)phi;
             const float hf = 0.5f * fpair;
@@ -282,6 +342,10 @@ __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__r
             acc[6] += (double)(dely * delz * hf);
           }
         }
+       }
+       fx += (double)cfx;
+       fy += (double)cfy;
+       fz += (double)cfz;
       }
     }
   }
@@ -316,11 +380,11 @@ void launch_t(b200_ctx *c, const EamArgs &a, cudaEvent_t mid) {
   const int grid = md_blocks((long long)a.n * TPA, B);
   if (c->prec == B200_PREC_MIXED) {
     k_eam_rho<TPA, EV, ATOM, true><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
-    if (mid) cudaEventRecord(mid, c->stream);
+    if (mid) cudaEventRecordWithFlags(mid, c->stream, cudaEventRecordExternal);
     k_eam_force<TPA, EV, ATOM, true><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
   } else {
     k_eam_rho<TPA, EV, ATOM, false><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
-    if (mid) cudaEventRecord(mid, c->stream);
+    if (mid) cudaEventRecordWithFlags(mid, c->stream, cudaEventRecordExternal);
     k_eam_force<TPA, EV, ATOM, false><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
   }
   c->launches += 2;

@@ -12,6 +12,12 @@
 // Mixed form: positions are read as FP32 offsets from the centre of the
 // atom's cell (float4, 16 B per gather); the pair force is FP32 and each
 // atom's force, energy and virial are summed in FP64.
+//
+// Memory-level parallelism: each thread reads four list entries with one
+// 16-byte load (slab layout, md_slab) and issues the four neighbor gathers
+// before using any of them.  The FP64 kernel forms 1/rsq by Newton's method
+// from the hardware reciprocal (rcp_nr); the mixed kernel uses the fast FP32
+// reciprocal and adds each slab's FP32 force sum to the FP64 accumulator.
 #include "md_state.h"
 
 namespace {
@@ -41,6 +47,11 @@ __device__ __forceinline__ Shift3 shifts(int c, int nc, double prd) {
 __device__ __forceinline__ double pick(const Shift3 &s, int d) {
   return d < 0 ? s.m : (d > 0 ? s.p : 0.0);
 }
+__device__ __forceinline__ void decode(unsigned int e, int &j, int &dx, int &dy, int &dz) {
+  md_entry(e, j, dx, dy, dz);
+}
+// neighbour-cell centre offset along one dimension (d = -1, 0, +1)
+__device__ __forceinline__ float offf(int d, float cs) { return d < 0 ? -cs : (d > 0 ? cs : 0.f); }
 
 template <int TPA, bool EV, bool ATOM, bool SINGLE>
 __global__ void __launch_bounds__(128) k_lj_fp64(PairArgs a, const double4 *__restrict__ x4) {
@@ -76,43 +87,50 @@ __global__ void __launch_bounds__(128) k_lj_fp64(PairArgs a, const double4 *__re
     const Shift3 sy = shifts(cy, a.box.ncell[1], a.box.prd[1]);
     const Shift3 sz = shifts(cz, a.box.ncell[2], a.box.prd[2]);
     const int num = a.numneigh[i];
-    for (int k = lane; k < num; k += TPA) {
-      const unsigned int e = (unsigned int)__ldcs(&a.nlist[(size_t)k * a.stride + i]);
-      const int j = (int)(e & MD_JMASK);
-      const int code = (int)(e >> MD_JBITS);
-      const int dz = code / 9 - 1, rem = code - 9 * (dz + 1);
-      const int dy = rem / 3 - 1, dx = rem - 3 * (dy + 1) - 1;
-      const double4 xj = x4[j];
-      const double delx = __dsub_rn(xi.x, __dadd_rn(xj.x, pick(sx, dx)));
-      const double dely = __dsub_rn(xi.y, __dadd_rn(xj.y, pick(sy, dy)));
-      const double delz = __dsub_rn(xi.z, __dadd_rn(xj.z, pick(sz, dz)));
-      const double rsq = dsq3(delx, dely, delz);
-      const int tj = (int)xj.w;
-      const int tt = ti * a.ntp1 + tj;
-      const double cs = SINGLE ? cutsq1 : tab[0 * nt2 + tt];
-      if (rsq < cs) {
-        const double c1 = SINGLE ? lj1 : tab[1 * nt2 + tt];
-        const double c2 = SINGLE ? lj2 : tab[2 * nt2 + tt];
-        const double r2inv = 1.0 / rsq;
-        const double r6inv = r2inv * r2inv * r2inv;
-        const double forcelj = r6inv * (c1 * r6inv - c2);
-        const double fpair = forcelj * r2inv;
-        fx += delx * fpair;
-        fy += dely * fpair;
-        fz += delz * fpair;
-        if (EV) {
-          const double c3 = SINGLE ? lj3 : tab[3 * nt2 + tt];
-          const double c4 = SINGLE ? lj4 : tab[4 * nt2 + tt];
-          const double co = SINGLE ? off : tab[5 * nt2 + tt];
-          const double evdwl = r6inv * (c3 * r6inv - c4) - co;
-          acc[0] += 0.5 * evdwl;
-          const double hf = 0.5 * fpair;
-          acc[1] += delx * delx * hf;
-          acc[2] += dely * dely * hf;
-          acc[3] += delz * delz * hf;
-          acc[4] += delx * dely * hf;
-          acc[5] += delx * delz * hf;
-          acc[6] += dely * delz * hf;
+    const int4 *nl4 = reinterpret_cast<const int4 *>(a.nlist);
+    for (int c4 = lane; 4 * c4 < num; c4 += TPA) {
+      const int4 e4 = nl4[(size_t)c4 * a.stride + i];
+      const int m = min(4, num - 4 * c4);
+      const unsigned int ee[4] = {(unsigned int)e4.x, (unsigned int)e4.y, (unsigned int)e4.z,
+                                  (unsigned int)e4.w};
+      double4 xj[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) xj[u] = x4[u < m ? (int)(ee[u] & MD_JMASK) : i];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        if (u >= m) break;
+        int j, dx, dy, dz;
+        decode(ee[u], j, dx, dy, dz);
+        const double delx = __dsub_rn(xi.x, __dadd_rn(xj[u].x, pick(sx, dx)));
+        const double dely = __dsub_rn(xi.y, __dadd_rn(xj[u].y, pick(sy, dy)));
+        const double delz = __dsub_rn(xi.z, __dadd_rn(xj[u].z, pick(sz, dz)));
+        const double rsq = dsq3(delx, dely, delz);
+        const int tt = ti * a.ntp1 + (int)xj[u].w;
+        const double cs = SINGLE ? cutsq1 : tab[0 * nt2 + tt];
+        if (rsq < cs) {
+          const double c1 = SINGLE ? lj1 : tab[1 * nt2 + tt];
+          const double c2 = SINGLE ? lj2 : tab[2 * nt2 + tt];
+          const double r2inv = rcp_nr(rsq);
+          const double r6inv = r2inv * r2inv * r2inv;
+          const double forcelj = r6inv * (c1 * r6inv - c2);
+          const double fpair = forcelj * r2inv;
+          fx += delx * fpair;
+          fy += dely * fpair;
+          fz += delz * fpair;
+          if (EV) {
+            const double c3 = SINGLE ? lj3 : tab[3 * nt2 + tt];
+            const double c4 = SINGLE ? lj4 : tab[4 * nt2 + tt];
+            const double co = SINGLE ? off : tab[5 * nt2 + tt];
+            const double evdwl = r6inv * (c3 * r6inv - c4) - co;
+            acc[0] += 0.5 * evdwl;
+            const double hf = 0.5 * fpair;
+            acc[1] += delx * delx * hf;
+            acc[2] += dely * dely * hf;
+            acc[3] += delz * delz * hf;
+            acc[4] += delx * dely * hf;
+            acc[5] += delx * delz * hf;
+            acc[6] += dely * delz * hf;
+          }
         }
       }
     }
@@ -172,46 +190,59 @@ __global__ void __launch_bounds__(128) k_lj_mixed(PairArgs a, const float4 *__re
     const int ti = __float_as_int(xi.w);
     const float csx = (float)a.box.cs[0], csy = (float)a.box.cs[1], csz = (float)a.box.cs[2];
     const int num = a.numneigh[i];
-    for (int k = lane; k < num; k += TPA) {
-      const unsigned int e = (unsigned int)__ldcs(&a.nlist[(size_t)k * a.stride + i]);
-      const int j = (int)(e & MD_JMASK);
-      const int code = (int)(e >> MD_JBITS);
-      const int dz = code / 9 - 1, rem = code - 9 * (dz + 1);
-      const int dy = rem / 3 - 1, dx = rem - 3 * (dy + 1) - 1;
-      const float4 xj = xr[j];
-      // x_i - (x_j + image shift) = (xr_i - xr_j) - (neighbour cell centre - own cell centre)
-      const float delx = (xi.x - xj.x) - (float)dx * csx;
-      const float dely = (xi.y - xj.y) - (float)dy * csy;
-      const float delz = (xi.z - xj.z) - (float)dz * csz;
-      const float rsq = delx * delx + dely * dely + delz * delz;
-      const int tj = __float_as_int(xj.w);
-      const int tt = ti * a.ntp1 + tj;
-      const float cs = SINGLE ? cutsq1 : tabf[0 * nt2 + tt];
-      if (rsq < cs) {
-        const float c1 = SINGLE ? lj1 : tabf[1 * nt2 + tt];
-        const float c2 = SINGLE ? lj2 : tabf[2 * nt2 + tt];
-        const float r2inv = __frcp_rn(rsq);
-        const float r6inv = r2inv * r2inv * r2inv;
-        const float forcelj = r6inv * (c1 * r6inv - c2);
-        const float fpair = forcelj * r2inv;
-        fx += (double)(delx * fpair);
-        fy += (double)(dely * fpair);
-        fz += (double)(delz * fpair);
-        if (EV) {
-          const float c3 = SINGLE ? lj3 : tabf[3 * nt2 + tt];
-          const float c4 = SINGLE ? lj4 : tabf[4 * nt2 + tt];
-          const float co = SINGLE ? off : tabf[5 * nt2 + tt];
-          const float evdwl = r6inv * (c3 * r6inv - c4) - co;
-          acc[0] += 0.5 * (double)evdwl;
-          const float hf = 0.5f * fpair;
-          acc[1] += (double)(delx * delx * hf);
-          acc[2] += (double)(dely * dely * hf);
-          acc[3] += (double)(delz * delz * hf);
-          acc[4] += (double)(delx * dely * hf);
-          acc[5] += (double)(delx * delz * hf);
-          acc[6] += (double)(dely * delz * hf);
+    const int4 *nl4 = reinterpret_cast<const int4 *>(a.nlist);
+    for (int c4 = lane; 4 * c4 < num; c4 += TPA) {
+      const int4 e4 = nl4[(size_t)c4 * a.stride + i];
+      const int m = min(4, num - 4 * c4);
+      const unsigned int ee[4] = {(unsigned int)e4.x, (unsigned int)e4.y, (unsigned int)e4.z,
+                                  (unsigned int)e4.w};
+      float4 xj[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) xj[u] = xr[u < m ? (int)(ee[u] & MD_JMASK) : i];
+      // the (at most four) pair forces of a slab are summed in FP32, the
+      // slab sum is added to the atom's FP64 accumulator
+      float cfx = 0.f, cfy = 0.f, cfz = 0.f;
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        if (u >= m) break;
+        int j, dx, dy, dz;
+        decode(ee[u], j, dx, dy, dz);
+        // x_i - (x_j + image shift) = (xr_i - xr_j) - (neighbour cell centre - own cell centre)
+        const float delx = (xi.x - xj[u].x) - offf(dx, csx);
+        const float dely = (xi.y - xj[u].y) - offf(dy, csy);
+        const float delz = (xi.z - xj[u].z) - offf(dz, csz);
+        const float rsq = delx * delx + dely * dely + delz * delz;
+        const int tt = ti * a.ntp1 + __float_as_int(xj[u].w);
+        const float cs = SINGLE ? cutsq1 : tabf[0 * nt2 + tt];
+        if (rsq < cs) {
+          const float c1 = SINGLE ? lj1 : tabf[1 * nt2 + tt];
+          const float c2 = SINGLE ? lj2 : tabf[2 * nt2 + tt];
+          const float r2inv = __fdividef(1.0f, rsq);
+          const float r6inv = r2inv * r2inv * r2inv;
+          const float forcelj = r6inv * (c1 * r6inv - c2);
+          const float fpair = forcelj * r2inv;
+          cfx += delx * fpair;
+          cfy += dely * fpair;
+          cfz += delz * fpair;
+          if (EV) {
+            const float c3 = SINGLE ? lj3 : tabf[3 * nt2 + tt];
+            const float c4 = SINGLE ? lj4 : tabf[4 * nt2 + tt];
+            const float co = SINGLE ? off : tabf[5 * nt2 + tt];
+            const float evdwl = r6inv * (c3 * r6inv - c4) - co;
+            acc[0] += 0.5 * (double)evdwl;
+            const float hf = 0.5f * fpair;
+            acc[1] += (double)(delx * delx * hf);
+            acc[2] += (double)(dely * dely * hf);
+            acc[3] += (double)(delz * delz * hf);
+            acc[4] += (double)(delx * dely * hf);
+            acc[5] += (double)(delx * delz * hf);
+            acc[6] += (double)(dely * delz * hf);
+          }
         }
       }
+      fx += (double)cfx;
+      fy += (double)cfy;
+      fz += (double)cfz;
     }
   }
   fx = lane_sum<TPA>(fx);

@@ -222,6 +222,9 @@ class System:
 
     PHASES = ("initial", "neigh", "pair1", "pair2", "final")
 
+    def set_graphs(self, on=True):
+        self._ck(self._L.b200_set_graphs(self._h, int(on)))
+
     def set_timing(self, on=True):
         self._ck(self._L.b200_set_timing(self._h, int(on)))
 

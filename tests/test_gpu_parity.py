@@ -121,3 +121,18 @@ def test_device_run_reproduces_reference_log(name):
     assert st["ncalls"] == case["stats"]["builds"]
     assert st["ndanger"] == case["stats"]["dangerous"]
     assert st["full_total"] == 2 * case["stats"]["neighbors"]
+
+
+def test_eager_launches_match_graph_replay():
+    """The graph path (device-conditional rebuild) and the kernel-by-kernel
+    path run the same kernels in the same order: identical thermo."""
+    case = LOGS["potentials_lj"]
+    a = device_case(case, "fp64")
+    b = device_case(case, "fp64")
+    b.set_graphs(False)
+    ra = [a.setup()] + a.run(case["run"])
+    rb = [b.setup()] + b.run(case["run"])
+    for x, y in zip(ra, rb):
+        for col in ("Temp", "E_pair", "Press"):
+            assert x[col] == y[col]
+    assert a.neigh_stats()["ncalls"] == b.neigh_stats()["ncalls"]
