@@ -71,6 +71,25 @@ def make_eam32k(precision, setfl, x, v, hi):
     return s
 
 
+def make_eam_cu(precision):
+    """The reference's own EAM benchmark (bench/in.eam): Cu_u3 funcfl table,
+    fcc 20^3 at a = 3.615, uniform velocities at 1600 K (seed 376847, loop
+    geom), skin 1.0, every 1 delay 5 check yes, dt 5 fs."""
+    from lammps_b200 import PairEAM, System, inputs
+    x = inputs.lattice("fcc", 20, 20, 20, 3.615)
+    s = System("metal", precision, device=DEVICE)
+    s.set_box([0.0, 0.0, 0.0], [20 * 3.615] * 3)
+    p = PairEAM(1)
+    p.coeff(1, os.path.join(ROOT, "tests", "golden", "Cu_u3.eam"))
+    s.set_pair(p)
+    v = inputs.velocity_create(x, np.ones(len(x), np.int32), s.mass, 1600.0, 376847, "metal")
+    s.set_neighbor(1.0, every=1, delay=5, check=True)
+    s.set_timestep(0.005)
+    s.set_thermo(0)
+    s.set_atoms(x, None, v)
+    return s, (x, v)
+
+
 def lj4m_inputs():
     from lammps_b200 import inputs
     a = inputs.lj_lattice_constant("fcc", 0.8442)
@@ -170,7 +189,15 @@ def load_traffic():
         return {}
 
 
-def device_time_run(sysm, torch, ext, flush, nsteps):
+def device_time_run(sysm, torch, ext, flush, nsteps, start=None):
+    """One bench step: (untimed) restore of the initial state and Verlet
+    setup, L2 flush, then `nsteps` NVE steps timed with CUDA events on the
+    engine's stream.  Restarting from the same state keeps every bench step
+    the same workload: the synthetic EAM box is far from equilibrium and
+    densifies as it runs, so a continuing trajectory would drift."""
+    if start is not None:
+        sysm.set_atoms(start[0], None, start[1])
+        sysm.setup()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     with torch.cuda.stream(ext):
@@ -182,15 +209,15 @@ def device_time_run(sysm, torch, ext, flush, nsteps):
     return e0.elapsed_time(e1)
 
 
-def time_form(sysm, torch, flush, K, W, timing=False):
+def time_form(sysm, torch, flush, K, W, start, timing=False):
     """Warm up, then K timed bench steps; returns (total ms, per-step ms list)."""
     ext = torch.cuda.ExternalStream(sysm.stream)
     sysm.setup()
     sysm.set_timing(timing)
     for _ in range(W):
-        device_time_run(sysm, torch, ext, flush, MD_STEPS)
+        device_time_run(sysm, torch, ext, flush, MD_STEPS, start)
     sysm.timing(reset=True)
-    ms = [device_time_run(sysm, torch, ext, flush, MD_STEPS) for _ in range(K)]
+    ms = [device_time_run(sysm, torch, ext, flush, MD_STEPS, start) for _ in range(K)]
     return sum(ms), ms
 
 
@@ -304,10 +331,10 @@ def profile_case(args):
         raise SystemExit(f"unknown case {args.case}")
     if args.eager:
         s.set_graphs(False)
-    total, per = time_form(s, torch, flush, args.steps, max(args.warmup, 1))
+    total, per = time_form(s, torch, flush, args.steps, max(args.warmup, 1), (x, v))
     s.set_timing(True)
     ext = torch.cuda.ExternalStream(s.stream)
-    device_time_run(s, torch, ext, flush, MD_STEPS)
+    device_time_run(s, torch, ext, flush, MD_STEPS, (x, v))
     ph = s.timing(reset=True)
     print(json.dumps({"case": args.case, "atoms": s.n, "steps": args.steps,
                       "matom_steps_per_s": s.n * MD_STEPS * args.steps / (total * 1e3),
@@ -333,8 +360,9 @@ def main():
         return profile_case(args)
     K, W = args.steps, max(args.warmup, 3)
     ws, rank, local = dist_setup()
-    config = {"workload": "eam-32k fcc 20^3 synthetic setfl, 100 NVE steps per bench step "
-                          "(configs[1]); also lj-4M fcc 100^3 (configs[4])",
+    config = {"workload": "eam-32k fcc 20^3 synthetic setfl, the first 100 NVE steps from the "
+                          "seeded initial state per bench step (configs[1]); also eam Cu_u3 32k "
+                          "(bench/in.eam) and lj-4M fcc 100^3 (configs[4])",
               "atoms": 32000, "md_steps_per_step": MD_STEPS, "precision": "mixed",
               "l2": "flushed (256 MB write) before every timed bench step",
               "parallelism": f"replicas x{ws}"}
@@ -369,14 +397,15 @@ def main():
     # ---- headline: mixed precision EAM, device-timed -----------------------
     launches0 = None
     sysm.setup()
+    start = (x, v)
     for _ in range(W):
-        device_time_run(sysm, torch, ext, flush, MD_STEPS)
+        device_time_run(sysm, torch, ext, flush, MD_STEPS, start)
     barrier(ws)
     torch.cuda.synchronize()
     clocks = ClockSampler(dev)
     clocks.start()
     launches0 = sysm.kernel_launches
-    per = [device_time_run(sysm, torch, ext, flush, MD_STEPS) for _ in range(K)]
+    per = [device_time_run(sysm, torch, ext, flush, MD_STEPS, start) for _ in range(K)]
     torch.cuda.synchronize()
     launches = sysm.kernel_launches - launches0
     barrier(ws)
@@ -387,9 +416,9 @@ def main():
     # ---- per-phase device timers over the same number of bench steps ------
     sysm.set_timing(True)
     for _ in range(2):
-        device_time_run(sysm, torch, ext, flush, MD_STEPS)
+        device_time_run(sysm, torch, ext, flush, MD_STEPS, start)
     sysm.timing(reset=True)
-    per_t = [device_time_run(sysm, torch, ext, flush, MD_STEPS) for _ in range(K)]
+    per_t = [device_time_run(sysm, torch, ext, flush, MD_STEPS, start) for _ in range(K)]
     ph = sysm.timing(reset=True)
     sysm.set_timing(False)
     steps_t = max(ph["steps"], 1)
@@ -422,21 +451,29 @@ def main():
     extras = {}
     if not args.no_extras:
         s64 = make_eam32k("fp64", setfl, x, v, hi)
-        t64, _ = time_form(s64, torch, flush, K, W)
+        t64, _ = time_form(s64, torch, flush, K, W, start)
         extras["eam_32k"] = {"mixed": value / ws, "fp64": n * MD_STEPS * K / (t64 * 1e3)}
         extras["eam_32k"]["mixed_over_fp64"] = extras["eam_32k"]["mixed"] / extras["eam_32k"]["fp64"]
         s64.close()
+        cu = {}
+        for prec in ("mixed", "fp64"):
+            scu, st = make_eam_cu(prec)
+            t, _ = time_form(scu, torch, flush, K, W, st)
+            cu[prec] = scu.n * MD_STEPS * K / (t * 1e3)
+            scu.close()
+        cu["mixed_over_fp64"] = cu["mixed"] / cu["fp64"]
+        extras["eam_cu_u3_32k"] = cu
         x4, v4, hi4 = lj4m_inputs()
         lj = {}
         for prec in ("mixed", "fp64"):
             s = make_lj(prec, x4, v4, hi4)
             k4 = max(2, K // 3)
-            t, _ = time_form(s, torch, flush, k4, 2)
+            t, _ = time_form(s, torch, flush, k4, 2, (x4, v4))
             s.set_timing(True)
             ext4 = torch.cuda.ExternalStream(s.stream)
-            device_time_run(s, torch, ext4, flush, MD_STEPS)
+            device_time_run(s, torch, ext4, flush, MD_STEPS, (x4, v4))
             s.timing(reset=True)
-            device_time_run(s, torch, ext4, flush, MD_STEPS)
+            device_time_run(s, torch, ext4, flush, MD_STEPS, (x4, v4))
             ph4 = s.timing(reset=True)
             lj[prec] = len(x4) * MD_STEPS * k4 / (t * 1e3)
             lj[prec + "_phases_ms_per_step"] = {k: ph4[k] / max(ph4["steps"], 1) for k in s.PHASES}

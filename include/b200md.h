@@ -138,8 +138,9 @@ int b200_nve_final(b200_ctx *ctx, double dtf);
    step with energy and virial.  Returns the thermo row of that step. */
 int b200_setup(b200_ctx *ctx, double *row);
 /* Verlet::run(nsteps) (src/verlet.cpp:207-309) with fix nve and the
-   neighbor schedule of b200_set_neighbor, entirely on the device (CUDA graph
-   per step, rebuild taken by a device-side decision).  Every `thermo_every`
+   neighbor schedule of b200_set_neighbor; the atoms never leave the device.
+   The host mirrors Neighbor::decide and reads the device's distance test
+   back only on steps where `check yes` could rebuild.  Every `thermo_every`
    steps and at the last step a thermo row is recorded:
      row = {step, sum m v^2, eng_vdwl, virial[0..5]}  (9 doubles)
    from which the host forms Temp, E_pair, TotEng and Press exactly as
@@ -165,7 +166,7 @@ int b200_neigh_stats(b200_ctx *ctx, long long *full_total, int *ncalls, int *nda
 /* EAM density and embedding derivative of the last compute (PairEAM rho, fp). */
 int b200_get_rho_fp(b200_ctx *ctx, double *rho, double *fp);
 
-/* Launch shape of the pair kernels: threads per atom (1,2,4,8; 0 = chosen by
+/* Launch shape of the pair kernels: threads per atom (1,2,4,8,16,32; 0 = chosen by
    the autotuner on the next b200_setup) and threads per block. */
 int b200_set_launch(b200_ctx *ctx, int threads_per_atom, int block_size);
 int b200_get_launch(const b200_ctx *ctx, int *threads_per_atom, int *block_size);
@@ -179,10 +180,11 @@ int b200_get_launch(const b200_ctx *ctx, int *threads_per_atom, int *block_size)
      4 fix nve final half-step (+ kinetic energy and thermo row on output steps)
    b200_get_timing returns milliseconds summed over the timed steps. */
 int b200_set_timing(b200_ctx *ctx, int on);
-/* on = 1 (default): b200_run replays one CUDA graph per step, the rebuild
-   held in a device-conditional IF node.  on = 0: the same kernels launched
-   one by one with the rebuild decision read back each step (for profilers,
-   which cannot look inside graphs with conditional nodes). */
+/* on = 1 (default): b200_run replays captured CUDA graphs of the step's
+   pieces (initial half-step + decision, rebuild, forces + final half-step).
+   on = 0: the same kernels launched one by one (for profilers and hosts
+   that do not want graphs).  Both follow the same host-mirrored rebuild
+   schedule and give identical results. */
 int b200_set_graphs(b200_ctx *ctx, int on);
 int b200_get_timing(b200_ctx *ctx, double phase_ms[5], long long *steps, int reset);
 /* Kernel launches issued by the context since creation (for accounting);

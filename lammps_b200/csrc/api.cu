@@ -47,7 +47,7 @@ void dfree(T *&p) {
 }
 
 void invalidate_graphs(b200_ctx *c) {
-  for (int k = 0; k < 2; k++) {
+  for (int k = 0; k < 4; k++) {
     if (c->step_exec[k]) cudaGraphExecDestroy(c->step_exec[k]);
     if (c->step_graph[k]) cudaGraphDestroy(c->step_graph[k]);
     c->step_exec[k] = nullptr;
@@ -305,8 +305,8 @@ int autotune(b200_ctx *c) {
   CK(cudaEventCreate(&e1));
   float best = 1e30f;
   int best_tpa = 1;
-  const int cand[4] = {1, 2, 4, 8};
-  for (int k = 0; k < 4; k++) {
+  const int cand[6] = {1, 2, 4, 8, 16, 32};
+  for (int k = 0; k < 6; k++) {
     c->tpa = cand[k];
     int rc = pair_compute_dev(c, false, false, nullptr, nullptr);
     if (rc) return rc;
@@ -339,167 +339,122 @@ int count_kernels(b200_ctx *c, cudaGraph_t g, int *kernels, std::vector<cudaGrap
   *kernels = 0;
   for (auto nd : nodes) {
     cudaGraphNodeType t;
-    // this runtime reports the conditional node's type as an error: such a
-    // node is neither a kernel nor an event record, so it is skipped
-    if (cudaGraphNodeGetType(nd, &t) != cudaSuccess) {
-      (void)cudaGetLastError();
-      continue;
-    }
+    CK(cudaGraphNodeGetType(nd, &t));
     if (t == cudaGraphNodeTypeKernel) (*kernels)++;
     if (events && t == cudaGraphNodeTypeEventRecord) events->push_back(nd);
   }
   return B200_OK;
 }
 
-int capture_step(b200_ctx *c, bool out, double dtv, double dtf, int slot) {
-  // One MD step (Verlet::run body, src/verlet.cpp:223-308) as a CUDA graph:
-  //   [nve initial, decide] -> IF(rebuild){wrap, sort, list} -> [pair, nve final, row]
-  // The decide kernel sets the IF node's condition on the device, so a step
-  // without a rebuild launches none of the rebuild kernels.  With timing on,
-  // event-record nodes mark the phase boundaries; their events are swapped
-  // per replay so every step's phases can be read back.
-  const bool tm = c->timing;
-  const long long launches0 = c->launches;
-  const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
-  cudaGraph_t g = nullptr;
-  CK(cudaGraphCreate(&g, 0));
-  cudaGraphConditionalHandle cond;
-  cudaError_t e = cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault);
-  // part 1
-  if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(c->stream, g, nullptr, nullptr, 0, mode);
-  if (e == cudaSuccess) {
-    cudaError_t ek = cudaSuccess;
-    if (tm) ek = cudaEventRecordWithFlags(c->ph_event[0], c->stream, cudaEventRecordExternal);
-    if (ek == cudaSuccess) ek = md_nve_initial(c, dtv, dtf);
-    if (ek == cudaSuccess) ek = md_decide(c, cond);
-    if (ek == cudaSuccess && tm)
-      ek = cudaEventRecordWithFlags(c->ph_event[1], c->stream, cudaEventRecordExternal);
-    std::vector<cudaGraphNode_t> tail;
-    if (ek == cudaSuccess) {
-      cudaStreamCaptureStatus st;
-      const cudaGraphNode_t *deps = nullptr;
-      size_t nd = 0;
-      ek = cudaStreamGetCaptureInfo(c->stream, &st, nullptr, nullptr, &deps, &nd);
-      if (ek == cudaSuccess) tail.assign(deps, deps + nd);
-    }
-    cudaGraph_t gout = nullptr;
-    e = cudaStreamEndCapture(c->stream, &gout);
-    if (e == cudaSuccess) e = ek;
-    // IF node holding the rebuild
-    cudaGraphNode_t cnode = nullptr;
-    cudaGraph_t body = nullptr;
+// A step (Verlet::run body, src/verlet.cpp:223-308) is three pieces:
+//   PRE     fix nve initial half-step + the rebuild decision
+//   REBUILD wrap, cell sort, neighbor list (only on rebuild steps)
+//   POST    pair forces, fix nve final half-step (+ kinetic energy and thermo
+//           row on output steps)
+// The host launches REBUILD exactly when the reference's Neighbor::decide
+// would rebuild: it mirrors the `ago` counter, so with `check no` the
+// schedule needs no device read-back, and with `check yes` it reads the
+// device's distance test only on the steps where a rebuild is possible.
+// Each piece is a captured CUDA graph (or, with graphs off, its kernels
+// launched one by one).  With timing on, events mark the phase boundaries:
+// PRE holds phases 0-1, POST phases 2-5; their events are swapped per
+// launch so every step's phases can be read back.
+enum { PIECE_PRE = 0, PIECE_REBUILD = 1, PIECE_POST_OUT = 2, PIECE_POST = 3 };
+
+cudaError_t record(b200_ctx *c, cudaEvent_t ev) {
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(c->stream, &st);
+  return st == cudaStreamCaptureStatusActive
+             ? cudaEventRecordWithFlags(ev, c->stream, cudaEventRecordExternal)
+             : cudaEventRecord(ev, c->stream);
+}
+
+// launch the kernels of one piece; ev (optional) are the piece's events
+cudaError_t launch_piece(b200_ctx *c, int kind, double dtv, double dtf, cudaEvent_t *ev) {
+  cudaError_t e = cudaSuccess;
+  if (kind == PIECE_PRE) {
+    if (ev) e = record(c, ev[0]);
+    if (e == cudaSuccess) e = md_nve_initial(c, dtv, dtf);
+    if (e == cudaSuccess) e = md_decide(c);
+    if (e == cudaSuccess && ev) e = record(c, ev[1]);
+  } else if (kind == PIECE_REBUILD) {
+    e = md_rebuild(c, nullptr);
+  } else {
+    const bool out = kind == PIECE_POST_OUT;
+    if (ev) e = record(c, ev[0]);
     if (e == cudaSuccess) {
-      cudaGraphNodeParams cp = {};
-      cp.type = cudaGraphNodeTypeConditional;
-      cp.conditional.handle = cond;
-      cp.conditional.type = cudaGraphCondTypeIf;
-      cp.conditional.size = 1;
-      e = cudaGraphAddNode(&cnode, g, tail.data(), tail.size(), &cp);
-      if (e == cudaSuccess) body = cp.conditional.phGraph_out[0];
-    }
-    if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(c->stream, body, nullptr, nullptr, 0, mode);
-    if (e == cudaSuccess) {
-      cudaError_t ek2 = md_rebuild(c, nullptr);
-      cudaGraph_t bout = nullptr;
-      e = cudaStreamEndCapture(c->stream, &bout);
-      if (e == cudaSuccess) e = ek2;
-    }
-    // part 2, after the IF node
-    if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(c->stream, g, &cnode, nullptr, 1, mode);
-    if (e == cudaSuccess) {
-      cudaError_t ek3 = cudaSuccess;
-      if (tm) ek3 = cudaEventRecordWithFlags(c->ph_event[2], c->stream, cudaEventRecordExternal);
-      if (ek3 == cudaSuccess) {
-        if (c->pstyle == B200_PAIR_LJ_CUT) {
-          ek3 = md_lj_compute(c, out, false, nullptr, nullptr);
-          if (ek3 == cudaSuccess && tm)
-            ek3 = cudaEventRecordWithFlags(c->ph_event[3], c->stream, cudaEventRecordExternal);
-        } else {
-          ek3 = md_eam_compute(c, out, false, nullptr, nullptr, tm ? c->ph_event[3] : nullptr);
-        }
+      if (c->pstyle == B200_PAIR_LJ_CUT) {
+        e = md_lj_compute(c, out, false, nullptr, nullptr);
+        if (e == cudaSuccess && ev) e = record(c, ev[1]);
+      } else {
+        e = md_eam_compute(c, out, false, nullptr, nullptr, ev ? ev[1] : nullptr);
       }
-      if (ek3 == cudaSuccess && tm)
-        ek3 = cudaEventRecordWithFlags(c->ph_event[4], c->stream, cudaEventRecordExternal);
-      if (ek3 == cudaSuccess) ek3 = md_nve_final(c, dtf, out);
-      if (ek3 == cudaSuccess && out) ek3 = md_record_row(c);
-      if (ek3 == cudaSuccess && tm)
-        ek3 = cudaEventRecordWithFlags(c->ph_event[5], c->stream, cudaEventRecordExternal);
-      cudaGraph_t gout2 = nullptr;
-      e = cudaStreamEndCapture(c->stream, &gout2);
-      if (e == cudaSuccess) e = ek3;
     }
-    if (e == cudaSuccess) {
-      int bk = 0;
-      int rc = count_kernels(c, body, &bk, nullptr);
-      if (rc) {
-        cudaGraphDestroy(g);
-        return rc;
-      }
-      c->rebuild_kernels = bk;
-    }
+    if (e == cudaSuccess && ev) e = record(c, ev[2]);
+    if (e == cudaSuccess) e = md_nve_final(c, dtf, out);
+    if (e == cudaSuccess && out) e = md_record_row(c);
+    if (e == cudaSuccess && ev) e = record(c, ev[3]);
   }
+  return e;
+}
+
+int capture_piece(b200_ctx *c, int kind, double dtv, double dtf) {
+  const bool tm = c->timing && kind != PIECE_REBUILD;
+  const long long launches0 = c->launches;
+  cudaGraph_t g = nullptr;
+  CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = launch_piece(c, kind, dtv, dtf, tm ? c->ph_event : nullptr);
+  cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
   c->launches = launches0;
-  if (e != cudaSuccess) {
-    cudaGraphDestroy(g);
-    return set_err(c, B200_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+  if (e != cudaSuccess || e2 != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return set_err(c, B200_ERR_CUDA, "graph capture: %s / %s", cudaGetErrorString(e),
+                   cudaGetErrorString(e2));
   }
   int kernels = 0;
-  c->ev_nodes[slot].clear();
-  int rc = count_kernels(c, g, &kernels, &c->ev_nodes[slot]);
+  c->ev_nodes[kind].clear();
+  int rc = count_kernels(c, g, &kernels, &c->ev_nodes[kind]);
   if (rc) {
     cudaGraphDestroy(g);
     return rc;
   }
-  if (tm && c->ev_nodes[slot].size() != MD_NPHASE + 1) {
+  const size_t want = !tm ? 0 : (kind == PIECE_PRE ? 2 : 4);
+  if (c->ev_nodes[kind].size() != want) {
     cudaGraphDestroy(g);
-    return set_err(c, B200_ERR_CUDA, "graph capture: expected %d event nodes, found %zu",
-                   MD_NPHASE + 1, c->ev_nodes[slot].size());
+    return set_err(c, B200_ERR_CUDA, "graph capture: expected %zu event nodes, found %zu", want,
+                   c->ev_nodes[kind].size());
   }
-  e = cudaGraphInstantiate(&c->step_exec[slot], g, 0);
+  e = cudaGraphInstantiate(&c->step_exec[kind], g, 0);
   if (e != cudaSuccess) {
     cudaGraphDestroy(g);
     return set_err(c, B200_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
   }
-  c->step_graph[slot] = g;
-  c->step_kernels[slot] = kernels;
+  c->step_graph[kind] = g;
+  c->step_kernels[kind] = kernels;
   return B200_OK;
 }
 
-// The same step as the graph, launched kernel by kernel; the rebuild
-// decision is read back to the host (one synchronisation per step).  Used
-// for profiling (tools cannot look inside graphs with conditional nodes) and
-// as a path without graphs.  `ev`, when given, receives the phase events.
-int eager_step(b200_ctx *c, bool out, double dtv, double dtf, cudaEvent_t *ev) {
-  if (ev) CK(cudaEventRecord(ev[0], c->stream));
-  CK(md_nve_initial(c, dtv, dtf));
-  CK(md_decide(c, 0));
-  if (ev) CK(cudaEventRecord(ev[1], c->stream));
-  int rebuild = 0;
-  CK(cudaMemcpyAsync(&c->status_host[ST_REBUILD], c->status + ST_REBUILD, sizeof(int),
-                     cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
-  rebuild = c->status_host[ST_REBUILD];
-  if (rebuild) CK(md_rebuild(c, nullptr));
-  if (ev) CK(cudaEventRecord(ev[2], c->stream));
-  if (c->pstyle == B200_PAIR_LJ_CUT) {
-    CK(md_lj_compute(c, out, false, nullptr, nullptr));
-    if (ev) CK(cudaEventRecord(ev[3], c->stream));
-  } else {
-    CK(md_eam_compute(c, out, false, nullptr, nullptr, ev ? ev[3] : nullptr));
+// run one piece: graph replay, or the kernels themselves with graphs off
+int run_piece(b200_ctx *c, int kind, double dtv, double dtf, cudaEvent_t *ev) {
+  if (!c->use_graphs) {
+    CK(launch_piece(c, kind, dtv, dtf, ev));
+    return B200_OK;
   }
-  if (ev) CK(cudaEventRecord(ev[4], c->stream));
-  CK(md_nve_final(c, dtf, out));
-  if (out) CK(md_record_row(c));
-  if (ev) CK(cudaEventRecord(ev[5], c->stream));
+  if (ev)
+    for (size_t k = 0; k < c->ev_nodes[kind].size(); k++)
+      CK(cudaGraphExecEventRecordNodeSetEvent(c->step_exec[kind], c->ev_nodes[kind][k], ev[k]));
+  CK(cudaGraphLaunch(c->step_exec[kind], c->stream));
+  c->launches += c->step_kernels[kind];
   return B200_OK;
 }
 
 int ensure_graphs(b200_ctx *c, double dtv, double dtf, double ftm2v) {
   if (!c->use_graphs) return B200_OK;
   if (c->graph_valid) return B200_OK;
-  int rc = capture_step(c, false, dtv, dtf, 0);
-  if (!rc) rc = capture_step(c, true, dtv, dtf, 1);
-  if (rc) return rc;
+  for (int kind = 0; kind < 4; kind++) {
+    int rc = capture_piece(c, kind, dtv, dtf);
+    if (rc) return rc;
+  }
   c->graph_valid = true;
   c->graph_dt = dtv;
   c->graph_ftm2v = ftm2v;
@@ -808,7 +763,9 @@ int b200_upload_atoms(b200_ctx *c, int n, const double *x, const double *v, cons
     CK(dalloc(&c->perm, stride));
     CK(dalloc(&c->cell_tmp, stride));
     CK(dalloc(&c->numneigh, stride));
-    c->partial_blocks = stride / 16 + 64;
+    // one partial per block of the widest pair launch (32 threads per atom,
+    // 128 threads per block)
+    c->partial_blocks = stride / 4 + 64;
     CK(dalloc(&c->partial, (size_t)c->partial_blocks * 8));
     c->nalloc = n;
     c->stride = stride;
@@ -1015,6 +972,7 @@ int b200_run(b200_ctx *c, int nsteps, double dt, double ftm2v, int thermo_every,
   const long long last = step0 + nsteps;
   long long s = step0 + 1;
   int replays = 0;
+  bool force_build = false;
   while (s <= last) {
     const long long s_end = (last - s + 1) > chunk ? s + chunk - 1 : last;
     // A list that outgrows its capacity during a chunk is recovered by
@@ -1023,29 +981,42 @@ int b200_run(b200_ctx *c, int nsteps, double dt, double ftm2v, int thermo_every,
     // overflow, boost neigh_modify one", src/neigh_half_bin.cpp:414-415).
     int rc = snapshot(c, true);
     if (rc) return rc;
-    const int ncalls0 = c->status_host[ST_NCALLS];
+    const int ago0 = c->status_host[ST_AGO];
+    auto is_out = [&](long long t) {
+      return (t == last) || (thermo_every > 0 && t % thermo_every == 0);
+    };
+    // host mirror of Neighbor::ago (src/neighbor.cpp:1301-1309)
+    int ago = c->status_host[ST_AGO];
     for (long long t = s; t <= s_end; t++) {
-      const bool out = (t == last) || (thermo_every > 0 && t % thermo_every == 0);
-      const int g = out ? 1 : 0;
-      const size_t base = (size_t)(t - s) * (MD_NPHASE + 1);
-      if (!c->use_graphs) {
-        rc = eager_step(c, out, dtv, dtf, c->timing ? &c->ev_pool[base] : nullptr);
+      cudaEvent_t *ev = c->timing ? &c->ev_pool[(size_t)(t - s) * (MD_NPHASE + 1)] : nullptr;
+      rc = run_piece(c, PIECE_PRE, dtv, dtf, ev);
+      if (rc) return rc;
+      ago++;
+      bool rebuild = false;
+      if (force_build) {
+        rebuild = true;  // replay after an overflow: the device decides the same
+        force_build = false;
+      } else if (ago >= c->delay && ago % c->every == 0) {
+        if (!c->check) {
+          rebuild = true;
+        } else {
+          // distance criterion: the decision the device just made
+          CK(cudaMemcpyAsync(&c->status_host[ST_REBUILD], c->status + ST_REBUILD, sizeof(int),
+                             cudaMemcpyDeviceToHost, c->stream));
+          CK(cudaStreamSynchronize(c->stream));
+          rebuild = c->status_host[ST_REBUILD] != 0;
+        }
+      }
+      if (rebuild) {
+        rc = run_piece(c, PIECE_REBUILD, dtv, dtf, nullptr);
         if (rc) return rc;
-        continue;
+        ago = 0;
       }
-      if (c->timing) {
-        for (int k = 0; k <= MD_NPHASE; k++)
-          CK(cudaGraphExecEventRecordNodeSetEvent(c->step_exec[g], c->ev_nodes[g][k],
-                                                  c->ev_pool[base + k]));
-      }
-      CK(cudaGraphLaunch(c->step_exec[g], c->stream));
-      c->launches += c->step_kernels[g];
+      rc = run_piece(c, is_out(t) ? PIECE_POST_OUT : PIECE_POST, dtv, dtf, ev ? ev + 2 : nullptr);
+      if (rc) return rc;
     }
     rc = read_status(c);
     if (rc) return rc;
-    // kernels of the rebuild body ran once per build taken in this chunk
-    if (c->use_graphs)
-      c->launches += (long long)c->rebuild_kernels * (c->status_host[ST_NCALLS] - ncalls0);
     if (c->status_host[ST_LOST]) return status_errors(c);
     if (c->status_host[ST_OVERFLOW]) {
       if (c->one_user > 0 || ++replays > 4) return status_errors(c);
@@ -1060,6 +1031,8 @@ int b200_run(b200_ctx *c, int nsteps, double dt, double ftm2v, int thermo_every,
       CK(cudaMemcpyAsync(c->status + ST_FORCE_BUILD, &one, sizeof(int), cudaMemcpyHostToDevice,
                          c->stream));
       CK(cudaStreamSynchronize(c->stream));
+      c->status_host[ST_AGO] = ago0;
+      force_build = true;
       c->overflow_replays++;
       continue;
     }
@@ -1171,8 +1144,8 @@ int b200_get_rho_fp(b200_ctx *c, double *rho, double *fp) {
 
 int b200_set_launch(b200_ctx *c, int tpa, int block) {
   if (!c) return B200_ERR_ARG;
-  if (!(tpa == 0 || tpa == 1 || tpa == 2 || tpa == 4 || tpa == 8))
-    return set_err(c, B200_ERR_ARG, "threads per atom must be 0, 1, 2, 4 or 8");
+  if (!(tpa == 0 || tpa == 1 || tpa == 2 || tpa == 4 || tpa == 8 || tpa == 16 || tpa == 32))
+    return set_err(c, B200_ERR_ARG, "threads per atom must be 0, 1, 2, 4, 8, 16 or 32");
   if (block != 0 && block != 128) return set_err(c, B200_ERR_ARG, "block size must be 128");
   c->tpa = tpa;
   c->tuned = tpa != 0;

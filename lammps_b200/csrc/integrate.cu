@@ -95,11 +95,10 @@ __global__ void __launch_bounds__(256) k_ke(int n, int stride, const double *__r
   block_partials_finish<1>(acc, red, partial, counter, out, false);
 }
 
-// Neighbor::decide (src/neighbor.cpp:1294-1309) on the device.  Inside a
-// step graph the decision also sets the condition of the IF node that holds
-// the rebuild kernels, so steps without a rebuild launch none of them.
-__global__ void k_decide(int *status, int every, int delay, int check,
-                         cudaGraphConditionalHandle cond) {
+// Neighbor::decide (src/neighbor.cpp:1294-1309) on the device: the host
+// mirrors the same schedule and reads ST_REBUILD only when the distance
+// criterion decides.
+__global__ void k_decide(int *status, int every, int delay, int check) {
   const int ago = status[ST_AGO] + 1;
   status[ST_AGO] = ago;
   int rebuild = 0;
@@ -116,7 +115,6 @@ __global__ void k_decide(int *status, int every, int delay, int check,
   }
   status[ST_MOVED] = 0;
   status[ST_REBUILD] = rebuild;
-  if (cond) cudaGraphSetConditional(cond, rebuild ? 1u : 0u);
   unsigned int lo = (unsigned int)status[ST_STEP_LO] + 1u;
   if (lo == 0u) status[ST_STEP_HI] += 1;
   status[ST_STEP_LO] = (int)lo;
@@ -169,8 +167,8 @@ cudaError_t md_ke(b200_ctx *c) {
   return cudaGetLastError();
 }
 
-cudaError_t md_decide(b200_ctx *c, cudaGraphConditionalHandle cond) {
-  k_decide<<<1, 1, 0, c->stream>>>(c->status, c->every, c->delay, c->check, cond);
+cudaError_t md_decide(b200_ctx *c) {
+  k_decide<<<1, 1, 0, c->stream>>>(c->status, c->every, c->delay, c->check);
   c->launches++;
   return cudaGetLastError();
 }

@@ -111,10 +111,11 @@ struct b200_ctx {
   bool tuned = false;
 
   // CUDA graph of one MD step (captured lazily by b200_run)
-  cudaGraphExec_t step_exec[2] = {nullptr, nullptr};  // [0] no output, [1] output
-  cudaGraph_t step_graph[2] = {nullptr, nullptr};
-  int step_kernels[2] = {0, 0};                         // kernel nodes per graph
-  int rebuild_kernels = 0;                              // kernel nodes of the rebuild body
+  // graphs of the step pieces: [0] initial half-step + decision, [1] rebuild,
+  // [2] forces + final half-step with thermo output, [3] the same without
+  cudaGraphExec_t step_exec[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaGraph_t step_graph[4] = {nullptr, nullptr, nullptr, nullptr};
+  int step_kernels[4] = {0, 0, 0, 0};                   // kernel nodes per graph
   bool graph_valid = false;
   double graph_dt = 0, graph_ftm2v = 0;
   int graph_tpa = 0;
@@ -125,7 +126,7 @@ struct b200_ctx {
   // event-record nodes at the phase boundaries of every step graph
   bool timing = false;
   cudaEvent_t ph_event[MD_NPHASE + 1] = {};           // placeholders used at capture
-  std::vector<cudaGraphNode_t> ev_nodes[2];            // event-record nodes per graph
+  std::vector<cudaGraphNode_t> ev_nodes[4];            // event-record nodes per graph
   std::vector<cudaEvent_t> ev_pool;                    // per-step events of a chunk
   double phase_ms[MD_NPHASE] = {0};
   long long phase_steps = 0;
@@ -146,8 +147,7 @@ cudaError_t md_eam_compute(b200_ctx *c, bool ev, bool atom_ev, double *eatom, do
 cudaError_t md_nve_initial(b200_ctx *c, double dtv, double dtf);
 cudaError_t md_nve_final(b200_ctx *c, double dtf, bool ke);
 cudaError_t md_ke(b200_ctx *c);
-// `cond` (0 outside graphs) receives the rebuild decision as an IF condition
-cudaError_t md_decide(b200_ctx *c, cudaGraphConditionalHandle cond);
+cudaError_t md_decide(b200_ctx *c);
 cudaError_t md_record_row(b200_ctx *c);
 cudaError_t md_zero_ev(b200_ctx *c);
 

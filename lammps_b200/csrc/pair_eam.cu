@@ -374,17 +374,29 @@ __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__r
   }
 }
 
+// phase event between the two passes: an event-record node when the stream
+// is being captured into a step graph, a plain record otherwise
+void record_mid(b200_ctx *c, cudaEvent_t mid) {
+  if (!mid) return;
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(c->stream, &st);
+  if (st == cudaStreamCaptureStatusActive)
+    cudaEventRecordWithFlags(mid, c->stream, cudaEventRecordExternal);
+  else
+    cudaEventRecord(mid, c->stream);
+}
+
 template <int TPA, bool EV, bool ATOM>
 void launch_t(b200_ctx *c, const EamArgs &a, cudaEvent_t mid) {
   const int B = 128;
   const int grid = md_blocks((long long)a.n * TPA, B);
   if (c->prec == B200_PREC_MIXED) {
     k_eam_rho<TPA, EV, ATOM, true><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
-    if (mid) cudaEventRecordWithFlags(mid, c->stream, cudaEventRecordExternal);
+    record_mid(c, mid);
     k_eam_force<TPA, EV, ATOM, true><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
   } else {
     k_eam_rho<TPA, EV, ATOM, false><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
-    if (mid) cudaEventRecordWithFlags(mid, c->stream, cudaEventRecordExternal);
+    record_mid(c, mid);
     k_eam_force<TPA, EV, ATOM, false><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
   }
   c->launches += 2;
@@ -439,7 +451,9 @@ cudaError_t md_eam_compute(b200_ctx *c, bool ev, bool atom_ev, double *eatom, do
     case 1: launch_tpa<1>(c, a, ev, atom_ev, mid); break;
     case 2: launch_tpa<2>(c, a, ev, atom_ev, mid); break;
     case 4: launch_tpa<4>(c, a, ev, atom_ev, mid); break;
-    default: launch_tpa<8>(c, a, ev, atom_ev, mid); break;
+    case 8: launch_tpa<8>(c, a, ev, atom_ev, mid); break;
+    case 16: launch_tpa<16>(c, a, ev, atom_ev, mid); break;
+    default: launch_tpa<32>(c, a, ev, atom_ev, mid); break;
   }
   return cudaGetLastError();
 }

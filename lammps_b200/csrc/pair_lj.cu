@@ -319,7 +319,9 @@ cudaError_t md_lj_compute(b200_ctx *c, bool ev, bool atom_ev, double *eatom, dou
     case 1: launch_tpa<1>(c, a, ev, atom_ev, single); break;
     case 2: launch_tpa<2>(c, a, ev, atom_ev, single); break;
     case 4: launch_tpa<4>(c, a, ev, atom_ev, single); break;
-    default: launch_tpa<8>(c, a, ev, atom_ev, single); break;
+    case 8: launch_tpa<8>(c, a, ev, atom_ev, single); break;
+    case 16: launch_tpa<16>(c, a, ev, atom_ev, single); break;
+    default: launch_tpa<32>(c, a, ev, atom_ev, single); break;
   }
   return cudaGetLastError();
 }
