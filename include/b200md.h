@@ -193,6 +193,27 @@ long long b200_kernel_launches(const b200_ctx *ctx);
 /* CUDA stream of the context, as a void* (cudaStream_t). */
 void *b200_stream(const b200_ctx *ctx);
 
+/* ---- allocation-free entry point -------------------------------------------- */
+
+/* No counterpart in the reference.  Sum over n atoms of
+   (vx^2 + vy^2 + vz^2) * mass[type[i]] -- the sum ComputeTemp::compute_scalar
+   forms before scaling -- written to out[0], for callers that must not
+   allocate device memory at the point of the call: code recording a CUDA
+   graph by stream capture (where cudaMalloc is not allowed) or a host whose
+   device memory belongs to another allocator.  No context is needed; v
+   (3n doubles, xyz interleaved), type (n ints, each in 1..ntypes), mass
+   (ntypes+1 doubles) and out are device pointers, and the call is ordered
+   on `stream` (a cudaStream_t; NULL = the legacy default stream).  It
+   allocates nothing: its reduction scratch is a fixed static device array
+   (1184 block partials and a counter, about 9.5 KB per device) whose address
+   is looked up on the first call on each device, so make that first call
+   before any stream capture begins.  n is limited to the engine's atom limit
+   (2^26 - 1) and ntypes to 8: larger values return B200_ERR_ARG.  All calls
+   share the one scratch array, so calls that may overlap on the GPU (other
+   streams, other host threads) race and must be serialised by the caller. */
+int b200_kinetic_sum_noalloc(int n, const double *v, const int *type, const double *mass,
+                             int ntypes, double *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
