@@ -1,9 +1,10 @@
 #!/usr/bin/env python
 """Throughput of the short-range MD step on B200, in Matom-steps/s.
 
-Workload (one bench step = 100 NVE timesteps of the box, continuing the
-trajectory): the EAM configuration -- 32,000 atoms, fcc 20^3, a = 3.615 A,
-synthetic 5000-point setfl tables (lammps_b200/eam_synth.py), Gaussian
+Workload (one bench step = the first 100 NVE timesteps from the seeded
+initial state; restore and Verlet setup are untimed): the EAM
+configuration -- 32,000 atoms, fcc 20^3, a = 3.615 A, synthetic
+5000-point setfl tables (lammps_b200/eam_synth.py), Gaussian
 velocities at 1600 K (seed 376847), dt = 5 fs, skin 1.0 A,
 `neigh_modify every 1 delay 5 check yes`, FP32-mixed precision.  The FP64
 form of the same workload and the 4,000,000-atom LJ configuration (fcc 100^3,
@@ -189,6 +190,26 @@ def load_traffic():
         return {}
 
 
+EAM_BYTES_PER_ATOM_STEP = 200.0   # x, v, f, rho, fp traffic of one EAM step (FP64 state)
+EAM_HALF_PAIRS = 21.0             # half pairs inside 4.95 A per atom on the fcc lattice
+EAM_FLOP_PER_ATOM_STEP = 80.0 * EAM_HALF_PAIRS + 15.0
+
+
+def step_roofline(n, step_ms, hbm_peak, clk):
+    """Whole-step fractions: algorithmic bytes against the measured copy
+    bandwidth and algorithmic FLOPs against the nominal FP32 FMA peak
+    (148 SMs x 128 lanes x 2 FLOP x the sampled maximum SM clock)."""
+    rate = n / (step_ms * 1e-3)  # atom-steps per second
+    mhz = (clk or {}).get("sm_max_mhz") or 1965.0
+    fp32_peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
+    gbs = EAM_BYTES_PER_ATOM_STEP * rate / 1e9
+    tflops = EAM_FLOP_PER_ATOM_STEP * rate / 1e12
+    return {"alg_bytes_per_atom_step": EAM_BYTES_PER_ATOM_STEP, "achieved_gbs": gbs,
+            "hbm_frac": gbs / hbm_peak, "alg_flop_per_atom_step": EAM_FLOP_PER_ATOM_STEP,
+            "achieved_tflops": tflops, "fp32_peak_tflops_nominal": fp32_peak,
+            "fp32_frac": tflops / fp32_peak}
+
+
 def device_time_run(sysm, torch, ext, flush, nsteps, start=None):
     """One bench step: (untimed) restore of the initial state and Verlet
     setup, L2 flush, then `nsteps` NVE steps timed with CUDA events on the
@@ -273,7 +294,7 @@ def cpu_reference(setfl, x, v, hi, seconds=10.0, threads=None):
     t0 = time.perf_counter()
     s.run(5)
     dt5 = time.perf_counter() - t0
-    nsteps = max(5, min(200, int(seconds / max(dt5 / 5, 1e-6))))
+    nsteps = max(5, min(5000, int(seconds / max(dt5 / 5, 1e-6))))
     t0 = time.perf_counter()
     s.run(nsteps)
     dt = time.perf_counter() - t0
@@ -331,6 +352,8 @@ def profile_case(args):
         raise SystemExit(f"unknown case {args.case}")
     if args.eager:
         s.set_graphs(False)
+    if args.tpa:
+        s.set_launch(args.tpa)
     total, per = time_form(s, torch, flush, args.steps, max(args.warmup, 1), (x, v))
     s.set_timing(True)
     ext = torch.cuda.ExternalStream(s.stream)
@@ -353,6 +376,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--eager", action="store_true",
                     help="with --case: launch kernels one by one (for profilers)")
+    ap.add_argument("--tpa", type=int, default=0,
+                    help="with --case: threads per atom of the pair kernels (0 = autotuned)")
     ap.add_argument("--case", default=None,
                     help="profile one form only: eam32k-mixed, eam32k-fp64, lj4m-mixed, lj4m-fp64")
     args = ap.parse_args()
@@ -360,9 +385,9 @@ def main():
         return profile_case(args)
     K, W = args.steps, max(args.warmup, 3)
     ws, rank, local = dist_setup()
-    config = {"workload": "eam-32k fcc 20^3 synthetic setfl, the first 100 NVE steps from the "
-                          "seeded initial state per bench step (configs[1]); also eam Cu_u3 32k "
-                          "(bench/in.eam) and lj-4M fcc 100^3 (configs[4])",
+    config = {"workload": "eam-32k: fcc 20^3 a=3.615, synthetic 5000-point setfl, 1600 K, "
+                          "the first 100 NVE steps from the seeded initial state per bench step; "
+                          "extras: eam Cu_u3 32k (bench/in.eam) and lj-4M fcc 100^3",
               "atoms": 32000, "md_steps_per_step": MD_STEPS, "precision": "mixed",
               "l2": "flushed (256 MB write) before every timed bench step",
               "parallelism": f"replicas x{ws}"}
@@ -436,8 +461,7 @@ def main():
                 "frac": achieved / peak, "traffic": traffic,
                 "kernel": "k_eam_force (mixed)" if dom == "pair2" else "k_eam_rho (mixed)",
                 "kernel_ms": phases[dom], "peak_source": f"{peak_kind} hbm_gbs",
-                "step": {"alg_bytes_per_atom_step": 200.0,
-                         "achieved_gbs": 200.0 * n / (step_ms * 1e-3) / 1e9}}
+                "step": step_roofline(n, step_ms, peak, clk)}
 
     # ---- end to end through the public API --------------------------------
     x_pin = np.ascontiguousarray(x)

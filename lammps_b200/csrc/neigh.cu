@@ -11,7 +11,8 @@
 //   4 k_sort_cells  order each cell by caller index (deterministic order)
 //   5 k_gather      permute x, v, ids; cell-relative FP32 copy; xhold
 //   6 k_copyback    permuted arrays back into the primary buffers
-//   7 k_neigh_full  full list over the 27 neighbor cells (cell >= rc+skin)
+//   7 k_neigh_tiles full list over the 27 neighbor cells (cell >= rc+skin),
+//                   neighbor-cell tiles staged in shared memory
 // The pair test is the reference's, bit for bit: the periodic image is
 // formed as x_j + s*L in FP64 and rsq = dx*dx + dy*dy + dz*dz is rounded
 // after every operation, then compared with `<=` to (rc+skin)^2

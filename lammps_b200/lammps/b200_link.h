@@ -1,0 +1,83 @@
+/* -*- c++ -*- ----------------------------------------------------------
+   B200 package for LAMMPS: the link between LAMMPS's host arrays and one
+   libb200md context (include/b200md.h).
+
+   Every /b200 style of a LAMMPS instance shares one B200Link, which owns the
+   device context (atoms, cell-sorted neighbor list and potential tables on
+   the GPU).  Two ways of driving it:
+
+   - per call (any run style): Pair::compute uploads the owned atoms, builds
+     the list on the device, evaluates forces/energy/virial and copies the
+     forces back into atom->f -- the contract of Pair::compute(eflag,vflag)
+     in src/pair.h:135 with the GPU package's device-neighbor mode as the
+     model (src/GPU/pair_lj_cut_gpu.cpp:97-140);
+   - resident (run_style verlet/b200 with fix nve/b200): the whole run
+     advances on the device through b200_run and host arrays are refreshed
+     only on output steps.
+
+   Limits checked at init: one MPI rank, orthogonal fully periodic box, at
+   most 8 atom types, per-type masses (no rmass).
+------------------------------------------------------------------------- */
+
+#ifndef LMP_B200_LINK_H
+#define LMP_B200_LINK_H
+
+#include "pointers.h"
+
+struct b200_ctx;
+
+namespace LAMMPS_NS {
+
+/* A pair style that can hand its coefficient tables to the device. */
+class B200PairTables {
+ public:
+  virtual ~B200PairTables() {}
+  /* upload the style's tables (after Pair::init) into ctx; returns a
+     B200_* status */
+  virtual int b200_upload_tables(b200_ctx *ctx) = 0;
+  /* B200_PREC_FP64 or B200_PREC_MIXED, from the pair_style keyword */
+  virtual int b200_precision() const = 0;
+};
+
+class B200Link : protected Pointers {
+ public:
+  /* the link of this LAMMPS instance, created on first use; every
+     instance() is paired with one release(), the last one frees it */
+  static B200Link *instance(class LAMMPS *);
+  static void release(class LAMMPS *);
+
+  B200Link(class LAMMPS *);
+  ~B200Link();
+
+  /* check the run can use the device at all (error->all otherwise) */
+  void check_supported(const char *style);
+  /* context with the requested precision on the device chosen by the
+     B200_DEVICE environment variable (default 0) */
+  b200_ctx *context(int precision);
+  /* map a B200_* status to error->all with the library's message */
+  void check(int status, const char *where);
+
+  /* per-call mode: box, neighbor settings and tables, then owned atoms */
+  void sync_settings(B200PairTables *tables);
+  void upload_atoms(int with_velocities);
+  /* per-call Pair::compute: build + forces, energy and virial */
+  void pair_compute(class Pair *pair, int eflag, int vflag);
+
+  /* resident mode: host x, v, f and image flags from the device */
+  void download_state();
+
+  b200_ctx *ctx;
+  int ctx_precision;
+  int tables_dirty;   // tables must be re-uploaded before the next compute
+  int refs;           // styles holding this link
+
+ private:
+  double *fbuf;       // nlocal*3 forces in caller order
+  int *ibuf;          // tags as int, image triplets
+  int nbuf;
+  void grow(int n);
+};
+
+}
+
+#endif

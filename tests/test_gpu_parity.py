@@ -3,7 +3,7 @@
 Bars: neighbor lists bit-exact as sorted per-atom sets of (owner, image);
 FP64 forces within 1e-12 norm-wise relative, energy and virial diagonal
 within 1e-12 relative, virial off-diagonals within 1e-12 of |trace|;
-mixed precision within 1e-5 (force) -- the targets of the north-star spec.
+mixed precision within 1e-5 (force).
 """
 import json
 import os
