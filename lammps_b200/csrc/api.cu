@@ -704,6 +704,10 @@ int b200_set_eam(b200_ctx *c, int ntypes, int nrho, double drho, int nr, double 
     E.type2rhor[i] = (i / ntp1 == 0 || i % ntp1 == 0) ? 0 : type2rhor[i];
     E.type2z2r[i] = (i / ntp1 == 0 || i % ntp1 == 0) ? 0 : type2z2r[i];
   }
+  E.rhor_sym = true;
+  for (int i = 1; i < ntp1; i++)
+    for (int j = 1; j < ntp1; j++)
+      if (E.type2rhor[i * ntp1 + j] != E.type2rhor[j * ntp1 + i]) E.rhor_sym = false;
   // repack [table][knot][7] -> [table][knot][8]; FP32 copies reordered
   // [c3 c4 c5 c6 | c0 c1 c2 0] for one-float4 value / derivative loads
   auto pack = [&](const double *src, int ntab, int nk, double **dd, float **df) -> int {

@@ -71,6 +71,21 @@ __host__ __device__ inline int md_code(int dx, int dy, int dz) {
   return (dx + 1) | ((dy + 1) << 2) | ((dz + 1) << 4);
 }
 #define MD_CODE_SELF 21  // md_code(0, 0, 0)
+// Filler of the unused tail of an atom's last slab: the atom itself at a
+// cell offset of +2 in every dimension (code bits 3), at least
+// sqrt(3) * cell edge > rc + skin away, so a kernel that reads whole slabs
+// rejects it by the cutoff test without checking the count.
+#define MD_CODE_PAD 63
+__host__ __device__ inline int md_pad_entry(int i) { return (int)((unsigned)i | (63u << MD_JBITS)); }
+
+// Cell offset d = bits - 1 (-1, 0, +1; +2 for the pad entry) of an entry
+// along one dimension, as a float, without an integer-to-float conversion:
+// the two code bits become the low mantissa bits of 2^23 (exact), and
+// 2^23 + 1 is subtracted (exact).  d * cell edge is exact for these d, so
+// fmaf(-d, cs, x) rounds once, like x - (d * cs).
+__device__ __forceinline__ float md_code_d(unsigned e, int shift) {
+  return __int_as_float((int)(0x4B000000u | ((e >> shift) & 3u))) - 8388609.0f;
+}
 __host__ __device__ inline void md_entry(unsigned int e, int &j, int &dx, int &dy, int &dz) {
   j = (int)(e & MD_JMASK);
   dx = (int)((e >> MD_JBITS) & 3u) - 1;

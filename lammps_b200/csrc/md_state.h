@@ -28,6 +28,10 @@ struct EAMDev {
   int type2frho[MD_MAXTYPES + 1];
   int type2rhor[(MD_MAXTYPES + 1) * (MD_MAXTYPES + 1)];
   int type2z2r[(MD_MAXTYPES + 1) * (MD_MAXTYPES + 1)];
+  // type2rhor[i][j] == type2rhor[j][i] for every type pair (one element, or
+  // a funcfl/setfl mapping symmetric in the pair): rho'_j(r) of a pair is
+  // then the same spline row as rho'_i(r) and is loaded once
+  bool rhor_sym = false;
 };
 
 // blocks of tables_dev, each TABSZ doubles
@@ -145,9 +149,9 @@ cudaError_t md_eam_compute(b200_ctx *c, bool ev, bool atom_ev, double *eatom, do
                            cudaEvent_t mid = nullptr);
 // ---- integration (integrate.cu) --------------------------------------------
 cudaError_t md_nve_initial(b200_ctx *c, double dtv, double dtf);
+cudaError_t md_decide(b200_ctx *c);
 cudaError_t md_nve_final(b200_ctx *c, double dtf, bool ke);
 cudaError_t md_ke(b200_ctx *c);
-cudaError_t md_decide(b200_ctx *c);
 cudaError_t md_record_row(b200_ctx *c);
 cudaError_t md_zero_ev(b200_ctx *c);
 

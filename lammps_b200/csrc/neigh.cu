@@ -255,12 +255,14 @@ __device__ __forceinline__ void append_entry(int *__restrict__ nlist, int stride
   count++;
 }
 
-// store the last, partly filled slab (its r entries sit at the end of buf)
+// store the last, partly filled slab (its r entries sit at the end of buf;
+// the rest of the slab is filled with the atom's pad entry)
 __device__ __forceinline__ void flush_entries(int *__restrict__ nlist, int stride, int i,
                                               int count, int capacity, const int4 &buf) {
   const int r = count & 3;
   if (r == 0 || count - 1 >= capacity) return;
-  int4 o = make_int4(0, 0, 0, 0);
+  const int pad = md_pad_entry(i);
+  int4 o = make_int4(pad, pad, pad, pad);
   if (r == 1) o.x = buf.w;
   else if (r == 2) { o.x = buf.z; o.y = buf.w; }
   else { o.x = buf.y; o.y = buf.z; o.z = buf.w; }
@@ -282,7 +284,7 @@ __global__ void __launch_bounds__(kNeighThreads) k_neigh_tiles(
     const double4 *__restrict__ x4, const int *__restrict__ cell_start, int *__restrict__ nlist,
     int *__restrict__ numneigh, int *__restrict__ status, const int *flag) {
   if (!rebuild_on(flag)) return;
-  __shared__ float4 sp[kStageCap];
+  __shared__ float4 sp[kStageCap + 32];  // 32 spare slots: a chunk may read past a row
   __shared__ int sj[kStageCap];
   __shared__ int s_start[kStageCells + 1];
   __shared__ int s_src[kStageCells];
@@ -346,10 +348,13 @@ __global__ void __launch_bounds__(kNeighThreads) k_neigh_tiles(
         const int o = s_start[id] + t;
         sp[o] = make_float4((float)(__dadd_rn(p.x, shx) - rx), (float)(__dadd_rn(p.y, shy) - ry),
                             (float)(__dadd_rn(p.z, shz) - rz), __int_as_float((int)p.w));
-        sj[o] = g0 + t;
+        sj[o] = (int)((unsigned)(g0 + t) | ((unsigned)(id % (kTileCells + 2)) << MD_JBITS));
       }
     }
   }
+  // the spare slots after the last staged row: far away, type 1
+  if (staged && threadIdx.x < 32)
+    sp[s_start[kStageCells] + threadIdx.x] = make_float4(1.0e30f, 1.0e30f, 1.0e30f, __int_as_float(1));
   __syncthreads();
   // Warp w owns cell (cx0 + w, cy, cz); each lane takes one of its atoms.
   // The 27 neighbour cells are 9 contiguous staged ranges (3 cells along x
@@ -379,50 +384,51 @@ __global__ void __launch_bounds__(kNeighThreads) k_neigh_tiles(
         for (int dy = -1; dy <= 1; dy++) {
           const int idL = warp + (kTileCells + 2) * ((1 + dy) + 3 * (1 + dz));  // dx = -1
           const int r0 = s_start[idL], r1 = s_start[idL + 3];
-          const int b1 = s_start[idL + 1], b2 = s_start[idL + 2];
+          // entry code of a candidate in staged column sx: dx + 1 = sx - warp
+          const unsigned rowadd = (unsigned)(((dy + 1) << 2) + ((dz + 1) << 4) - warp) << MD_JBITS;
           for (int cb = r0; cb < r1; cb += 32) {
             const int nc = min(32, r1 - cb);
             unsigned acc = 0u, band = 0u;
-            if (SINGLE && nc == 32) {
 #pragma unroll
-              for (int t = 0; t < 32; t++) {
-                const float4 pj = sp[cb + t];
-                const float ddx = pix - pj.x, ddy = piy - pj.y, ddz = piz - pj.z;
-                const float r2 = ddx * ddx + ddy * ddy + ddz * ddz;
-                acc |= (r2 <= hi1) ? (1u << t) : 0u;
-                band |= (r2 >= lo1) ? (1u << t) : 0u;
+            for (int t = 0; t < 32; t++) {
+              const float4 pj = sp[cb + t];
+              const float ddx = pix - pj.x, ddy = piy - pj.y, ddz = piz - pj.z;
+              const float r2 = ddx * ddx + ddy * ddy + ddz * ddz;
+              float lo = lo1, hi = hi1;
+              if (!SINGLE) {
+                const int tt = ti * ntp1 + (__float_as_int(pj.w) & 15);
+                lo = cns_lo[tt];
+                hi = cns_hi[tt];
               }
-            } else {
-              for (int t = 0; t < nc; t++) {
-                const float4 pj = sp[cb + t];
-                const float ddx = pix - pj.x, ddy = piy - pj.y, ddz = piz - pj.z;
-                const float r2 = ddx * ddx + ddy * ddy + ddz * ddz;
-                float lo = lo1, hi = hi1;
-                if (!SINGLE) {
-                  const int tt = ti * ntp1 + __float_as_int(pj.w);
-                  lo = cns_lo[tt];
-                  hi = cns_hi[tt];
-                }
-                acc |= (r2 <= hi) ? (1u << t) : 0u;
-                band |= (r2 >= lo) ? (1u << t) : 0u;
-              }
+              acc |= (r2 <= hi) ? (1u << t) : 0u;
+              band |= (r2 >= lo) ? (1u << t) : 0u;
             }
+            // candidates past the row end are not neighbours
+            acc &= nc == 32 ? 0xffffffffu : ((1u << nc) - 1u);
             if (my_m >= cb && my_m < cb + nc) acc &= ~(1u << (my_m - cb));
             band &= acc;
-            while (acc) {
-              const int t = __ffs(acc) - 1;
-              acc &= acc - 1u;
-              const int m = cb + t;
-              const int j = sj[m];
-              const int dxl = (m >= b1) + (m >= b2);  // staged column of the candidate
-              // inside the FP32 uncertainty band: the reference's FP64 test
-              if (((band >> t) & 1u) &&
-                  !exact_pair(xi, x4[j], s_sh[idL + dxl][0], s_sh[idL + dxl][1],
-                              s_sh[idL + dxl][2],
-                              SINGLE ? cut1 : cns[ti * ntp1 + __float_as_int(sp[m].w)]))
-                continue;
-              append_entry(nlist, stride, i, count, capacity,
-                           j | (md_code(dxl - 1, dy, dz) << MD_JBITS), buf);
+            if (band == 0u) {
+              while (acc) {
+                const int t = __ffs(acc) - 1;
+                acc &= acc - 1u;
+                append_entry(nlist, stride, i, count, capacity,
+                             (int)((unsigned)sj[cb + t] + rowadd), buf);
+              }
+            } else {
+              while (acc) {
+                const int t = __ffs(acc) - 1;
+                acc &= acc - 1u;
+                const int m = cb + t;
+                const unsigned bits = (unsigned)sj[m];
+                // inside the FP32 uncertainty band: the reference's FP64 test
+                if ((band >> t) & 1u) {
+                  const int id = idL - warp + (int)(bits >> MD_JBITS);
+                  if (!exact_pair(xi, x4[bits & MD_JMASK], s_sh[id][0], s_sh[id][1], s_sh[id][2],
+                                  SINGLE ? cut1 : cns[ti * ntp1 + (__float_as_int(sp[m].w) & 15)]))
+                    continue;
+                }
+                append_entry(nlist, stride, i, count, capacity, (int)(bits + rowadd), buf);
+              }
             }
           }
         }

@@ -26,6 +26,7 @@ struct EamArgs {
   BoxGeom box;
   const int *cell, *nlist, *numneigh, *orig;
   int nrho, nr;
+  bool rhor_sym;  // rho'_j spline row == rho'_i spline row for every pair
   double rdr, rdrho, rhomax, cutforcesq;
   const double *frho, *rhor, *z2r;
   const float *rhor_f, *z2r_f;
@@ -54,8 +55,6 @@ __device__ __forceinline__ double pick(const Shift3 &s, int d) {
 __device__ __forceinline__ void decode(unsigned int e, int &j, int &dx, int &dy, int &dz) {
   md_entry(e, j, dx, dy, dz);
 }
-// neighbour-cell centre offset along one dimension (d = -1, 0, +1)
-__device__ __forceinline__ float offf(int d, float cs) { return d < 0 ? -cs : (d > 0 ? cs : 0.f); }
 
 // Embedding F(rho) and F'(rho) of one atom, FP64, reference clamps.
 __device__ __forceinline__ void embed(const EamArgs &a, int itype_frho, double rho, double &fp,
@@ -135,22 +134,19 @@ __global__ void __launch_bounds__(128) k_eam_rho(EamArgs a, const double4 *__res
       const int4 *nl4 = reinterpret_cast<const int4 *>(a.nlist);
       for (int c4 = lane; 4 * c4 < num; c4 += TPA) {
         const int4 e4 = nl4[(size_t)c4 * a.stride + i];
-        const int mm = min(4, num - 4 * c4);
+        // whole slabs: pad entries in the last slab fail the cutoff test
         const unsigned int ee[4] = {(unsigned int)e4.x, (unsigned int)e4.y, (unsigned int)e4.z,
                                     (unsigned int)e4.w};
         float4 xq[4];
 #pragma unroll
-        for (int u = 0; u < 4; u++) xq[u] = xr[u < mm ? (int)(ee[u] & MD_JMASK) : i];
+        for (int u = 0; u < 4; u++) xq[u] = xr[ee[u] & MD_JMASK];
         float crho = 0.f;  // FP32 slab sum, added to the FP64 density
 #pragma unroll
         for (int u = 0; u < 4; u++) {
-          if (u >= mm) break;
-          int j, dx, dy, dz;
-          decode(ee[u], j, dx, dy, dz);
           const float4 xj = xq[u];
-          const float delx = (xi.x - xj.x) - offf(dx, csx);
-          const float dely = (xi.y - xj.y) - offf(dy, csy);
-          const float delz = (xi.z - xj.z) - offf(dz, csz);
+          const float delx = fmaf(-md_code_d(ee[u], MD_JBITS), csx, xi.x - xj.x);
+          const float dely = fmaf(-md_code_d(ee[u], MD_JBITS + 2), csy, xi.y - xj.y);
+          const float delz = fmaf(-md_code_d(ee[u], MD_JBITS + 4), csz, xi.z - xj.z);
           const float rsq = delx * delx + dely * dely + delz * delz;
           if (rsq < cutf) {
             float p = sqrtf(rsq) * rdrf + 1.0f;
@@ -246,8 +242,11 @@ __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__r
           p = fmin(p, 1.0);
           const double *ci = a.rhor + ((size_t)s_t2rhor[ti * a.ntp1 + tj] * (a.nr + 1) + m) * 8;
           const double rhoip = (ci[0] * p + ci[1]) * p + ci[2];
-          const double *cj = a.rhor + ((size_t)s_t2rhor[tj * a.ntp1 + ti] * (a.nr + 1) + m) * 8;
-          const double rhojp = (cj[0] * p + cj[1]) * p + cj[2];
+          double rhojp = rhoip;
+          if (!a.rhor_sym) {
+            const double *cj = a.rhor + ((size_t)s_t2rhor[tj * a.ntp1 + ti] * (a.nr + 1) + m) * 8;
+            rhojp = (cj[0] * p + cj[1]) * p + cj[2];
+          }
           const double *cz2 = a.z2r + ((size_t)s_t2z2r[ti * a.ntp1 + tj] * (a.nr + 1) + m) * 8;
           const double z2p = (cz2[0] * p + cz2[1]) * p + cz2[2];
           const double z2 = ((cz2[3] * p + cz2[4]) * p + cz2[5]) * p + cz2[6];
@@ -281,14 +280,14 @@ __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__r
       const int4 *nl4 = reinterpret_cast<const int4 *>(a.nlist);
       for (int c4 = lane; 4 * c4 < num; c4 += TPA) {
        const int4 e4 = nl4[(size_t)c4 * a.stride + i];
-       const int mm = min(4, num - 4 * c4);
+       // whole slabs: pad entries in the last slab fail the cutoff test
        const unsigned int ee[4] = {(unsigned int)e4.x, (unsigned int)e4.y, (unsigned int)e4.z,
                                    (unsigned int)e4.w};
        float4 xq[4];
        float fpq[4];
 #pragma unroll
        for (int u = 0; u < 4; u++) {
-         const int jj = u < mm ? (int)(ee[u] & MD_JMASK) : i;
+         const int jj = (int)(ee[u] & MD_JMASK);
          xq[u] = xr[jj];
          fpq[u] = a.fpf[jj];
        }
@@ -296,13 +295,10 @@ __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__r
        float cfx = 0.f, cfy = 0.f, cfz = 0.f;
 #pragma unroll
        for (int u = 0; u < 4; u++) {
-        if (u >= mm) break;
-        int j, dx, dy, dz;
-        decode(ee[u], j, dx, dy, dz);
         const float4 xj = xq[u];
-        const float delx = (xi.x - xj.x) - offf(dx, csx);
-        const float dely = (xi.y - xj.y) - offf(dy, csy);
-        const float delz = (xi.z - xj.z) - offf(dz, csz);
+        const float delx = fmaf(-md_code_d(ee[u], MD_JBITS), csx, xi.x - xj.x);
+        const float dely = fmaf(-md_code_d(ee[u], MD_JBITS + 2), csy, xi.y - xj.y);
+        const float delz = fmaf(-md_code_d(ee[u], MD_JBITS + 4), csz, xi.z - xj.z);
         const float rsq = delx * delx + dely * dely + delz * delz;
         if (rsq < cutf) {
           const int tj = __float_as_int(xj.w);
@@ -316,9 +312,12 @@ __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__r
           const float4 ci = *reinterpret_cast<const float4 *>(
               a.rhor_f + ((size_t)s_t2rhor[ti * a.ntp1 + tj] * (a.nr + 1) + m) * 8 + 4);
           const float rhoip = (ci.x * p + ci.y) * p + ci.z;
-          const float4 cj = *reinterpret_cast<const float4 *>(
-              a.rhor_f + ((size_t)s_t2rhor[tj * a.ntp1 + ti] * (a.nr + 1) + m) * 8 + 4);
-          const float rhojp = (cj.x * p + cj.y) * p + cj.z;
+          float rhojp = rhoip;
+          if (!a.rhor_sym) {
+            const float4 cj = *reinterpret_cast<const float4 *>(
+                a.rhor_f + ((size_t)s_t2rhor[tj * a.ntp1 + ti] * (a.nr + 1) + m) * 8 + 4);
+            rhojp = (cj.x * p + cj.y) * p + cj.z;
+          }
           const float *zb = a.z2r_f + ((size_t)s_t2z2r[ti * a.ntp1 + tj] * (a.nr + 1) + m) * 8;
           const float4 zv = *reinterpret_cast<const float4 *>(zb);
           const float4 zd = *reinterpret_cast<const float4 *>(zb + 4);
@@ -424,6 +423,7 @@ cudaError_t md_eam_compute(b200_ctx *c, bool ev, bool atom_ev, double *eatom, do
   a.orig = c->orig;
   a.nrho = c->eam.nrho;
   a.nr = c->eam.nr;
+  a.rhor_sym = c->eam.rhor_sym;
   a.rdr = c->eam.rdr;
   a.rdrho = c->eam.rdrho;
   a.rhomax = c->eam.rhomax;

@@ -50,8 +50,6 @@ __device__ __forceinline__ double pick(const Shift3 &s, int d) {
 __device__ __forceinline__ void decode(unsigned int e, int &j, int &dx, int &dy, int &dz) {
   md_entry(e, j, dx, dy, dz);
 }
-// neighbour-cell centre offset along one dimension (d = -1, 0, +1)
-__device__ __forceinline__ float offf(int d, float cs) { return d < 0 ? -cs : (d > 0 ? cs : 0.f); }
 
 template <int TPA, bool EV, bool ATOM, bool SINGLE>
 __global__ void __launch_bounds__(128) k_lj_fp64(PairArgs a, const double4 *__restrict__ x4) {
@@ -191,26 +189,25 @@ __global__ void __launch_bounds__(128) k_lj_mixed(PairArgs a, const float4 *__re
     const float csx = (float)a.box.cs[0], csy = (float)a.box.cs[1], csz = (float)a.box.cs[2];
     const int num = a.numneigh[i];
     const int4 *nl4 = reinterpret_cast<const int4 *>(a.nlist);
+    // whole slabs: the tail of the last slab holds pad entries, which the
+    // cutoff test rejects, so no per-entry count check is needed
     for (int c4 = lane; 4 * c4 < num; c4 += TPA) {
       const int4 e4 = nl4[(size_t)c4 * a.stride + i];
-      const int m = min(4, num - 4 * c4);
       const unsigned int ee[4] = {(unsigned int)e4.x, (unsigned int)e4.y, (unsigned int)e4.z,
                                   (unsigned int)e4.w};
       float4 xj[4];
 #pragma unroll
-      for (int u = 0; u < 4; u++) xj[u] = xr[u < m ? (int)(ee[u] & MD_JMASK) : i];
-      // the (at most four) pair forces of a slab are summed in FP32, the
-      // slab sum is added to the atom's FP64 accumulator
+      for (int u = 0; u < 4; u++) xj[u] = xr[ee[u] & MD_JMASK];
+      // the four pair forces of a slab are summed in FP32, the slab sum is
+      // added to the atom's FP64 accumulator
       float cfx = 0.f, cfy = 0.f, cfz = 0.f;
 #pragma unroll
       for (int u = 0; u < 4; u++) {
-        if (u >= m) break;
-        int j, dx, dy, dz;
-        decode(ee[u], j, dx, dy, dz);
-        // x_i - (x_j + image shift) = (xr_i - xr_j) - (neighbour cell centre - own cell centre)
-        const float delx = (xi.x - xj[u].x) - offf(dx, csx);
-        const float dely = (xi.y - xj[u].y) - offf(dy, csy);
-        const float delz = (xi.z - xj[u].z) - offf(dz, csz);
+        // x_i - (x_j + image shift) = (xr_i - xr_j) - d * cell edge, with d
+        // the offset of the neighbour's cell from the atom's cell
+        const float delx = fmaf(-md_code_d(ee[u], MD_JBITS), csx, xi.x - xj[u].x);
+        const float dely = fmaf(-md_code_d(ee[u], MD_JBITS + 2), csy, xi.y - xj[u].y);
+        const float delz = fmaf(-md_code_d(ee[u], MD_JBITS + 4), csz, xi.z - xj[u].z);
         const float rsq = delx * delx + dely * dely + delz * delz;
         const int tt = ti * a.ntp1 + __float_as_int(xj[u].w);
         const float cs = SINGLE ? cutsq1 : tabf[0 * nt2 + tt];
@@ -225,18 +222,18 @@ __global__ void __launch_bounds__(128) k_lj_mixed(PairArgs a, const float4 *__re
           cfy += dely * fpair;
           cfz += delz * fpair;
           if (EV) {
-            const float c3 = SINGLE ? lj3 : tabf[3 * nt2 + tt];
-            const float c4 = SINGLE ? lj4 : tabf[4 * nt2 + tt];
-            const float co = SINGLE ? off : tabf[5 * nt2 + tt];
-            const float evdwl = r6inv * (c3 * r6inv - c4) - co;
-            acc[0] += 0.5 * (double)evdwl;
-            const float hf = 0.5f * fpair;
-            acc[1] += (double)(delx * delx * hf);
-            acc[2] += (double)(dely * dely * hf);
-            acc[3] += (double)(delz * delz * hf);
-            acc[4] += (double)(delx * dely * hf);
-            acc[5] += (double)(delx * delz * hf);
-            acc[6] += (double)(dely * delz * hf);
+          const float c3 = SINGLE ? lj3 : tabf[3 * nt2 + tt];
+          const float c4 = SINGLE ? lj4 : tabf[4 * nt2 + tt];
+          const float co = SINGLE ? off : tabf[5 * nt2 + tt];
+          const float evdwl = r6inv * (c3 * r6inv - c4) - co;
+          acc[0] += 0.5 * (double)evdwl;
+          const float hf = 0.5f * fpair;
+          acc[1] += (double)(delx * delx * hf);
+          acc[2] += (double)(dely * dely * hf);
+          acc[3] += (double)(delz * delz * hf);
+          acc[4] += (double)(delx * dely * hf);
+          acc[5] += (double)(delx * delz * hf);
+          acc[6] += (double)(dely * delz * hf);
           }
         }
       }
