@@ -508,6 +508,16 @@ def main():
         extras["lj_4M"] = lj
 
     if not args.no_extras:
+        from lammps_b200.forcematch import force_matching_case, gradient_check
+        fm = force_matching_case()
+        rng = np.random.default_rng(99)
+        eps0 = fm["eps"] * (1 + 0.08 * rng.standard_normal(3))
+        sig0 = fm["sigma"] * (1 + 0.02 * rng.standard_normal(3))
+        extras["force_matching_8k"] = gradient_check(fm, eps0, sig0, device=DEVICE)
+        extras["force_matching_8k"]["note"] = (
+            "2-type lj/cut, 8000 atoms, 10x10x20 fcc rho*=0.85 + 0.05 jitter; errors of "
+            "dL/d(eps,sigma) vs FP64 central differences (h=1e-5, cutoffs held) relative to "
+            "the largest component, and of dL/dx along 8 unit directions relative to |dL/dx|")
         extras["mixed_force_error"] = {
             "eam_32k": mixed_error(lambda prec: make_eam32k(prec, setfl, x, v, hi)),
             "lj_4M": mixed_error(lambda prec: make_lj(prec, x4, v4, hi4)),

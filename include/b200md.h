@@ -193,6 +193,29 @@ long long b200_kernel_launches(const b200_ctx *ctx);
 /* CUDA stream of the context, as a void* (cudaStream_t). */
 void *b200_stream(const b200_ctx *ctx);
 
+/* ---- differentiable force matching (pair_style lj/cut) ------------------- */
+
+/* No counterpart in the reference: gradients of a force-matching loss for
+   lj/cut with up to 4 atom types.  The context holds the atoms and the list
+   (b200_set_lj with the cutoffs to use, b200_upload_atoms, b200_neigh_build).
+   lj1, lj2 and cutsq are host (ntypes+1)^2 tables as in b200_set_lj;
+   x, f, g and gx are DEVICE arrays of 3n doubles in the caller's atom order.
+   Each call returns after its kernels have finished.
+
+   Replace the positions (device array) and rebuild the list. */
+int b200_adj_set_positions(b200_ctx *ctx, const double *x);
+/* F_i = sum_j phi(r_ij) (x_i - x_j), phi = (lj1 r^-6 - lj2) r^-8 inside
+   cutsq (PairLJCut::compute's pair force, src/pair_lj_cut.cpp:100-113);
+   FP32 pair math with FP64 sums for a B200_PREC_MIXED context, FP64
+   otherwise.  Each cutsq entry must lie within the list's cutoff. */
+int b200_adj_forces(b200_ctx *ctx, const double *lj1, const double *lj2, const double *cutsq,
+                    double *f);
+/* Given g = dL/dF: gx = dL/dx (the Hessian-vector product of the forces
+   with g) and glj1, glj2 = dL/dlj1, dL/dlj2 per type pair (host,
+   (ntypes+1)^2; the cutoff itself is held fixed). */
+int b200_adj_backward(b200_ctx *ctx, const double *lj1, const double *lj2, const double *cutsq,
+                      const double *g, double *gx, double *glj1, double *glj2);
+
 /* ---- allocation-free entry point -------------------------------------------- */
 
 /* No counterpart in the reference.  Sum over n atoms of

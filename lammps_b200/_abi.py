@@ -55,6 +55,9 @@ SIGNATURES = {
     "b200_set_graphs": (C.c_int, [_vp, C.c_int]),
     "b200_get_timing": (C.c_int, [_vp, _dp, C.POINTER(C.c_longlong), C.c_int]),
     "b200_stream": (_vp, [_vp]),
+    "b200_adj_set_positions": (C.c_int, [_vp, _vp]),
+    "b200_adj_forces": (C.c_int, [_vp, _dp, _dp, _dp, _vp]),
+    "b200_adj_backward": (C.c_int, [_vp, _dp, _dp, _dp, _vp, _vp, _dp, _dp]),
     "b200_kinetic_sum_noalloc": (C.c_int, [C.c_int, _vp, _vp, _vp, C.c_int, _vp, _vp]),
 }
 

@@ -577,6 +577,7 @@ int b200_destroy(b200_ctx *c) {
   dfree(c->cell_count); dfree(c->cell_start); dfree(c->scan_tmp);
   dfree(c->slot); dfree(c->perm); dfree(c->cell_tmp);
   dfree(c->nlist); dfree(c->numneigh); dfree(c->partial); dfree(c->counter); dfree(c->ev);
+  dfree(c->adj_gs); dfree(c->adj_gtab);
   dfree(c->status); dfree(c->rows); dfree(c->tables_dev);
   dfree(c->snap_x4); dfree(c->snap_xhold); dfree(c->snap_v); dfree(c->snap_f);
   dfree(c->snap_orig); dfree(c->snap_image); dfree(c->snap_cell); dfree(c->snap_xr);
@@ -1195,3 +1196,76 @@ int b200_get_timing(b200_ctx *c, double *phase_ms, long long *steps, int reset) 
 void *b200_stream(const b200_ctx *c) { return c ? (void *)c->stream : nullptr; }
 
 }  // extern "C"
+
+// ---- force matching --------------------------------------------------------
+
+namespace {
+int adj_check(b200_ctx *c, const double *lj1, const double *lj2, const double *cutsq) {
+  if (!c || !lj1 || !lj2 || !cutsq) return B200_ERR_ARG;
+  if (c->pstyle != B200_PAIR_LJ_CUT) return set_err(c, B200_ERR_STATE, "force matching needs lj/cut");
+  if (c->ntypes > MD_ADJ_MAXTYPES)
+    return set_err(c, B200_ERR_ARG, "force matching supports at most %d types", MD_ADJ_MAXTYPES);
+  if (!c->sorted_once) return set_err(c, B200_ERR_STATE, "neighbor list not built");
+  const int w = c->ntypes + 1;
+  for (int a = 1; a <= c->ntypes; a++)
+    for (int b = 1; b <= c->ntypes; b++) {
+      const double cs = cutsq[a * w + b];
+      if (!(cs >= 0.0) || cs > c->cutneighsq[a * w + b])
+        return set_err(c, B200_ERR_ARG,
+                       "cutoff of types %d,%d beyond the neighbor list (set_lj, then build)", a, b);
+    }
+  CK(cudaSetDevice(c->device));
+  return B200_OK;
+}
+}  // namespace
+
+int b200_adj_set_positions(b200_ctx *c, const double *x) {
+  if (!c || !x) return B200_ERR_ARG;
+  if (!c->have_atoms) return set_err(c, B200_ERR_STATE, "no atoms uploaded");
+  CK(cudaSetDevice(c->device));
+  CK(md_adj_positions(c, x));
+  int rc = prepare(c);
+  if (rc) return rc;
+  rc = rebuild_sync(c);
+  if (rc) return rc;
+  c->sorted_once = true;
+  return B200_OK;
+}
+
+int b200_adj_forces(b200_ctx *c, const double *lj1, const double *lj2, const double *cutsq,
+                    double *f) {
+  int rc = adj_check(c, lj1, lj2, cutsq);
+  if (rc) return rc;
+  if (!f) return set_err(c, B200_ERR_ARG, "null force array");
+  CK(md_adj_forward(c, lj1, lj2, cutsq, f));
+  CK(cudaStreamSynchronize(c->stream));
+  return B200_OK;
+}
+
+int b200_adj_backward(b200_ctx *c, const double *lj1, const double *lj2, const double *cutsq,
+                      const double *g, double *gx, double *glj1, double *glj2) {
+  int rc = adj_check(c, lj1, lj2, cutsq);
+  if (rc) return rc;
+  if (!g || !gx) return set_err(c, B200_ERR_ARG, "null gradient array");
+  if (c->adj_n < c->n) {
+    CK(dalloc(&c->adj_gs, 3 * (size_t)c->stride));
+    c->adj_n = c->stride;
+  }
+  if (!c->adj_gtab) CK(dalloc(&c->adj_gtab, 2 * MD_ADJ_MAXTYPES * MD_ADJ_MAXTYPES));
+  CK(md_adj_backward(c, lj1, lj2, cutsq, g, gx, c->adj_gs, c->adj_gtab));
+  double h[2 * MD_ADJ_MAXTYPES * MD_ADJ_MAXTYPES];
+  CK(cudaMemcpyAsync(h, c->adj_gtab, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  const int w = c->ntypes + 1;
+  for (int k = 0; k < w * w; k++) {
+    if (glj1) glj1[k] = 0.0;
+    if (glj2) glj2[k] = 0.0;
+  }
+  for (int a = 1; a <= c->ntypes; a++)
+    for (int b = 1; b <= c->ntypes; b++) {
+      const int p = (a - 1) * c->ntypes + (b - 1);
+      if (glj1) glj1[a * w + b] = h[2 * p];
+      if (glj2) glj2[a * w + b] = h[2 * p + 1];
+    }
+  return B200_OK;
+}

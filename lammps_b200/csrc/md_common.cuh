@@ -17,6 +17,7 @@
 #include <stdint.h>
 
 #define MD_MAXTYPES 8
+#define MD_ADJ_MAXTYPES 4  // types of the force-matching adjoint (16 type pairs)
 #define MD_JBITS 26
 #define MD_JMASK ((1u << MD_JBITS) - 1u)
 #define MD_MAX_ATOMS ((int)MD_JMASK)
@@ -77,6 +78,21 @@ __host__ __device__ inline int md_code(int dx, int dy, int dz) {
 // rejects it by the cutoff test without checking the count.
 #define MD_CODE_PAD 63
 __host__ __device__ inline int md_pad_entry(int i) { return (int)((unsigned)i | (63u << MD_JBITS)); }
+
+// Periodic shift of a neighbour in the cell at offset d (-1, 0, +1) from
+// cell c along one dimension: -prd / +prd when that cell wraps, else 0
+struct Shift3 {
+  double m, p;
+};
+__device__ __forceinline__ Shift3 shifts(int c, int nc, double prd) {
+  Shift3 s;
+  s.m = (c - 1 < 0) ? -prd : 0.0;
+  s.p = (c + 1 >= nc) ? prd : 0.0;
+  return s;
+}
+__device__ __forceinline__ double pick(const Shift3 &s, int d) {
+  return d < 0 ? s.m : (d > 0 ? s.p : 0.0);
+}
 
 // Cell offset d = bits - 1 (-1, 0, +1; +2 for the pad entry) of an entry
 // along one dimension, as a float, without an integer-to-float conversion:

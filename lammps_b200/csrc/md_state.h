@@ -104,6 +104,9 @@ struct b200_ctx {
   double *partial = nullptr;     // per-block partial sums
   int partial_blocks = 0;
   unsigned int *counter = nullptr;
+  double *adj_gs = nullptr;    // force-matching scratch: G in the sorted order
+  double *adj_gtab = nullptr;  // force-matching parameter gradients
+  int adj_n = 0;
   double *ev = nullptr;          // [0] eng, [1..6] virial, [7] sum m v^2
   int *status = nullptr;         // ST_* words
   int *status_host = nullptr;    // pinned mirror
@@ -154,6 +157,17 @@ cudaError_t md_nve_final(b200_ctx *c, double dtf, bool ke);
 cudaError_t md_ke(b200_ctx *c);
 cudaError_t md_record_row(b200_ctx *c);
 cudaError_t md_zero_ev(b200_ctx *c);
+
+// ---- force-matching adjoint (adjoint.cu) ------------------------------------
+// lj1, lj2, cutsq: host (ntypes+1)^2 tables; f, g, gx: device, 3n doubles in
+// the caller's order; gs: device scratch of 3n doubles; gtab: device, 2 *
+// MD_ADJ_MAXTYPES^2 doubles (dL/dlj1, dL/dlj2 per type pair)
+cudaError_t md_adj_forward(b200_ctx *c, const double *lj1, const double *lj2, const double *cutsq,
+                           double *f);
+cudaError_t md_adj_backward(b200_ctx *c, const double *lj1, const double *lj2,
+                            const double *cutsq, const double *g, double *gx, double *gs,
+                            double *gtab);
+cudaError_t md_adj_positions(b200_ctx *c, const double *x);
 
 inline int md_blocks(long long work, int block) {
   return (int)((work + block - 1) / block);

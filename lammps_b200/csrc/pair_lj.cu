@@ -34,19 +34,6 @@ struct PairArgs {
   double *eatom, *vatom;
 };
 
-// per-atom periodic shifts for cell offsets -1, 0, +1 along one dimension
-struct Shift3 {
-  double m, p;
-};
-__device__ __forceinline__ Shift3 shifts(int c, int nc, double prd) {
-  Shift3 s;
-  s.m = (c - 1 < 0) ? -prd : 0.0;
-  s.p = (c + 1 >= nc) ? prd : 0.0;
-  return s;
-}
-__device__ __forceinline__ double pick(const Shift3 &s, int d) {
-  return d < 0 ? s.m : (d > 0 ? s.p : 0.0);
-}
 __device__ __forceinline__ void decode(unsigned int e, int &j, int &dx, int &dy, int &dz) {
   md_entry(e, j, dx, dy, dz);
 }
