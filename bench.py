@@ -303,6 +303,38 @@ def cpu_reference(setfl, x, v, hi, seconds=10.0, threads=None):
                        f"{dt:.1f} s")
 
 
+def replica_bench(prec, batch, torch, steps=1000, lat_steps=200):
+    """Batched replicas: replica-steps/s over `steps` NVE steps of every
+    replica (graph replay, events on the engine stream), then the device time
+    of each of `lat_steps` steps with phase events on (p50 / p99)."""
+    from lammps_b200.replicas import make_batch
+    s = make_batch(batch, prec, device=DEVICE)
+    s.setup()
+    s.run(40)
+    ext = torch.cuda.ExternalStream(s.stream)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(ext)
+    s.run(steps)
+    e1.record(ext)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    s.set_timing(True)
+    s.run(20)
+    s.step_times(reset=True)
+    s.run(lat_steps)
+    st = s.step_times(reset=True)
+    s.set_timing(False)
+    nrep = len(batch["natoms"])
+    out = {"replica_steps_per_s": nrep * steps / (ms * 1e-3),
+           "matom_steps_per_s": float(batch["natoms"].sum()) * steps / (ms * 1e3),
+           "ms_per_step": ms / steps, "launch": s.launch(),
+           "step_ms_p50": float(np.percentile(st, 50)), "step_ms_p99": float(np.percentile(st, 99))}
+    s.close()
+    return out
+
+
 def dist_setup():
     import torch
     ws = int(os.environ.get("WORLD_SIZE", "1"))
@@ -348,6 +380,11 @@ def profile_case(args):
     elif work == "lj4m":
         x, v, hi = lj4m_inputs()
         s = make_lj(prec, x, v, hi)
+    elif work == "c3":
+        from lammps_b200.replicas import make_batch, replica_batch
+        batch = replica_batch(nrep=256)
+        x, v = batch["x"], batch["v"]
+        s = make_batch(batch, prec)
     else:
         raise SystemExit(f"unknown case {args.case}")
     if args.eager:
@@ -379,7 +416,8 @@ def main():
     ap.add_argument("--tpa", type=int, default=0,
                     help="with --case: threads per atom of the pair kernels (0 = autotuned)")
     ap.add_argument("--case", default=None,
-                    help="profile one form only: eam32k-mixed, eam32k-fp64, lj4m-mixed, lj4m-fp64")
+                    help="profile one form only: eam32k-mixed, eam32k-fp64, lj4m-mixed, lj4m-fp64, "
+                         "c3-mixed, c3-fp64 (256 replicas)")
     args = ap.parse_args()
     if args.case:
         return profile_case(args)
@@ -508,6 +546,18 @@ def main():
         extras["lj_4M"] = lj
 
     if not args.no_extras:
+        from lammps_b200.replicas import replica_batch
+        batch = replica_batch(nrep=256)
+        rep = {"replicas": 256, "atoms": int(batch["natoms"].sum()),
+               "natoms_min": int(batch["natoms"].min()), "natoms_max": int(batch["natoms"].max()),
+               "steps": 1000, "note": "256 fcc LJ boxes, 4n^3 atoms with n = 5..12 from log-uniform "
+                                      "500-8000, rho* U(0.70,0.95), T* U(0.8,2.0), rc 2.5 skin 0.3 "
+                                      "every 20; one set of launches per step for all replicas; "
+                                      "p50/p99 with phase events recorded in the step graphs"}
+        for prec in ("mixed", "fp64"):
+            rep[prec] = replica_bench(prec, batch, torch)
+        rep["mixed_over_fp64"] = rep["mixed"]["replica_steps_per_s"] / rep["fp64"]["replica_steps_per_s"]
+        extras["replicas_256"] = rep
         from lammps_b200.forcematch import force_matching_case, gradient_check
         fm = force_matching_case()
         rng = np.random.default_rng(99)

@@ -187,11 +187,36 @@ int b200_set_timing(b200_ctx *ctx, int on);
    schedule and give identical results. */
 int b200_set_graphs(b200_ctx *ctx, int on);
 int b200_get_timing(b200_ctx *ctx, double phase_ms[5], long long *steps, int reset);
+/* Device time of every step timed since the last reset (milliseconds, from
+   the step's first phase event to its last; timing must be on): *count
+   receives the number of steps, at most cap are written. */
+int b200_get_step_times(b200_ctx *ctx, double *ms, int cap, int *count, int reset);
 /* Kernel launches issued by the context since creation (for accounting);
    kernels replayed inside step graphs are counted per replay. */
 long long b200_kernel_launches(const b200_ctx *ctx);
 /* CUDA stream of the context, as a void* (cudaStream_t). */
 void *b200_stream(const b200_ctx *ctx);
+
+/* ---- batched replicas ---------------------------------------------------- */
+
+/* No counterpart in the reference (which runs one box per process): make the
+   context hold nrep independent orthogonal periodic boxes, replica r with
+   natoms[r] atoms in the box lo[3r..3r+2], hi[3r..3r+2] (Domain boxlo/boxhi
+   per replica).  Replaces b200_set_box; the next b200_upload_atoms takes the
+   replicas' atoms concatenated in replica order (sum natoms atoms).  All
+   replicas share the pair style (lj/cut), masses, neighbor settings and
+   timestep, and b200_setup / b200_run advance them together -- each kernel
+   covers every replica, each atom and each cell tile knowing its own box.
+   The thermo rows of b200_run then sum over all replicas; per-replica rows
+   come from b200_replica_thermo. */
+int b200_set_replicas(b200_ctx *ctx, int nrep, const int *natoms, const double *lo,
+                      const double *hi);
+int b200_replica_count(const b200_ctx *ctx);
+/* Per-replica thermo of the current positions and velocities (forces are
+   recomputed with per-atom energy and virial): rows[9r..9r+8] =
+   {natoms, sum m v^2, eng_vdwl, virial[0..5]}, from which Temp, E_pair and
+   Press of replica r follow as for b200_run's rows. */
+int b200_replica_thermo(b200_ctx *ctx, double *rows);
 
 /* ---- differentiable force matching (pair_style lj/cut) ------------------- */
 

@@ -55,6 +55,10 @@ SIGNATURES = {
     "b200_set_graphs": (C.c_int, [_vp, C.c_int]),
     "b200_get_timing": (C.c_int, [_vp, _dp, C.POINTER(C.c_longlong), C.c_int]),
     "b200_stream": (_vp, [_vp]),
+    "b200_get_step_times": (C.c_int, [_vp, _dp, C.c_int, _ip, C.c_int]),
+    "b200_set_replicas": (C.c_int, [_vp, C.c_int, _ip, _dp, _dp]),
+    "b200_replica_count": (C.c_int, [_vp]),
+    "b200_replica_thermo": (C.c_int, [_vp, _dp]),
     "b200_adj_set_positions": (C.c_int, [_vp, _vp]),
     "b200_adj_forces": (C.c_int, [_vp, _dp, _dp, _dp, _vp]),
     "b200_adj_backward": (C.c_int, [_vp, _dp, _dp, _dp, _vp, _vp, _dp, _dp]),

@@ -130,6 +130,89 @@ int check_ready(b200_ctx *c) {
   if (!c->have_atoms) return set_err(c, B200_ERR_STATE, "no atoms uploaded");
   if (c->pstyle == B200_PAIR_NONE) return set_err(c, B200_ERR_STATE, "no pair style set");
   if (!c->mass_set) return set_err(c, B200_ERR_STATE, "masses not set");
+  if (c->nrep && c->rep_atom_start[c->nrep] != c->n)
+    return set_err(c, B200_ERR_STATE, "replica atom counts sum to %d, %d atoms uploaded",
+                   c->rep_atom_start[c->nrep], c->n);
+  if (c->nrep && c->pstyle != B200_PAIR_LJ_CUT)
+    return set_err(c, B200_ERR_STATE, "replicas run pair_style lj/cut");
+  return B200_OK;
+}
+
+// The cell grid of one periodic box for neighbor cutoff cutneighmax: cells
+// at least cutneighmax wide, one periodic image per side
+// (CommBrick::setup, src/comm_brick.cpp:128-170).
+int box_cells(b200_ctx *c, BoxGeom &b, long long *ncells) {
+  *ncells = 1;
+  for (int d = 0; d < 3; d++) {
+    int maxneed = (int)(c->cutneighmax * 1 / b.prd[d]) + 1;
+    if (maxneed != 1)
+      return set_err(c, B200_ERR_BOX, "box edge %g in dim %d is not larger than the ghost cutoff %g",
+                     b.prd[d], d, c->cutneighmax);
+    int nc = (int)(b.prd[d] / c->cutneighmax);
+    if (nc < 1) nc = 1;
+    if (nc > MD_MAX_CELLS_DIM - 1) nc = MD_MAX_CELLS_DIM - 1;
+    b.ncell[d] = nc;
+    b.cs[d] = b.prd[d] / nc;
+    b.cinv[d] = nc / b.prd[d];
+    *ncells *= nc;
+  }
+  return B200_OK;
+}
+
+// Cell grids, cell and builder-tile offsets of every replica, and their
+// device copies (b200_set_replicas).
+int init_replica_cells(b200_ctx *c) {
+  const int R = c->nrep;
+  c->rep_cell_base.assign(R, 0);
+  c->rep_tile_base.assign(R + 1, 0);
+  long long cells = 0, tiles = 0;
+  for (int r = 0; r < R; r++) {
+    long long nc = 0;
+    int rc = box_cells(c, c->rep_box[r], &nc);
+    if (rc) return set_err(c, rc, "replica %d: %s", r, c->err.c_str());
+    c->rep_cell_base[r] = (int)cells;
+    c->rep_tile_base[r] = (int)tiles;
+    cells += nc;
+    const BoxGeom &b = c->rep_box[r];
+    tiles += (long long)((b.ncell[0] + MD_TILE_CELLS - 1) / MD_TILE_CELLS) * b.ncell[1] * b.ncell[2];
+  }
+  c->rep_tile_base[R] = (int)tiles;
+  if (cells > (long long)4096 * 4096 - 1 || tiles > 0x7fffffffLL)
+    return set_err(c, B200_ERR_ARG, "too many cells (%lld)", cells);
+  if ((int)cells != c->ncells || (int)tiles != c->ntiles) invalidate_graphs(c);
+  c->ncells = (int)cells;
+  c->ntiles = (int)tiles;
+  c->box = c->rep_box[0];
+  std::vector<int> tile_rep(tiles), rep_of_atom(c->n);
+  for (int r = 0; r < R; r++) {
+    for (int t = c->rep_tile_base[r]; t < c->rep_tile_base[r + 1]; t++) tile_rep[t] = r;
+    for (int i = c->rep_atom_start[r]; i < c->rep_atom_start[r + 1]; i++) rep_of_atom[i] = r;
+  }
+  if (c->rep_dev_r < R) {
+    CK(dalloc(&c->d_rep_box, (size_t)R));
+    CK(dalloc(&c->d_rep_cell_base, (size_t)R));
+    CK(dalloc(&c->d_rep_tile_base, (size_t)R + 1));
+    c->rep_dev_r = R;
+    invalidate_graphs(c);
+  }
+  if (c->rep_dev_tiles < (int)tiles) {
+    CK(dalloc(&c->d_tile_rep, (size_t)tiles));
+    c->rep_dev_tiles = (int)tiles;
+    invalidate_graphs(c);
+  }
+  if (c->rep_dev_n < c->n) {
+    CK(dalloc(&c->d_rep_of_atom, (size_t)c->n));
+    c->rep_dev_n = c->n;
+    invalidate_graphs(c);
+  }
+  CK(cudaMemcpy(c->d_rep_box, c->rep_box.data(), R * sizeof(BoxGeom), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_rep_cell_base, c->rep_cell_base.data(), R * sizeof(int),
+                cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_rep_tile_base, c->rep_tile_base.data(), (R + 1) * sizeof(int),
+                cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_tile_rep, tile_rep.data(), tiles * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_rep_of_atom, rep_of_atom.data(), c->n * sizeof(int),
+                cudaMemcpyHostToDevice));
   return B200_OK;
 }
 
@@ -157,6 +240,7 @@ int init_cutoffs_and_cells(b200_ctx *c) {
       if (cutoff > c->cutforce_max) c->cutforce_max = cutoff;
     }
   if (!(c->cutneighmax > 0.0)) return set_err(c, B200_ERR_ARG, "zero neighbor cutoff");
+  if (c->nrep) return init_replica_cells(c);
   long long ncells = 1;
   for (int d = 0; d < 3; d++) {
     // CommBrick::setup needs one periodic image per side: cutghost < prd
@@ -241,8 +325,12 @@ int alloc_list(b200_ctx *c, int capacity) {
 }
 
 int default_capacity(const b200_ctx *c) {
-  const double vol = c->box.prd[0] * c->box.prd[1] * c->box.prd[2];
-  const double dens = c->n / vol;
+  double dens = c->n / (c->box.prd[0] * c->box.prd[1] * c->box.prd[2]);
+  for (int r = 0; r < c->nrep; r++) {
+    const BoxGeom &b = c->rep_box[r];
+    const double d = c->rep_natoms[r] / (b.prd[0] * b.prd[1] * b.prd[2]);
+    dens = r == 0 ? d : (d > dens ? d : dens);
+  }
   const double pi = 3.14159265358979323846;
   const double expect = 4.0 / 3.0 * pi * c->cutneighmax * c->cutneighmax * c->cutneighmax * dens;
   int cap = (int)(2.0 * expect + 64.0);
@@ -578,6 +666,8 @@ int b200_destroy(b200_ctx *c) {
   dfree(c->slot); dfree(c->perm); dfree(c->cell_tmp);
   dfree(c->nlist); dfree(c->numneigh); dfree(c->partial); dfree(c->counter); dfree(c->ev);
   dfree(c->adj_gs); dfree(c->adj_gtab);
+  dfree(c->d_rep_box); dfree(c->d_rep_of_atom); dfree(c->d_rep_cell_base); dfree(c->d_tile_rep);
+  dfree(c->d_rep_tile_base); dfree(c->rep_eatom); dfree(c->rep_vatom); dfree(c->rep_rows);
   dfree(c->status); dfree(c->rows); dfree(c->tables_dev);
   dfree(c->snap_x4); dfree(c->snap_xhold); dfree(c->snap_v); dfree(c->snap_f);
   dfree(c->snap_orig); dfree(c->snap_image); dfree(c->snap_cell); dfree(c->snap_xr);
@@ -1057,6 +1147,9 @@ int b200_run(b200_ctx *c, int nsteps, double dt, double ftm2v, int thermo_every,
           CK(cudaEventElapsedTime(&ms, c->ev_pool[base + k], c->ev_pool[base + k + 1]));
           c->phase_ms[k] += ms;
         }
+        float step = 0.f;
+        CK(cudaEventElapsedTime(&step, c->ev_pool[base], c->ev_pool[base + MD_NPHASE]));
+        c->step_ms.push_back(step);
       }
       c->phase_steps += s_end - s + 1;
     }
@@ -1195,6 +1288,16 @@ int b200_get_timing(b200_ctx *c, double *phase_ms, long long *steps, int reset) 
 
 void *b200_stream(const b200_ctx *c) { return c ? (void *)c->stream : nullptr; }
 
+int b200_get_step_times(b200_ctx *c, double *ms, int cap, int *count, int reset) {
+  if (!c) return B200_ERR_ARG;
+  const int n = (int)c->step_ms.size();
+  if (count) *count = n;
+  if (ms)
+    for (int k = 0; k < n && k < cap; k++) ms[k] = c->step_ms[k];
+  if (reset) c->step_ms.clear();
+  return B200_OK;
+}
+
 }  // extern "C"
 
 // ---- force matching --------------------------------------------------------
@@ -1268,4 +1371,65 @@ int b200_adj_backward(b200_ctx *c, const double *lj1, const double *lj2, const d
       if (glj2) glj2[a * w + b] = h[2 * p + 1];
     }
   return B200_OK;
+}
+
+// ---- replicas --------------------------------------------------------------
+
+int b200_set_replicas(b200_ctx *c, int nrep, const int *natoms, const double *lo,
+                      const double *hi) {
+  if (!c || nrep < 1 || !natoms || !lo || !hi) return B200_ERR_ARG;
+  long long total = 0;
+  for (int r = 0; r < nrep; r++) {
+    if (natoms[r] < 1) return set_err(c, B200_ERR_ARG, "replica %d has no atoms", r);
+    for (int d = 0; d < 3; d++)
+      if (!(hi[3 * r + d] > lo[3 * r + d]))
+        return set_err(c, B200_ERR_ARG, "replica %d: box hi <= lo in dim %d", r, d);
+    total += natoms[r];
+  }
+  if (total > MD_MAX_ATOMS) return set_err(c, B200_ERR_ARG, "too many atoms (%lld)", total);
+  c->nrep = nrep;
+  c->rep_natoms.assign(natoms, natoms + nrep);
+  c->rep_atom_start.assign(nrep + 1, 0);
+  for (int r = 0; r < nrep; r++) c->rep_atom_start[r + 1] = c->rep_atom_start[r] + natoms[r];
+  c->rep_lo.assign(lo, lo + 3 * nrep);
+  c->rep_hi.assign(hi, hi + 3 * nrep);
+  c->rep_box.assign(nrep, BoxGeom{});
+  for (int r = 0; r < nrep; r++)
+    for (int d = 0; d < 3; d++) {
+      c->rep_box[r].lo[d] = lo[3 * r + d];
+      c->rep_box[r].hi[d] = hi[3 * r + d];
+      c->rep_box[r].prd[d] = hi[3 * r + d] - lo[3 * r + d];  // Domain::set_global_box
+    }
+  c->box = c->rep_box[0];
+  c->box_set = true;
+  c->sorted_once = false;
+  invalidate_graphs(c);
+  return B200_OK;
+}
+
+int b200_replica_count(const b200_ctx *c) { return c ? c->nrep : 0; }
+
+int b200_replica_thermo(b200_ctx *c, double *rows) {
+  if (!c || !rows) return B200_ERR_ARG;
+  if (!c->nrep) return set_err(c, B200_ERR_STATE, "no replicas set");
+  if (!c->sorted_once) return set_err(c, B200_ERR_STATE, "neighbor list not built");
+  CK(cudaSetDevice(c->device));
+  const int n = c->n, R = c->nrep;
+  CK(cudaMallocAsync((void **)&c->rep_eatom, (size_t)n * sizeof(double), c->stream));
+  CK(cudaMallocAsync((void **)&c->rep_vatom, 6 * (size_t)n * sizeof(double), c->stream));
+  CK(cudaMallocAsync((void **)&c->rep_rows, 9 * (size_t)R * sizeof(double), c->stream));
+  int rc = pair_compute_dev(c, true, true, c->rep_eatom, c->rep_vatom);
+  if (!rc) {
+    cudaError_t e = md_rep_rows(c, c->rep_eatom, c->rep_vatom, c->rep_rows);
+    if (e != cudaSuccess) rc = set_err(c, B200_ERR_CUDA, "replica rows: %s", cudaGetErrorString(e));
+  }
+  if (!rc)
+    CK(cudaMemcpyAsync(rows, c->rep_rows, 9 * (size_t)R * sizeof(double), cudaMemcpyDeviceToHost,
+                       c->stream));
+  CK(cudaFreeAsync(c->rep_eatom, c->stream));
+  CK(cudaFreeAsync(c->rep_vatom, c->stream));
+  CK(cudaFreeAsync(c->rep_rows, c->stream));
+  c->rep_eatom = c->rep_vatom = c->rep_rows = nullptr;
+  CK(cudaStreamSynchronize(c->stream));
+  return rc;
 }

@@ -11,13 +11,15 @@
 
 namespace {
 
+template <bool BATCH>
 __global__ void __launch_bounds__(256) k_nve_initial(int n, int stride, double dtv, double dtf,
                                                       const double *__restrict__ mass,
                                                       double4 *__restrict__ x4,
                                                       double *__restrict__ v,
                                                       const double *__restrict__ f,
                                                       float4 *__restrict__ xr,
-                                                      const int *__restrict__ cell, BoxGeom box,
+                                                      const int *__restrict__ cell, BoxGeom box1,
+                                                      Reps reps,
                                                       const double4 *__restrict__ xhold,
                                                       double triggersq, int *__restrict__ status) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -36,6 +38,7 @@ __global__ void __launch_bounds__(256) k_nve_initial(int n, int stride, double d
     v[2 * stride + i] = vz;
     x4[i] = p;
     if (xr) {
+      const BoxGeom &box = BATCH ? reps.box[reps.rep_of_atom[i]] : box1;
       int cx, cy, cz;
       md_cell_unpack(cell[i], cx, cy, cz);
       const double ox = box.lo[0] + (cx + 0.5) * box.cs[0];
@@ -139,10 +142,16 @@ __global__ void k_record_row(int *status, const double *ev, double *rows, int ca
 cudaError_t md_nve_initial(b200_ctx *c, double dtv, double dtf) {
   const int B = 256;
   const double triggersq = 0.25 * c->skin * c->skin;  // src/neighbor.cpp:239
-  k_nve_initial<<<md_blocks(c->n, B), B, 0, c->stream>>>(
-      c->n, c->stride, dtv, dtf, c->mass_dev, c->x4, c->v, c->f,
-      c->prec == B200_PREC_MIXED ? c->xr : nullptr, c->cell, c->box,
-      c->check ? c->xhold : nullptr, triggersq, c->status);
+  if (c->nrep)
+    k_nve_initial<true><<<md_blocks(c->n, B), B, 0, c->stream>>>(
+        c->n, c->stride, dtv, dtf, c->mass_dev, c->x4, c->v, c->f,
+        c->prec == B200_PREC_MIXED ? c->xr : nullptr, c->cell, c->box, c->reps(),
+        c->check ? c->xhold : nullptr, triggersq, c->status);
+  else
+    k_nve_initial<false><<<md_blocks(c->n, B), B, 0, c->stream>>>(
+        c->n, c->stride, dtv, dtf, c->mass_dev, c->x4, c->v, c->f,
+        c->prec == B200_PREC_MIXED ? c->xr : nullptr, c->cell, c->box, c->reps(),
+        c->check ? c->xhold : nullptr, triggersq, c->status);
   c->launches++;
   return cudaGetLastError();
 }

@@ -17,6 +17,7 @@
 #include <stdint.h>
 
 #define MD_MAXTYPES 8
+#define MD_TILE_CELLS 4    // cells along x owned by one neighbor-builder CTA
 #define MD_ADJ_MAXTYPES 4  // types of the force-matching adjoint (16 type pairs)
 #define MD_JBITS 26
 #define MD_JMASK ((1u << MD_JBITS) - 1u)
@@ -46,6 +47,19 @@ struct BoxGeom {
   double cinv[3];    // cells per unit length: ncell/prd
   double cs[3];      // cell edge prd/ncell
   int ncell[3];
+};
+
+// Replica tables of a batched context: several independent periodic boxes
+// advanced together in one set of device arrays.  The atoms of replica r
+// always occupy the sorted indices [atom_start[r], atom_start[r+1]) (a
+// rebuild only permutes atoms within their replica), and its cells the
+// global cell indices [cell_base[r], cell_base[r] + ncells(r)).
+struct Reps {
+  const BoxGeom *box;      // per replica
+  const int *rep_of_atom;  // per sorted atom index (fixed)
+  const int *cell_base;    // per replica
+  const int *tile_rep;     // per neighbor-builder tile
+  const int *tile_base;    // per replica: its first builder tile
 };
 
 struct LJParamsDev {

@@ -50,6 +50,21 @@ struct b200_ctx {
   BoxGeom box{};
   int ncells = 0;
 
+  // replicas (b200_set_replicas): nrep independent boxes in one context;
+  // nrep == 0 is the single box `box`
+  int nrep = 0;
+  std::vector<int> rep_natoms, rep_atom_start, rep_cell_base, rep_tile_base;
+  std::vector<double> rep_lo, rep_hi;
+  std::vector<BoxGeom> rep_box;
+  int ntiles = 0;  // builder tiles over all replicas
+  BoxGeom *d_rep_box = nullptr;
+  int *d_rep_of_atom = nullptr, *d_rep_cell_base = nullptr, *d_tile_rep = nullptr,
+      *d_rep_tile_base = nullptr;
+  int rep_dev_n = 0, rep_dev_tiles = 0, rep_dev_r = 0;
+  double *rep_eatom = nullptr, *rep_vatom = nullptr, *rep_rows = nullptr;
+  Reps reps() const { return Reps{d_rep_box, d_rep_of_atom, d_rep_cell_base, d_tile_rep,
+                                  d_rep_tile_base}; }
+
   // settings
   double skin = 0.3;
   int every = 1, delay = 10, check = 1, one_user = 0;
@@ -136,6 +151,7 @@ struct b200_ctx {
   std::vector<cudaGraphNode_t> ev_nodes[4];            // event-record nodes per graph
   std::vector<cudaEvent_t> ev_pool;                    // per-step events of a chunk
   double phase_ms[MD_NPHASE] = {0};
+  std::vector<float> step_ms;  // device time of each timed step (first to last phase event)
   long long phase_steps = 0;
 };
 
@@ -168,6 +184,11 @@ cudaError_t md_adj_backward(b200_ctx *c, const double *lj1, const double *lj2,
                             const double *cutsq, const double *g, double *gx, double *gs,
                             double *gtab);
 cudaError_t md_adj_positions(b200_ctx *c, const double *x);
+
+// ---- replicas (replica.cu) ------------------------------------------------------
+// per-replica thermo rows {natoms, sum m v^2, eng_vdwl, virial[6]} from the
+// per-atom energy/virial of the last compute (eatom, vatom in caller order)
+cudaError_t md_rep_rows(b200_ctx *c, const double *eatom, const double *vatom, double *rows);
 
 inline int md_blocks(long long work, int block) {
   return (int)((work + block - 1) / block);

@@ -29,12 +29,16 @@ constexpr int kScanTile = kScanThreads * kScanItems;
 
 __device__ __forceinline__ bool rebuild_on(const int *flag) { return flag == nullptr || *flag != 0; }
 
-__global__ void k_wrap_bin(int n, BoxGeom box, double4 *__restrict__ x4, int *__restrict__ image,
-                           int *__restrict__ cell_count, int *__restrict__ slot,
-                           int *__restrict__ cell_tmp, int *__restrict__ status, const int *flag) {
+template <bool BATCH>
+__global__ void k_wrap_bin(int n, BoxGeom box1, Reps reps, double4 *__restrict__ x4,
+                           int *__restrict__ image, int *__restrict__ cell_count,
+                           int *__restrict__ slot, int *__restrict__ cell_tmp,
+                           int *__restrict__ status, const int *flag) {
   if (!rebuild_on(flag)) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const int rep = BATCH ? reps.rep_of_atom[i] : 0;
+  const BoxGeom &box = BATCH ? reps.box[rep] : box1;
   double4 p = x4[i];
   double xs[3] = {p.x, p.y, p.z};
   int img = image[i];
@@ -69,6 +73,7 @@ __global__ void k_wrap_bin(int n, BoxGeom box, double4 *__restrict__ x4, int *__
   x4[i] = make_double4(xs[0], xs[1], xs[2], p.w);
   image[i] = md_img_pack(im[0], im[1], im[2]);
   int c = cc[0] + box.ncell[0] * (cc[1] + box.ncell[1] * cc[2]);
+  if (BATCH) c += reps.cell_base[rep];
   slot[i] = atomicAdd(&cell_count[c], 1);
   cell_tmp[i] = c;
 }
@@ -178,7 +183,8 @@ __global__ void k_sort_cells(int ncells, const int *__restrict__ cell_start, int
   }
 }
 
-__global__ void k_gather(int n, int stride, BoxGeom box, const int *__restrict__ perm,
+template <bool BATCH>
+__global__ void k_gather(int n, int stride, BoxGeom box1, Reps reps, const int *__restrict__ perm,
                          const double4 *__restrict__ x4, double4 *__restrict__ x4b,
                          const double *__restrict__ v, double *__restrict__ vb,
                          const int *__restrict__ orig, int *__restrict__ origb,
@@ -197,6 +203,9 @@ __global__ void k_gather(int n, int stride, BoxGeom box, const int *__restrict__
   origb[k] = orig[old];
   imageb[k] = image[old];
   int c = cell_tmp[old];
+  const int rep = BATCH ? reps.rep_of_atom[k] : 0;
+  const BoxGeom &box = BATCH ? reps.box[rep] : box1;
+  if (BATCH) c -= reps.cell_base[rep];
   int cx = c % box.ncell[0];
   int cy = (c / box.ncell[0]) % box.ncell[1];
   int cz = c / (box.ncell[0] * box.ncell[1]);
@@ -237,7 +246,7 @@ __global__ void k_copyback(int n, int stride, const double4 *__restrict__ x4b,
 // outside a relative band of 1e-5 around (rc+skin)^2; pairs inside the band
 // are decided by the reference's FP64 arithmetic on the global FP64
 // positions, so the list is bit-identical to the FP64 criterion.
-constexpr int kTileCells = 4;
+constexpr int kTileCells = MD_TILE_CELLS;
 constexpr int kStageCap = 2048;
 constexpr int kStageCells = 3 * 3 * (kTileCells + 2);
 constexpr int kNeighThreads = 32 * kTileCells;  // one warp per owned cell
@@ -278,12 +287,18 @@ __device__ __forceinline__ bool exact_pair(const double4 &xi, const double4 &xj,
   return dsq3(delx, dely, delz) <= cutsq;
 }
 
-template <bool SINGLE>
+template <bool SINGLE, bool BATCH>
 __global__ void __launch_bounds__(kNeighThreads) k_neigh_tiles(
-    int n, int stride, int capacity, BoxGeom box, int ntp1, const double *__restrict__ cutneighsq_g,
-    const double4 *__restrict__ x4, const int *__restrict__ cell_start, int *__restrict__ nlist,
-    int *__restrict__ numneigh, int *__restrict__ status, const int *flag) {
+    int n, int stride, int capacity, BoxGeom box1, Reps reps, int ntp1,
+    const double *__restrict__ cutneighsq_g, const double4 *__restrict__ x4,
+    const int *__restrict__ cell_start_g, int *__restrict__ nlist, int *__restrict__ numneigh,
+    int *__restrict__ status, const int *flag) {
   if (!rebuild_on(flag)) return;
+  // batched: this tile's replica, its box and its cells' slice of cell_start
+  const int rep = BATCH ? reps.tile_rep[blockIdx.x] : 0;
+  const int tile = BATCH ? blockIdx.x - reps.tile_base[rep] : blockIdx.x;
+  const BoxGeom &box = BATCH ? reps.box[rep] : box1;
+  const int *__restrict__ cell_start = BATCH ? cell_start_g + reps.cell_base[rep] : cell_start_g;
   __shared__ float4 sp[kStageCap + 32];  // 32 spare slots: a chunk may read past a row
   __shared__ int sj[kStageCap];
   __shared__ int s_start[kStageCells + 1];
@@ -294,9 +309,9 @@ __global__ void __launch_bounds__(kNeighThreads) k_neigh_tiles(
   __shared__ float cns_hi[(MD_MAXTYPES + 1) * (MD_MAXTYPES + 1)];
   const int ncx = box.ncell[0], ncy = box.ncell[1], ncz = box.ncell[2];
   const int tiles_x = (ncx + kTileCells - 1) / kTileCells;
-  const int bx = blockIdx.x % tiles_x;
-  const int cy = (blockIdx.x / tiles_x) % ncy;
-  const int cz = blockIdx.x / (tiles_x * ncy);
+  const int bx = tile % tiles_x;
+  const int cy = (tile / tiles_x) % ncy;
+  const int cz = tile / (tiles_x * ncy);
   const int cx0 = bx * kTileCells;
   const int ow = min(kTileCells, ncx - cx0);  // owned cells in this tile
   for (int k = threadIdx.x; k < ntp1 * ntp1; k += blockDim.x) {
@@ -605,8 +620,15 @@ cudaError_t md_rebuild(b200_ctx *c, const int *d_flag) {
   const int n = c->n, B = 256;
   const int m = c->ncells + 1;
   k_zero_counts<<<md_blocks(m, B), B, 0, c->stream>>>(m, c->cell_count, d_flag);
-  k_wrap_bin<<<md_blocks(n, B), B, 0, c->stream>>>(n, c->box, c->x4, c->image, c->cell_count,
-                                                   c->slot, c->cell_tmp, c->status, d_flag);
+  const Reps R = c->reps();
+  if (c->nrep)
+    k_wrap_bin<true><<<md_blocks(n, B), B, 0, c->stream>>>(n, c->box, R, c->x4, c->image,
+                                                           c->cell_count, c->slot, c->cell_tmp,
+                                                           c->status, d_flag);
+  else
+    k_wrap_bin<false><<<md_blocks(n, B), B, 0, c->stream>>>(n, c->box, R, c->x4, c->image,
+                                                            c->cell_count, c->slot, c->cell_tmp,
+                                                            c->status, d_flag);
   c->launches += 2;
   cudaError_t e = launch_scan(c, m, c->cell_count, c->cell_start, d_flag);
   if (e != cudaSuccess) return e;
@@ -614,23 +636,34 @@ cudaError_t md_rebuild(b200_ctx *c, const int *d_flag) {
                                                   d_flag);
   k_sort_cells<<<md_blocks(c->ncells, kSortWarps), kSortWarps * 32, 0, c->stream>>>(
       c->ncells, c->cell_start, c->perm, c->slot, c->orig, d_flag);
-  k_gather<<<md_blocks(n, B), B, 0, c->stream>>>(
-      n, c->stride, c->box, c->perm, c->x4, c->x4b, c->v, c->vb, c->orig, c->origb, c->image,
-      c->imageb, c->cell_tmp, c->cell, c->prec == 1 ? c->xr : nullptr,
-      c->check ? c->xhold : nullptr, d_flag);
+  if (c->nrep)
+    k_gather<true><<<md_blocks(n, B), B, 0, c->stream>>>(
+        n, c->stride, c->box, R, c->perm, c->x4, c->x4b, c->v, c->vb, c->orig, c->origb, c->image,
+        c->imageb, c->cell_tmp, c->cell, c->prec == 1 ? c->xr : nullptr,
+        c->check ? c->xhold : nullptr, d_flag);
+  else
+    k_gather<false><<<md_blocks(n, B), B, 0, c->stream>>>(
+        n, c->stride, c->box, R, c->perm, c->x4, c->x4b, c->v, c->vb, c->orig, c->origb, c->image,
+        c->imageb, c->cell_tmp, c->cell, c->prec == 1 ? c->xr : nullptr,
+        c->check ? c->xhold : nullptr, d_flag);
   k_copyback<<<md_blocks(n, B), B, 0, c->stream>>>(n, c->stride, c->x4b, c->x4, c->vb, c->v,
                                                    c->origb, c->orig, c->imageb, c->image, d_flag);
   {
-    const int tiles = ((c->box.ncell[0] + kTileCells - 1) / kTileCells) * c->box.ncell[1] *
-                      c->box.ncell[2];
-    if (c->ntypes == 1)
-      k_neigh_tiles<true><<<tiles, kNeighThreads, 0, c->stream>>>(
-          n, c->stride, c->capacity, c->box, c->ntypes + 1, c->cutneighsq_dev, c->x4,
-          c->cell_start, c->nlist, c->numneigh, c->status, d_flag);
+    const int tiles = c->nrep ? c->ntiles
+                              : ((c->box.ncell[0] + kTileCells - 1) / kTileCells) *
+                                    c->box.ncell[1] * c->box.ncell[2];
+#define MD_NEIGH_ARGS                                                                         \
+  n, c->stride, c->capacity, c->box, R, c->ntypes + 1, c->cutneighsq_dev, c->x4, c->cell_start, \
+      c->nlist, c->numneigh, c->status, d_flag
+    if (c->ntypes == 1 && !c->nrep)
+      k_neigh_tiles<true, false><<<tiles, kNeighThreads, 0, c->stream>>>(MD_NEIGH_ARGS);
+    else if (c->ntypes == 1)
+      k_neigh_tiles<true, true><<<tiles, kNeighThreads, 0, c->stream>>>(MD_NEIGH_ARGS);
+    else if (!c->nrep)
+      k_neigh_tiles<false, false><<<tiles, kNeighThreads, 0, c->stream>>>(MD_NEIGH_ARGS);
     else
-      k_neigh_tiles<false><<<tiles, kNeighThreads, 0, c->stream>>>(
-          n, c->stride, c->capacity, c->box, c->ntypes + 1, c->cutneighsq_dev, c->x4,
-          c->cell_start, c->nlist, c->numneigh, c->status, d_flag);
+      k_neigh_tiles<false, true><<<tiles, kNeighThreads, 0, c->stream>>>(MD_NEIGH_ARGS);
+#undef MD_NEIGH_ARGS
   }
   k_build_done<<<1, 1, 0, c->stream>>>(c->status, c->check, d_flag);
   c->launches += 5;

@@ -25,6 +25,7 @@ namespace {
 struct PairArgs {
   int n, stride, ntp1;
   BoxGeom box;
+  Reps reps;  // replica boxes of a batched context
   const double *tables;
   const int *cell, *nlist, *numneigh, *orig;
   double *f;
@@ -38,7 +39,7 @@ __device__ __forceinline__ void decode(unsigned int e, int &j, int &dx, int &dy,
   md_entry(e, j, dx, dy, dz);
 }
 
-template <int TPA, bool EV, bool ATOM, bool SINGLE>
+template <int TPA, bool EV, bool ATOM, bool SINGLE, bool BATCH>
 __global__ void __launch_bounds__(128) k_lj_fp64(PairArgs a, const double4 *__restrict__ x4) {
   __shared__ double tab[6 * TABSZ];
   __shared__ double red[7 * 4];
@@ -68,9 +69,10 @@ __global__ void __launch_bounds__(128) k_lj_fp64(PairArgs a, const double4 *__re
     const int ti = (int)xi.w;
     int cx, cy, cz;
     md_cell_unpack(a.cell[i], cx, cy, cz);
-    const Shift3 sx = shifts(cx, a.box.ncell[0], a.box.prd[0]);
-    const Shift3 sy = shifts(cy, a.box.ncell[1], a.box.prd[1]);
-    const Shift3 sz = shifts(cz, a.box.ncell[2], a.box.prd[2]);
+    const BoxGeom &box = BATCH ? a.reps.box[a.reps.rep_of_atom[i]] : a.box;
+    const Shift3 sx = shifts(cx, box.ncell[0], box.prd[0]);
+    const Shift3 sy = shifts(cy, box.ncell[1], box.prd[1]);
+    const Shift3 sz = shifts(cz, box.ncell[2], box.prd[2]);
     const int num = a.numneigh[i];
     const int4 *nl4 = reinterpret_cast<const int4 *>(a.nlist);
     for (int c4 = lane; 4 * c4 < num; c4 += TPA) {
@@ -145,7 +147,7 @@ __global__ void __launch_bounds__(128) k_lj_fp64(PairArgs a, const double4 *__re
   }
 }
 
-template <int TPA, bool EV, bool ATOM, bool SINGLE>
+template <int TPA, bool EV, bool ATOM, bool SINGLE, bool BATCH>
 __global__ void __launch_bounds__(128) k_lj_mixed(PairArgs a, const float4 *__restrict__ xr) {
   __shared__ float tabf[6 * TABSZ];
   __shared__ double red[7 * 4];
@@ -173,7 +175,8 @@ __global__ void __launch_bounds__(128) k_lj_mixed(PairArgs a, const float4 *__re
     }
     const float4 xi = xr[i];
     const int ti = __float_as_int(xi.w);
-    const float csx = (float)a.box.cs[0], csy = (float)a.box.cs[1], csz = (float)a.box.cs[2];
+    const BoxGeom &box = BATCH ? a.reps.box[a.reps.rep_of_atom[i]] : a.box;
+    const float csx = (float)box.cs[0], csy = (float)box.cs[1], csz = (float)box.cs[2];
     const int num = a.numneigh[i];
     const int4 *nl4 = reinterpret_cast<const int4 *>(a.nlist);
     // whole slabs: the tail of the last slab holds pad entries, which the
@@ -254,29 +257,35 @@ __global__ void __launch_bounds__(128) k_lj_mixed(PairArgs a, const float4 *__re
   }
 }
 
-template <int TPA, bool EV, bool ATOM, bool SINGLE>
+template <int TPA, bool EV, bool ATOM, bool SINGLE, bool BATCH>
 void launch_t(b200_ctx *c, const PairArgs &a) {
   const int B = 128;
   const int grid = md_blocks((long long)a.n * TPA, B);
   if (c->prec == B200_PREC_MIXED)
-    k_lj_mixed<TPA, EV, ATOM, SINGLE><<<grid, B, 0, c->stream>>>(a, c->xr);
+    k_lj_mixed<TPA, EV, ATOM, SINGLE, BATCH><<<grid, B, 0, c->stream>>>(a, c->xr);
   else
-    k_lj_fp64<TPA, EV, ATOM, SINGLE><<<grid, B, 0, c->stream>>>(a, c->x4);
+    k_lj_fp64<TPA, EV, ATOM, SINGLE, BATCH><<<grid, B, 0, c->stream>>>(a, c->x4);
   c->launches++;
+}
+
+template <int TPA, bool BATCH>
+void launch_tb(b200_ctx *c, const PairArgs &a, bool ev, bool atom, bool single) {
+  if (!ev) {
+    if (single) launch_t<TPA, false, false, true, BATCH>(c, a);
+    else launch_t<TPA, false, false, false, BATCH>(c, a);
+  } else if (!atom) {
+    if (single) launch_t<TPA, true, false, true, BATCH>(c, a);
+    else launch_t<TPA, true, false, false, BATCH>(c, a);
+  } else {
+    if (single) launch_t<TPA, true, true, true, BATCH>(c, a);
+    else launch_t<TPA, true, true, false, BATCH>(c, a);
+  }
 }
 
 template <int TPA>
 void launch_tpa(b200_ctx *c, const PairArgs &a, bool ev, bool atom, bool single) {
-  if (!ev) {
-    if (single) launch_t<TPA, false, false, true>(c, a);
-    else launch_t<TPA, false, false, false>(c, a);
-  } else if (!atom) {
-    if (single) launch_t<TPA, true, false, true>(c, a);
-    else launch_t<TPA, true, false, false>(c, a);
-  } else {
-    if (single) launch_t<TPA, true, true, true>(c, a);
-    else launch_t<TPA, true, true, false>(c, a);
-  }
+  if (c->nrep) launch_tb<TPA, true>(c, a, ev, atom, single);
+  else launch_tb<TPA, false>(c, a, ev, atom, single);
 }
 
 }  // namespace
@@ -287,6 +296,7 @@ cudaError_t md_lj_compute(b200_ctx *c, bool ev, bool atom_ev, double *eatom, dou
   a.stride = c->stride;
   a.ntp1 = c->ntypes + 1;
   a.box = c->box;
+  a.reps = c->reps();
   a.tables = c->tables_dev;
   a.cell = c->cell;
   a.nlist = c->nlist;

@@ -158,8 +158,10 @@ class System:
         return out
 
     def _row_to_thermo(self, row):
+        return self._thermo(row, self.n, float(np.prod(self.box_hi - self.box_lo)))
+
+    def _thermo(self, row, n, vol):
         u = self.u
-        n = self.n
         dof = 3.0 * n - 3.0
         tfactor = u["mvv2e"] / (dof * u["boltz"]) if dof > 0 else 0.0
         temp = row[1] * tfactor
@@ -168,7 +170,6 @@ class System:
         ke = temp * 0.5 * dof * u["boltz"]
         if u["normflag"]:
             ke /= n
-        vol = float(np.prod(self.box_hi - self.box_lo))
         press = (dof * u["boltz"] * temp + row[3] + row[4] + row[5]) / 3.0 * (1.0 / vol) * u["nktv2p"]
         return dict(Step=int(round(row[0])), Temp=temp, E_pair=epair, E_mol=0.0,
                     TotEng=epair + ke, Press=press, eng=pe, virial=np.array(row[3:9]), ke2=row[1])
@@ -233,6 +234,45 @@ class System:
         steps = C.c_longlong()
         self._ck(self._L.b200_get_timing(self._h, _abi.dptr(ms), C.byref(steps), int(reset)))
         return dict(zip(self.PHASES, ms.tolist()), steps=steps.value)
+
+    def step_times(self, reset=True):
+        """Device milliseconds of every step timed since the last reset."""
+        cnt = C.c_int()
+        self._ck(self._L.b200_get_step_times(self._h, None, 0, C.byref(cnt), 0))
+        ms = np.zeros(max(cnt.value, 1))
+        self._ck(self._L.b200_get_step_times(self._h, _abi.dptr(ms), cnt.value, C.byref(cnt),
+                                             int(reset)))
+        return ms[:cnt.value]
+
+    # ---- replicas --------------------------------------------------------
+    def set_replicas(self, natoms, lo, hi):
+        """Independent periodic boxes advanced together: replica r has
+        natoms[r] atoms in [lo[r], hi[r]); the next set_atoms takes their
+        atoms concatenated in replica order (replaces set_box)."""
+        natoms = np.ascontiguousarray(natoms, dtype=np.int32)
+        lo = np.ascontiguousarray(lo, dtype=np.float64).reshape(-1, 3)
+        hi = np.ascontiguousarray(hi, dtype=np.float64).reshape(-1, 3)
+        self._ck(self._L.b200_set_replicas(self._h, len(natoms), _abi.iptr(natoms),
+                                           _abi.dptr(lo), _abi.dptr(hi)))
+        self.rep_natoms = natoms
+        self.rep_lo, self.rep_hi = lo, hi
+        self.box_lo, self.box_hi = lo[0], hi[0]
+
+    def replica_thermo(self):
+        """Per-replica thermo (Temp, E_pair, TotEng, Press as thermo_style
+        one, normalised per atom in lj units) of the current state."""
+        R = len(self.rep_natoms)
+        rows = np.zeros((R, 9))
+        self._ck(self._L.b200_replica_thermo(self._h, _abi.dptr(rows)))
+        out = []
+        for r in range(R):
+            row = rows[r].copy()
+            n = int(round(row[0]))
+            row[0] = self.ntimestep
+            t = self._thermo(row, n, float(np.prod(self.rep_hi[r] - self.rep_lo[r])))
+            t["natoms"] = n
+            out.append(t)
+        return out
 
     @property
     def kernel_launches(self):
