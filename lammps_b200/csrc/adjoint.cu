@@ -39,12 +39,12 @@ __device__ __forceinline__ void pair_geom(const AdjTables &T, int i, unsigned e,
                                           const Shift3 &sy, const Shift3 &sz, float csx,
                                           float csy, float csz, double &dx, double &dy,
                                           double &dz, double &rsq, int &tt) {
-  const int j = (int)(e & MD_JMASK);
+  const int j = md_entry_j(e);
   if (MIXED) {
     const float4 xi = xr[i], xj = xr[j];
-    const float fx = fmaf(-md_code_d(e, MD_JBITS), csx, xi.x - xj.x);
-    const float fy = fmaf(-md_code_d(e, MD_JBITS + 2), csy, xi.y - xj.y);
-    const float fz = fmaf(-md_code_d(e, MD_JBITS + 4), csz, xi.z - xj.z);
+    const float fx = fmaf(-md_code_dx(e), csx, xi.x - xj.x);
+    const float fy = fmaf(-md_code_dy4(e), 0.25f * csy, xi.y - xj.y);
+    const float fz = fmaf(-md_code_dz16(e), 0.0625f * csz, xi.z - xj.z);
     dx = fx;
     dy = fy;
     dz = fz;
@@ -52,8 +52,8 @@ __device__ __forceinline__ void pair_geom(const AdjTables &T, int i, unsigned e,
     tt = (__float_as_int(xi.w) - 1) * T.ntypes + (__float_as_int(xj.w) - 1);
   } else {
     const double4 xi = x4[i], xj = x4[j];
-    const int ex = (int)((e >> MD_JBITS) & 3u) - 1, ey = (int)((e >> (MD_JBITS + 2)) & 3u) - 1,
-              ez = (int)(e >> (MD_JBITS + 4)) - 1;
+    int jj, ex, ey, ez;
+    md_entry(e, jj, ex, ey, ez);
     dx = xi.x - (xj.x + pick(sx, ex));
     dy = xi.y - (xj.y + pick(sy, ey));
     dz = xi.z - (xj.z + pick(sz, ez));
@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(kAdjThreads)
     double hx = 0.0, hy = 0.0, hz = 0.0;
     for (int k = 0; k < num; k++) {
       const unsigned e = (unsigned)nlist[md_slab(k, i, stride)];
-      const int j = (int)(e & MD_JMASK);
+      const int j = md_entry_j(e);
       double dx, dy, dz, rsq;
       int tt;
       pair_geom<MIXED>(T, i, e, x4, xr, sx, sy, sz, csx, csy, csz, dx, dy, dz, rsq, tt);

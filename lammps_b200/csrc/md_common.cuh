@@ -6,9 +6,9 @@
 //   f[3][n]    double SoA                     -- forces (owner-summed; no ghosts)
 //   xr[i]      float4 (cell-relative x,y,z, type bits) -- mixed precision only
 //   cell[i]    packed cell coordinates cx | cy<<10 | cz<<20 of the last build
-//   nlist      neighbor list in int4 slabs (md_slab): bits 0..25 = neighbor
-//              atom index, bits 26..31 = offset of the neighbor's cell from
-//              the atom's cell, two bits per dimension (d+1 for d = -1,0,1).
+//   nlist      neighbor list in int4 slabs (md_slab): bits 6..31 = neighbor
+//              atom index, bits 0..5 = offset of the neighbor's cell from the
+//              atom's cell, two bits per dimension (d+1 for d = -1,0,1).
 // Periodic images are never stored: a neighbor in a wrapped cell is the owner
 // atom plus the box shift implied by the offset code, so the reference's
 // ghost atoms, forward_comm and reverse_comm disappear.
@@ -91,7 +91,12 @@ __host__ __device__ inline int md_code(int dx, int dy, int dz) {
 // sqrt(3) * cell edge > rc + skin away, so a kernel that reads whole slabs
 // rejects it by the cutoff test without checking the count.
 #define MD_CODE_PAD 63
-__host__ __device__ inline int md_pad_entry(int i) { return (int)((unsigned)i | (63u << MD_JBITS)); }
+__host__ __device__ inline int md_pad_entry(int i) { return (int)(((unsigned)i << 6) | 63u); }
+// list entry of neighbor j in the cell at offset code `code`
+__host__ __device__ inline int md_make_entry(int j, int code) {
+  return (int)(((unsigned)j << 6) | (unsigned)code);
+}
+__host__ __device__ inline int md_entry_j(unsigned e) { return (int)(e >> 6); }
 
 // Periodic shift of a neighbour in the cell at offset d (-1, 0, +1) from
 // cell c along one dimension: -prd / +prd when that cell wraps, else 0
@@ -108,19 +113,26 @@ __device__ __forceinline__ double pick(const Shift3 &s, int d) {
   return d < 0 ? s.m : (d > 0 ? s.p : 0.0);
 }
 
-// Cell offset d = bits - 1 (-1, 0, +1; +2 for the pad entry) of an entry
-// along one dimension, as a float, without an integer-to-float conversion:
-// the two code bits become the low mantissa bits of 2^23 (exact), and
-// 2^23 + 1 is subtracted (exact).  d * cell edge is exact for these d, so
-// fmaf(-d, cs, x) rounds once, like x - (d * cs).
-__device__ __forceinline__ float md_code_d(unsigned e, int shift) {
-  return __int_as_float((int)(0x4B000000u | ((e >> shift) & 3u))) - 8388609.0f;
+// Cell offset of an entry along x, y, z as a float, without an
+// integer-to-float conversion: the code bits are ORed into the low mantissa
+// of 2^23 (exact) and 2^23 plus the bias is subtracted (exact).  With
+// d = bits - 1 (-1, 0, +1; +2 for the pad entry) they return d, 4 d and
+// 16 d, to be multiplied by cs, cs/4 and cs/16: the products are exact, so
+// fmaf(-offset, scaled cs, x) rounds once, like x - d * cs.
+__device__ __forceinline__ float md_code_dx(unsigned e) {
+  return __int_as_float((int)(0x4B000000u | (e & 3u))) - 8388609.0f;
+}
+__device__ __forceinline__ float md_code_dy4(unsigned e) {
+  return __int_as_float((int)(0x4B000000u | (e & 12u))) - 8388612.0f;
+}
+__device__ __forceinline__ float md_code_dz16(unsigned e) {
+  return __int_as_float((int)(0x4B000000u | (e & 48u))) - 8388624.0f;
 }
 __host__ __device__ inline void md_entry(unsigned int e, int &j, int &dx, int &dy, int &dz) {
-  j = (int)(e & MD_JMASK);
-  dx = (int)((e >> MD_JBITS) & 3u) - 1;
-  dy = (int)((e >> (MD_JBITS + 2)) & 3u) - 1;
-  dz = (int)(e >> (MD_JBITS + 4)) - 1;
+  j = (int)(e >> 6);
+  dx = (int)(e & 3u) - 1;
+  dy = (int)((e >> 2) & 3u) - 1;
+  dz = (int)((e >> 4) & 3u) - 1;
 }
 
 // Slab layout of the neighbor list: entry k of atom i is at

@@ -363,7 +363,7 @@ __global__ void __launch_bounds__(kNeighThreads) k_neigh_tiles(
         const int o = s_start[id] + t;
         sp[o] = make_float4((float)(__dadd_rn(p.x, shx) - rx), (float)(__dadd_rn(p.y, shy) - ry),
                             (float)(__dadd_rn(p.z, shz) - rz), __int_as_float((int)p.w));
-        sj[o] = (int)((unsigned)(g0 + t) | ((unsigned)(id % (kTileCells + 2)) << MD_JBITS));
+        sj[o] = md_make_entry(g0 + t, id % (kTileCells + 2));
       }
     }
   }
@@ -400,7 +400,7 @@ __global__ void __launch_bounds__(kNeighThreads) k_neigh_tiles(
           const int idL = warp + (kTileCells + 2) * ((1 + dy) + 3 * (1 + dz));  // dx = -1
           const int r0 = s_start[idL], r1 = s_start[idL + 3];
           // entry code of a candidate in staged column sx: dx + 1 = sx - warp
-          const unsigned rowadd = (unsigned)(((dy + 1) << 2) + ((dz + 1) << 4) - warp) << MD_JBITS;
+          const unsigned rowadd = (unsigned)(((dy + 1) << 2) + ((dz + 1) << 4) - warp);
           for (int cb = r0; cb < r1; cb += 32) {
             const int nc = min(32, r1 - cb);
             unsigned acc = 0u, band = 0u;
@@ -437,8 +437,8 @@ __global__ void __launch_bounds__(kNeighThreads) k_neigh_tiles(
                 const unsigned bits = (unsigned)sj[m];
                 // inside the FP32 uncertainty band: the reference's FP64 test
                 if ((band >> t) & 1u) {
-                  const int id = idL - warp + (int)(bits >> MD_JBITS);
-                  if (!exact_pair(xi, x4[bits & MD_JMASK], s_sh[id][0], s_sh[id][1], s_sh[id][2],
+                  const int id = idL - warp + (int)(bits & 7u);
+                  if (!exact_pair(xi, x4[md_entry_j(bits)], s_sh[id][0], s_sh[id][1], s_sh[id][2],
                                   SINGLE ? cut1 : cns[ti * ntp1 + (__float_as_int(sp[m].w) & 15)]))
                     continue;
                 }
@@ -469,15 +469,15 @@ __global__ void __launch_bounds__(kNeighThreads) k_neigh_tiles(
       for (int dy = -1; dy <= 1; dy++)
         for (int dx = -1; dx <= 1; dx++) {
           const int id = (warp + 1 + dx) + (kTileCells + 2) * ((1 + dy) + 3 * (1 + dz));
-          const int codebits = md_code(dx, dy, dz) << MD_JBITS;
+          const int code = md_code(dx, dy, dz);
           const int g = s_src[id];
           const int j1 = cell_start[g + 1];
           for (int j = cell_start[g]; j < j1; j++) {
-            if (codebits == (MD_CODE_SELF << MD_JBITS) && j == i) continue;
+            if (code == MD_CODE_SELF && j == i) continue;
             const double4 xj = x4[j];
             if (exact_pair(xi, xj, s_sh[id][0], s_sh[id][1], s_sh[id][2],
                            cns[ti * ntp1 + (int)xj.w]))
-              append_entry(nlist, stride, i, count, capacity, j | codebits, buf);
+              append_entry(nlist, stride, i, count, capacity, md_make_entry(j, code), buf);
           }
         }
     flush_entries(nlist, stride, i, count, capacity, buf);

@@ -91,7 +91,7 @@ __global__ void __launch_bounds__(128) k_eam_rho(EamArgs a, const double4 *__res
                                     (unsigned int)e4.w};
         double4 xq[4];
 #pragma unroll
-        for (int u = 0; u < 4; u++) xq[u] = x4[u < mm ? (int)(ee[u] & MD_JMASK) : i];
+        for (int u = 0; u < 4; u++) xq[u] = x4[u < mm ? md_entry_j(ee[u]) : i];
 #pragma unroll
         for (int u = 0; u < 4; u++) {
           if (u >= mm) break;
@@ -117,7 +117,8 @@ __global__ void __launch_bounds__(128) k_eam_rho(EamArgs a, const double4 *__res
     } else {
       const float4 xi = xr[i];
       ti = __float_as_int(xi.w);
-      const float csx = (float)a.box.cs[0], csy = (float)a.box.cs[1], csz = (float)a.box.cs[2];
+      const float csx = (float)a.box.cs[0], csy4 = 0.25f * (float)a.box.cs[1],
+                  csz16 = 0.0625f * (float)a.box.cs[2];
       const float cutf = (float)a.cutforcesq, rdrf = (float)a.rdr;
       const int4 *nl4 = reinterpret_cast<const int4 *>(a.nlist);
       for (int c4 = lane; 4 * c4 < num; c4 += TPA) {
@@ -127,14 +128,14 @@ __global__ void __launch_bounds__(128) k_eam_rho(EamArgs a, const double4 *__res
                                     (unsigned int)e4.w};
         float4 xq[4];
 #pragma unroll
-        for (int u = 0; u < 4; u++) xq[u] = xr[ee[u] & MD_JMASK];
+        for (int u = 0; u < 4; u++) xq[u] = xr[md_entry_j(ee[u])];
         float crho = 0.f;  // FP32 slab sum, added to the FP64 density
 #pragma unroll
         for (int u = 0; u < 4; u++) {
           const float4 xj = xq[u];
-          const float delx = fmaf(-md_code_d(ee[u], MD_JBITS), csx, xi.x - xj.x);
-          const float dely = fmaf(-md_code_d(ee[u], MD_JBITS + 2), csy, xi.y - xj.y);
-          const float delz = fmaf(-md_code_d(ee[u], MD_JBITS + 4), csz, xi.z - xj.z);
+          const float delx = fmaf(-md_code_dx(ee[u]), csx, xi.x - xj.x);
+          const float dely = fmaf(-md_code_dy4(ee[u]), csy4, xi.y - xj.y);
+          const float delz = fmaf(-md_code_dz16(ee[u]), csz16, xi.z - xj.z);
           const float rsq = delx * delx + dely * dely + delz * delz;
           if (rsq < cutf) {
             float p = sqrtf(rsq) * rdrf + 1.0f;
@@ -206,7 +207,7 @@ __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__r
        double fpq[4];
 #pragma unroll
        for (int u = 0; u < 4; u++) {
-         const int jj = u < mm ? (int)(ee[u] & MD_JMASK) : i;
+         const int jj = u < mm ? md_entry_j(ee[u]) : i;
          xq[u] = x4[jj];
          fpq[u] = a.fp[jj];
        }
@@ -263,7 +264,8 @@ __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__r
       const float4 xi = xr[i];
       const int ti = __float_as_int(xi.w);
       const float fpi = a.fpf[i];
-      const float csx = (float)a.box.cs[0], csy = (float)a.box.cs[1], csz = (float)a.box.cs[2];
+      const float csx = (float)a.box.cs[0], csy4 = 0.25f * (float)a.box.cs[1],
+                  csz16 = 0.0625f * (float)a.box.cs[2];
       const float cutf = (float)a.cutforcesq, rdrf = (float)a.rdr;
       const int4 *nl4 = reinterpret_cast<const int4 *>(a.nlist);
       for (int c4 = lane; 4 * c4 < num; c4 += TPA) {
@@ -275,7 +277,7 @@ __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__r
        float fpq[4];
 #pragma unroll
        for (int u = 0; u < 4; u++) {
-         const int jj = (int)(ee[u] & MD_JMASK);
+         const int jj = md_entry_j(ee[u]);
          xq[u] = xr[jj];
          fpq[u] = a.fpf[jj];
        }
@@ -284,9 +286,9 @@ __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__r
 #pragma unroll
        for (int u = 0; u < 4; u++) {
         const float4 xj = xq[u];
-        const float delx = fmaf(-md_code_d(ee[u], MD_JBITS), csx, xi.x - xj.x);
-        const float dely = fmaf(-md_code_d(ee[u], MD_JBITS + 2), csy, xi.y - xj.y);
-        const float delz = fmaf(-md_code_d(ee[u], MD_JBITS + 4), csz, xi.z - xj.z);
+        const float delx = fmaf(-md_code_dx(ee[u]), csx, xi.x - xj.x);
+        const float dely = fmaf(-md_code_dy4(ee[u]), csy4, xi.y - xj.y);
+        const float delz = fmaf(-md_code_dz16(ee[u]), csz16, xi.z - xj.z);
         const float rsq = delx * delx + dely * dely + delz * delz;
         if (rsq < cutf) {
           const int tj = __float_as_int(xj.w);

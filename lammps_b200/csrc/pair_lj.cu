@@ -82,7 +82,7 @@ __global__ void __launch_bounds__(128) k_lj_fp64(PairArgs a, const double4 *__re
                                   (unsigned int)e4.w};
       double4 xj[4];
 #pragma unroll
-      for (int u = 0; u < 4; u++) xj[u] = x4[u < m ? (int)(ee[u] & MD_JMASK) : i];
+      for (int u = 0; u < 4; u++) xj[u] = x4[u < m ? md_entry_j(ee[u]) : i];
 #pragma unroll
       for (int u = 0; u < 4; u++) {
         if (u >= m) break;
@@ -176,7 +176,8 @@ __global__ void __launch_bounds__(128) k_lj_mixed(PairArgs a, const float4 *__re
     const float4 xi = xr[i];
     const int ti = __float_as_int(xi.w);
     const BoxGeom &box = BATCH ? a.reps.box[a.reps.rep_of_atom[i]] : a.box;
-    const float csx = (float)box.cs[0], csy = (float)box.cs[1], csz = (float)box.cs[2];
+    const float csx = (float)box.cs[0], csy4 = 0.25f * (float)box.cs[1],
+                csz16 = 0.0625f * (float)box.cs[2];
     const int num = a.numneigh[i];
     const int4 *nl4 = reinterpret_cast<const int4 *>(a.nlist);
     // whole slabs: the tail of the last slab holds pad entries, which the
@@ -187,7 +188,7 @@ __global__ void __launch_bounds__(128) k_lj_mixed(PairArgs a, const float4 *__re
                                   (unsigned int)e4.w};
       float4 xj[4];
 #pragma unroll
-      for (int u = 0; u < 4; u++) xj[u] = xr[ee[u] & MD_JMASK];
+      for (int u = 0; u < 4; u++) xj[u] = xr[md_entry_j(ee[u])];
       // the four pair forces of a slab are summed in FP32, the slab sum is
       // added to the atom's FP64 accumulator
       float cfx = 0.f, cfy = 0.f, cfz = 0.f;
@@ -195,9 +196,9 @@ __global__ void __launch_bounds__(128) k_lj_mixed(PairArgs a, const float4 *__re
       for (int u = 0; u < 4; u++) {
         // x_i - (x_j + image shift) = (xr_i - xr_j) - d * cell edge, with d
         // the offset of the neighbour's cell from the atom's cell
-        const float delx = fmaf(-md_code_d(ee[u], MD_JBITS), csx, xi.x - xj[u].x);
-        const float dely = fmaf(-md_code_d(ee[u], MD_JBITS + 2), csy, xi.y - xj[u].y);
-        const float delz = fmaf(-md_code_d(ee[u], MD_JBITS + 4), csz, xi.z - xj[u].z);
+        const float delx = fmaf(-md_code_dx(ee[u]), csx, xi.x - xj[u].x);
+        const float dely = fmaf(-md_code_dy4(ee[u]), csy4, xi.y - xj[u].y);
+        const float delz = fmaf(-md_code_dz16(ee[u]), csz16, xi.z - xj[u].z);
         const float rsq = delx * delx + dely * dely + delz * delz;
         const int tt = ti * a.ntp1 + __float_as_int(xj[u].w);
         const float cs = SINGLE ? cutsq1 : tabf[0 * nt2 + tt];
