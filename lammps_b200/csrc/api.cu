@@ -47,7 +47,7 @@ void dfree(T *&p) {
 }
 
 void invalidate_graphs(b200_ctx *c) {
-  for (int k = 0; k < 4; k++) {
+  for (int k = 0; k < MD_NPIECES; k++) {
     if (c->step_exec[k]) cudaGraphExecDestroy(c->step_exec[k]);
     if (c->step_graph[k]) cudaGraphDestroy(c->step_graph[k]);
     c->step_exec[k] = nullptr;
@@ -447,7 +447,14 @@ int count_kernels(b200_ctx *c, cudaGraph_t g, int *kernels, std::vector<cudaGrap
 // launched one by one).  With timing on, events mark the phase boundaries:
 // PRE holds phases 0-1, POST phases 2-5; their events are swapped per
 // launch so every step's phases can be read back.
-enum { PIECE_PRE = 0, PIECE_REBUILD = 1, PIECE_POST_OUT = 2, PIECE_POST = 3 };
+enum {
+  PIECE_PRE = 0,
+  PIECE_REBUILD = 1,
+  PIECE_POST_OUT = 2,
+  PIECE_POST = 3,
+  PIECE_FUSED_OUT = 4,  // POST_OUT + the next step's initial half-step and decision
+  PIECE_FUSED = 5       // POST + the same
+};
 
 cudaError_t record(b200_ctx *c, cudaEvent_t ev) {
   cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
@@ -468,7 +475,8 @@ cudaError_t launch_piece(b200_ctx *c, int kind, double dtv, double dtf, cudaEven
   } else if (kind == PIECE_REBUILD) {
     e = md_rebuild(c, nullptr);
   } else {
-    const bool out = kind == PIECE_POST_OUT;
+    const bool out = kind == PIECE_POST_OUT || kind == PIECE_FUSED_OUT;
+    const bool fused = kind == PIECE_FUSED_OUT || kind == PIECE_FUSED;
     if (ev) e = record(c, ev[0]);
     if (e == cudaSuccess) {
       if (c->pstyle == B200_PAIR_LJ_CUT) {
@@ -479,8 +487,9 @@ cudaError_t launch_piece(b200_ctx *c, int kind, double dtv, double dtf, cudaEven
       }
     }
     if (e == cudaSuccess && ev) e = record(c, ev[2]);
-    if (e == cudaSuccess) e = md_nve_final(c, dtf, out);
+    if (e == cudaSuccess) e = fused ? md_nve_fused(c, dtv, dtf, out) : md_nve_final(c, dtf, out);
     if (e == cudaSuccess && out) e = md_record_row(c);
+    if (e == cudaSuccess && fused) e = md_decide(c);
     if (e == cudaSuccess && ev) e = record(c, ev[3]);
   }
   return e;
@@ -539,7 +548,10 @@ int run_piece(b200_ctx *c, int kind, double dtv, double dtf, cudaEvent_t *ev) {
 int ensure_graphs(b200_ctx *c, double dtv, double dtf, double ftm2v) {
   if (!c->use_graphs) return B200_OK;
   if (c->graph_valid) return B200_OK;
-  for (int kind = 0; kind < 4; kind++) {
+  for (int kind = 0; kind < MD_NPIECES; kind++) {
+    // the fused pieces are not used with phase timers on (their events
+    // would mix two steps)
+    if (c->timing && (kind == PIECE_FUSED || kind == PIECE_FUSED_OUT)) continue;
     int rc = capture_piece(c, kind, dtv, dtf);
     if (rc) return rc;
   }
@@ -1082,9 +1094,14 @@ int b200_run(b200_ctx *c, int nsteps, double dt, double ftm2v, int thermo_every,
     };
     // host mirror of Neighbor::ago (src/neighbor.cpp:1301-1309)
     int ago = c->status_host[ST_AGO];
+    // Within a chunk (timers off) the final half-step of step t and the
+    // initial half-step and decision of step t+1 run as one piece; a chunk
+    // starts with its own initial half-step, so snapshots and replays see
+    // whole steps.
+    bool pre_done = false;
     for (long long t = s; t <= s_end; t++) {
       cudaEvent_t *ev = c->timing ? &c->ev_pool[(size_t)(t - s) * (MD_NPHASE + 1)] : nullptr;
-      rc = run_piece(c, PIECE_PRE, dtv, dtf, ev);
+      if (!pre_done) rc = run_piece(c, PIECE_PRE, dtv, dtf, ev);
       if (rc) return rc;
       ago++;
       bool rebuild = false;
@@ -1107,8 +1124,12 @@ int b200_run(b200_ctx *c, int nsteps, double dt, double ftm2v, int thermo_every,
         if (rc) return rc;
         ago = 0;
       }
-      rc = run_piece(c, is_out(t) ? PIECE_POST_OUT : PIECE_POST, dtv, dtf, ev ? ev + 2 : nullptr);
+      const bool fuse = !c->timing && t < s_end;
+      const int post = fuse ? (is_out(t) ? PIECE_FUSED_OUT : PIECE_FUSED)
+                            : (is_out(t) ? PIECE_POST_OUT : PIECE_POST);
+      rc = run_piece(c, post, dtv, dtf, ev ? ev + 2 : nullptr);
       if (rc) return rc;
+      pre_done = fuse;
     }
     rc = read_status(c);
     if (rc) return rc;

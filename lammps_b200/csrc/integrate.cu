@@ -83,6 +83,67 @@ __global__ void __launch_bounds__(256) k_nve_final(int n, int stride, double dtf
   if (KE) block_partials_finish<1>(acc, red, partial, counter, out, false);
 }
 
+// FixNVE::final_integrate of this step, the kinetic-energy term of the
+// thermo output (KE), then FixNVE::initial_integrate of the next step: the
+// same rounded operations as k_nve_final followed by k_nve_initial, with v, f
+// and x read once.
+template <bool KE, bool BATCH>
+__global__ void __launch_bounds__(256) k_nve_fused(int n, int stride, double dtv, double dtf,
+                                                    const double *__restrict__ mass,
+                                                    double4 *__restrict__ x4,
+                                                    double *__restrict__ v,
+                                                    const double *__restrict__ f,
+                                                    float4 *__restrict__ xr,
+                                                    const int *__restrict__ cell, BoxGeom box1,
+                                                    Reps reps, const double4 *__restrict__ xhold,
+                                                    double triggersq, int *__restrict__ status,
+                                                    double *partial, unsigned int *counter,
+                                                    double *out) {
+  __shared__ double red[8];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double acc[1] = {0.0};
+  bool moved = false;
+  if (i < n) {
+    double4 p = x4[i];
+    const double m = mass[(int)p.w];
+    const double dtfm = dtf / m;
+    const double fx = f[i], fy = f[stride + i], fz = f[2 * stride + i];
+    double vx = __dadd_rn(v[i], __dmul_rn(dtfm, fx));
+    double vy = __dadd_rn(v[stride + i], __dmul_rn(dtfm, fy));
+    double vz = __dadd_rn(v[2 * stride + i], __dmul_rn(dtfm, fz));
+    // ComputeTemp::compute_scalar term of this step (src/compute_temp.cpp:84-86)
+    if (KE) acc[0] = (vx * vx + vy * vy + vz * vz) * m;
+    vx = __dadd_rn(vx, __dmul_rn(dtfm, fx));
+    vy = __dadd_rn(vy, __dmul_rn(dtfm, fy));
+    vz = __dadd_rn(vz, __dmul_rn(dtfm, fz));
+    p.x = __dadd_rn(p.x, __dmul_rn(dtv, vx));
+    p.y = __dadd_rn(p.y, __dmul_rn(dtv, vy));
+    p.z = __dadd_rn(p.z, __dmul_rn(dtv, vz));
+    v[i] = vx;
+    v[stride + i] = vy;
+    v[2 * stride + i] = vz;
+    x4[i] = p;
+    if (xr) {
+      const BoxGeom &box = BATCH ? reps.box[reps.rep_of_atom[i]] : box1;
+      int cx, cy, cz;
+      md_cell_unpack(cell[i], cx, cy, cz);
+      const double ox = box.lo[0] + (cx + 0.5) * box.cs[0];
+      const double oy = box.lo[1] + (cy + 0.5) * box.cs[1];
+      const double oz = box.lo[2] + (cz + 0.5) * box.cs[2];
+      xr[i] = make_float4((float)(p.x - ox), (float)(p.y - oy), (float)(p.z - oz),
+                          __int_as_float((int)p.w));
+    }
+    if (xhold) {
+      const double4 h = xhold[i];
+      const double rsq = dsq3(__dsub_rn(p.x, h.x), __dsub_rn(p.y, h.y), __dsub_rn(p.z, h.z));
+      moved = rsq > triggersq;
+    }
+  }
+  if (xhold && __any_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0)
+    atomicExch(&status[ST_MOVED], 1);
+  if (KE) block_partials_finish<1>(acc, red, partial, counter, out, false);
+}
+
 __global__ void __launch_bounds__(256) k_ke(int n, int stride, const double *__restrict__ mass,
                                              const double4 *__restrict__ x4,
                                              const double *__restrict__ v, double *partial,
@@ -164,6 +225,23 @@ cudaError_t md_nve_final(b200_ctx *c, double dtf, bool ke) {
   else
     k_nve_final<false><<<md_blocks(c->n, B), B, 0, c->stream>>>(
         c->n, c->stride, dtf, c->mass_dev, c->x4, c->v, c->f, c->partial, c->counter, c->ev + 7);
+  c->launches++;
+  return cudaGetLastError();
+}
+
+cudaError_t md_nve_fused(b200_ctx *c, double dtv, double dtf, bool ke) {
+  const int B = 256;
+  const double triggersq = 0.25 * c->skin * c->skin;  // src/neighbor.cpp:239
+#define MD_FUSED_ARGS                                                                           \
+  c->n, c->stride, dtv, dtf, c->mass_dev, c->x4, c->v, c->f,                                  \
+      c->prec == B200_PREC_MIXED ? c->xr : nullptr, c->cell, c->box, c->reps(),               \
+      c->check ? c->xhold : nullptr, triggersq, c->status, c->partial, c->counter, c->ev + 7
+  const int grid = md_blocks(c->n, B);
+  if (ke && c->nrep) k_nve_fused<true, true><<<grid, B, 0, c->stream>>>(MD_FUSED_ARGS);
+  else if (ke) k_nve_fused<true, false><<<grid, B, 0, c->stream>>>(MD_FUSED_ARGS);
+  else if (c->nrep) k_nve_fused<false, true><<<grid, B, 0, c->stream>>>(MD_FUSED_ARGS);
+  else k_nve_fused<false, false><<<grid, B, 0, c->stream>>>(MD_FUSED_ARGS);
+#undef MD_FUSED_ARGS
   c->launches++;
   return cudaGetLastError();
 }

@@ -7,6 +7,11 @@
 #include <vector>
 
 #include "md_common.cuh"
+
+// graph pieces of a step (api.cu): initial half-step + decision, rebuild,
+// forces + final half-step (with / without thermo output), and the same two
+// with the next step's initial half-step and decision fused in
+#define MD_NPIECES 6
 #include "../../include/b200md.h"
 
 // timer phases of one step
@@ -135,9 +140,9 @@ struct b200_ctx {
   // CUDA graph of one MD step (captured lazily by b200_run)
   // graphs of the step pieces: [0] initial half-step + decision, [1] rebuild,
   // [2] forces + final half-step with thermo output, [3] the same without
-  cudaGraphExec_t step_exec[4] = {nullptr, nullptr, nullptr, nullptr};
-  cudaGraph_t step_graph[4] = {nullptr, nullptr, nullptr, nullptr};
-  int step_kernels[4] = {0, 0, 0, 0};                   // kernel nodes per graph
+  cudaGraphExec_t step_exec[MD_NPIECES] = {};
+  cudaGraph_t step_graph[MD_NPIECES] = {};
+  int step_kernels[MD_NPIECES] = {};                    // kernel nodes per graph
   bool graph_valid = false;
   double graph_dt = 0, graph_ftm2v = 0;
   int graph_tpa = 0;
@@ -148,7 +153,7 @@ struct b200_ctx {
   // event-record nodes at the phase boundaries of every step graph
   bool timing = false;
   cudaEvent_t ph_event[MD_NPHASE + 1] = {};           // placeholders used at capture
-  std::vector<cudaGraphNode_t> ev_nodes[4];            // event-record nodes per graph
+  std::vector<cudaGraphNode_t> ev_nodes[MD_NPIECES];   // event-record nodes per graph
   std::vector<cudaEvent_t> ev_pool;                    // per-step events of a chunk
   double phase_ms[MD_NPHASE] = {0};
   std::vector<float> step_ms;  // device time of each timed step (first to last phase event)
@@ -170,6 +175,8 @@ cudaError_t md_eam_compute(b200_ctx *c, bool ev, bool atom_ev, double *eatom, do
 cudaError_t md_nve_initial(b200_ctx *c, double dtv, double dtf);
 cudaError_t md_decide(b200_ctx *c);
 cudaError_t md_nve_final(b200_ctx *c, double dtf, bool ke);
+// final half-step of this step (+ KE) and initial half-step of the next
+cudaError_t md_nve_fused(b200_ctx *c, double dtv, double dtf, bool ke);
 cudaError_t md_ke(b200_ctx *c);
 cudaError_t md_record_row(b200_ctx *c);
 cudaError_t md_zero_ev(b200_ctx *c);
