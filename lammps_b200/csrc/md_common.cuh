@@ -166,6 +166,15 @@ __device__ __forceinline__ double rcp_nr(double x) {
   return fma(y, e, y);
 }
 
+// 1/x in FP32 from the hardware reciprocal approximation alone (one
+// instruction, relative error below 2^-22); the mixed-precision kernels use it
+// where the pair term's FP32 error budget is far larger.
+__device__ __forceinline__ float rcp_approx_f32(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 // FP64 helpers that keep a*b+c rounded twice, as the reference's x86-64
 // build computes them; used wherever a comparison must be bit-exact.
 __device__ __forceinline__ double dsq3(double a, double b, double c) {

@@ -14,10 +14,12 @@
 // atom's force, energy and virial are summed in FP64.
 //
 // Memory-level parallelism: each thread reads four list entries with one
-// 16-byte load (slab layout, md_slab) and issues the four neighbor gathers
-// before using any of them.  The FP64 kernel forms 1/rsq by Newton's method
-// from the hardware reciprocal (rcp_nr); the mixed kernel uses the fast FP32
-// reciprocal and adds each slab's FP32 force sum to the FP64 accumulator.
+// 16-byte load (slab layout, md_slab).  The FP64 kernel issues a slab's four
+// neighbor gathers before using any of them and forms 1/rsq by Newton's
+// method from the hardware reciprocal (rcp_nr).  The mixed kernel works on
+// four slabs at a time with the next four already loading, evaluates every
+// entry branch-free with the one-instruction FP32 reciprocal, and adds the
+// FP32 force sum of each eight entries to the FP64 accumulator.
 #include "md_state.h"
 
 namespace {
@@ -178,59 +180,83 @@ __global__ void __launch_bounds__(128) k_lj_mixed(PairArgs a, const float4 *__re
     const BoxGeom &box = BATCH ? a.reps.box[a.reps.rep_of_atom[i]] : a.box;
     const float csx = (float)box.cs[0], csy4 = 0.25f * (float)box.cs[1],
                 csz16 = 0.0625f * (float)box.cs[2];
-    const int num = a.numneigh[i];
+    const int nslab = (a.numneigh[i] + 3) >> 2;
     const int4 *nl4 = reinterpret_cast<const int4 *>(a.nlist);
-    // whole slabs: the tail of the last slab holds pad entries, which the
-    // cutoff test rejects, so no per-entry count check is needed
-    for (int c4 = lane; 4 * c4 < num; c4 += TPA) {
-      const int4 e4 = nl4[(size_t)c4 * a.stride + i];
-      const unsigned int ee[4] = {(unsigned int)e4.x, (unsigned int)e4.y, (unsigned int)e4.z,
-                                  (unsigned int)e4.w};
-      float4 xj[4];
+    // Four slabs (16 entries) per iteration: the sixteen gathers are in
+    // flight together, and the next four slabs' entries are loaded
+    // (streaming, evict-first) before these are used, so the list's DRAM
+    // latency overlaps the gathers and the arithmetic of the slabs before
+    // them.  Slabs past the atom's count, and the tail of its last slab, hold
+    // pad entries, which the cutoff test rejects, so no per-entry count check
+    // is needed.
+    const int pe = md_pad_entry(i);
+    const int4 pad4 = make_int4(pe, pe, pe, pe);
+    auto slab = [&](int c) {
+      return c < nslab ? __ldcs(&nl4[(size_t)c * a.stride + i]) : pad4;
+    };
+    int c4 = lane;
+    int4 a0 = slab(c4), a1 = slab(c4 + TPA), a2 = slab(c4 + 2 * TPA), a3 = slab(c4 + 3 * TPA);
+    while (c4 < nslab) {
+      const int cn = c4 + 4 * TPA;
+      const int4 b0 = slab(cn), b1 = slab(cn + TPA), b2 = slab(cn + 2 * TPA),
+                 b3 = slab(cn + 3 * TPA);
+      const unsigned int eall[16] = {(unsigned)a0.x, (unsigned)a0.y, (unsigned)a0.z, (unsigned)a0.w,
+                                     (unsigned)a1.x, (unsigned)a1.y, (unsigned)a1.z, (unsigned)a1.w,
+                                     (unsigned)a2.x, (unsigned)a2.y, (unsigned)a2.z, (unsigned)a2.w,
+                                     (unsigned)a3.x, (unsigned)a3.y, (unsigned)a3.z, (unsigned)a3.w};
+      float4 xall[16];
 #pragma unroll
-      for (int u = 0; u < 4; u++) xj[u] = xr[md_entry_j(ee[u])];
-      // the four pair forces of a slab are summed in FP32, the slab sum is
-      // added to the atom's FP64 accumulator
-      float cfx = 0.f, cfy = 0.f, cfz = 0.f;
+      for (int u = 0; u < 16; u++) xall[u] = __ldg(&xr[md_entry_j(eall[u])]);
+      // the pair forces of each group of eight entries are summed in FP32,
+      // the group sum is added to the atom's FP64 accumulator
 #pragma unroll
-      for (int u = 0; u < 4; u++) {
-        // x_i - (x_j + image shift) = (xr_i - xr_j) - d * cell edge, with d
-        // the offset of the neighbour's cell from the atom's cell
-        const float delx = fmaf(-md_code_dx(ee[u]), csx, xi.x - xj[u].x);
-        const float dely = fmaf(-md_code_dy4(ee[u]), csy4, xi.y - xj[u].y);
-        const float delz = fmaf(-md_code_dz16(ee[u]), csz16, xi.z - xj[u].z);
-        const float rsq = delx * delx + dely * dely + delz * delz;
-        const int tt = ti * a.ntp1 + __float_as_int(xj[u].w);
-        const float cs = SINGLE ? cutsq1 : tabf[0 * nt2 + tt];
-        if (rsq < cs) {
+      for (int h = 0; h < 2; h++) {
+        const unsigned int *ee = eall + 8 * h;
+        const float4 *xj = xall + 8 * h;
+        float cfx = 0.f, cfy = 0.f, cfz = 0.f;
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          // x_i - (x_j + image shift) = (xr_i - xr_j) - d * cell edge, with d
+          // the offset of the neighbour's cell from the atom's cell
+          const float delx = fmaf(-md_code_dx(ee[u]), csx, xi.x - xj[u].x);
+          const float dely = fmaf(-md_code_dy4(ee[u]), csy4, xi.y - xj[u].y);
+          const float delz = fmaf(-md_code_dz16(ee[u]), csz16, xi.z - xj[u].z);
+          const float rsq = delx * delx + dely * dely + delz * delz;
+          const int tt = ti * a.ntp1 + __float_as_int(xj[u].w);
+          const float cs = SINGLE ? cutsq1 : tabf[0 * nt2 + tt];
           const float c1 = SINGLE ? lj1 : tabf[1 * nt2 + tt];
           const float c2 = SINGLE ? lj2 : tabf[2 * nt2 + tt];
-          const float r2inv = __fdividef(1.0f, rsq);
+          const bool in = rsq < cs;
+          const float r2inv = rcp_approx_f32(rsq);
           const float r6inv = r2inv * r2inv * r2inv;
-          const float forcelj = r6inv * (c1 * r6inv - c2);
-          const float fpair = forcelj * r2inv;
-          cfx += delx * fpair;
-          cfy += dely * fpair;
-          cfz += delz * fpair;
+          const float fpair = in ? r6inv * (c1 * r6inv - c2) * r2inv : 0.f;
+          cfx = fmaf(delx, fpair, cfx);
+          cfy = fmaf(dely, fpair, cfy);
+          cfz = fmaf(delz, fpair, cfz);
           if (EV) {
-          const float c3 = SINGLE ? lj3 : tabf[3 * nt2 + tt];
-          const float c4 = SINGLE ? lj4 : tabf[4 * nt2 + tt];
-          const float co = SINGLE ? off : tabf[5 * nt2 + tt];
-          const float evdwl = r6inv * (c3 * r6inv - c4) - co;
-          acc[0] += 0.5 * (double)evdwl;
-          const float hf = 0.5f * fpair;
-          acc[1] += (double)(delx * delx * hf);
-          acc[2] += (double)(dely * dely * hf);
-          acc[3] += (double)(delz * delz * hf);
-          acc[4] += (double)(delx * dely * hf);
-          acc[5] += (double)(delx * delz * hf);
-          acc[6] += (double)(dely * delz * hf);
+            const float c3 = SINGLE ? lj3 : tabf[3 * nt2 + tt];
+            const float c4 = SINGLE ? lj4 : tabf[4 * nt2 + tt];
+            const float co = SINGLE ? off : tabf[5 * nt2 + tt];
+            const float evdwl = in ? r6inv * (c3 * r6inv - c4) - co : 0.f;
+            acc[0] += 0.5 * (double)evdwl;
+            const float hf = 0.5f * fpair;
+            acc[1] += (double)(delx * delx * hf);
+            acc[2] += (double)(dely * dely * hf);
+            acc[3] += (double)(delz * delz * hf);
+            acc[4] += (double)(delx * dely * hf);
+            acc[5] += (double)(delx * delz * hf);
+            acc[6] += (double)(dely * delz * hf);
           }
         }
+        fx += (double)cfx;
+        fy += (double)cfy;
+        fz += (double)cfz;
       }
-      fx += (double)cfx;
-      fy += (double)cfy;
-      fz += (double)cfz;
+      a0 = b0;
+      a1 = b1;
+      a2 = b2;
+      a3 = b3;
+      c4 = cn;
     }
   }
   fx = lane_sum<TPA>(fx);
