@@ -373,6 +373,7 @@ int rebuild_sync(b200_ctx *c) {
     int rc = read_status(c);
     if (rc) return rc;
     if (c->status_host[ST_LOST]) return status_errors(c);
+    if (md_stage_feedback(c, c->status_host[ST_MAXSTAGE])) invalidate_graphs(c);
     if (!c->status_host[ST_OVERFLOW]) return B200_OK;
     if (c->one_user > 0) return status_errors(c);
     int need = c->status_host[ST_MAXNEIGH];
@@ -1134,6 +1135,13 @@ int b200_run(b200_ctx *c, int nsteps, double dt, double ftm2v, int thermo_every,
     rc = read_status(c);
     if (rc) return rc;
     if (c->status_host[ST_LOST]) return status_errors(c);
+    if (md_stage_feedback(c, c->status_host[ST_MAXSTAGE])) {
+      // a builder tile staged more atoms than its shared memory held (it
+      // took the slower global-memory path): larger staging from now on
+      invalidate_graphs(c);
+      rc = ensure_graphs(c, dtv, dtf, ftm2v);
+      if (rc) return rc;
+    }
     if (c->status_host[ST_OVERFLOW]) {
       if (c->one_user > 0 || ++replays > 4) return status_errors(c);
       const int need = c->status_host[ST_MAXNEIGH];

@@ -39,6 +39,7 @@ enum {
   ST_STEP_LO = 9,    // current timestep (low/high 32 bits)
   ST_STEP_HI = 10,
   ST_FORCE_BUILD = 11,  // rebuild on the next step regardless of the schedule
+  ST_MAXSTAGE = 12,     // most atoms staged by one neighbor-builder tile since setup
   ST_COUNT = 16
 };
 

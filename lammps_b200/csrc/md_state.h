@@ -109,6 +109,7 @@ struct b200_ctx {
   // neighbor list
   int *nlist = nullptr, *numneigh = nullptr;
   int capacity = 0;     // entries per atom
+  int stage_need = 0;   // staged atoms per builder tile seen by earlier builds
   long long nlist_alloc = 0;
 
   // run-chunk snapshot for overflow replay (x4, v, f, xhold planes + ids)
@@ -163,6 +164,8 @@ struct b200_ctx {
 // ---- launchers (neigh.cu) -------------------------------------------------
 // full rebuild: wrap, cell counting sort, permute, neighbor list
 cudaError_t md_rebuild(b200_ctx *c, const int *d_flag);
+int md_stage_cap(const b200_ctx *c);
+bool md_stage_feedback(b200_ctx *c, int staged_max);
 // LAMMPS half list derived from the full list; returns entry count via *total
 cudaError_t md_half_list(b200_ctx *c, int *d_num, int *d_jowner, int *d_jimage, long long cap,
                          long long *total);

@@ -247,7 +247,7 @@ __global__ void k_copyback(int n, int stride, const double4 *__restrict__ x4b,
 // are decided by the reference's FP64 arithmetic on the global FP64
 // positions, so the list is bit-identical to the FP64 criterion.
 constexpr int kTileCells = MD_TILE_CELLS;
-constexpr int kStageCap = 2048;
+constexpr int kStageCapMax = 2048;  // keeps the builder within 48 KB of shared memory
 constexpr int kStageCells = 3 * 3 * (kTileCells + 2);
 constexpr int kNeighThreads = 32 * kTileCells;  // one warp per owned cell
 
@@ -287,9 +287,15 @@ __device__ __forceinline__ bool exact_pair(const double4 &xi, const double4 &xj,
   return dsq3(delx, dely, delz) <= cutsq;
 }
 
+// Shared memory of k_neigh_tiles: stage_cap + 32 float4 positions (32 spare
+// slots: a chunk may read past a row) and stage_cap int entries.
+static size_t neigh_smem(int stage_cap) {
+  return (size_t)(stage_cap + 32) * sizeof(float4) + (size_t)stage_cap * sizeof(int);
+}
+
 template <bool SINGLE, bool BATCH>
-__global__ void __launch_bounds__(kNeighThreads) k_neigh_tiles(
-    int n, int stride, int capacity, BoxGeom box1, Reps reps, int ntp1,
+__global__ void __launch_bounds__(kNeighThreads, 8) k_neigh_tiles(
+    int n, int stride, int capacity, int stage_cap, BoxGeom box1, Reps reps, int ntp1,
     const double *__restrict__ cutneighsq_g, const double4 *__restrict__ x4,
     const int *__restrict__ cell_start_g, int *__restrict__ nlist, int *__restrict__ numneigh,
     int *__restrict__ status, const int *flag) {
@@ -299,8 +305,9 @@ __global__ void __launch_bounds__(kNeighThreads) k_neigh_tiles(
   const int tile = BATCH ? blockIdx.x - reps.tile_base[rep] : blockIdx.x;
   const BoxGeom &box = BATCH ? reps.box[rep] : box1;
   const int *__restrict__ cell_start = BATCH ? cell_start_g + reps.cell_base[rep] : cell_start_g;
-  __shared__ float4 sp[kStageCap + 32];  // 32 spare slots: a chunk may read past a row
-  __shared__ int sj[kStageCap];
+  extern __shared__ float4 s_stage[];
+  float4 *sp = s_stage;
+  int *sj = reinterpret_cast<int *>(s_stage + stage_cap + 32);
   __shared__ int s_start[kStageCells + 1];
   __shared__ int s_src[kStageCells];
   __shared__ double s_sh[kStageCells][3];
@@ -347,7 +354,8 @@ __global__ void __launch_bounds__(kNeighThreads) k_neigh_tiles(
     for (int id = 0; id < kStageCells; id++) s_start[id + 1] += s_start[id];
   }
   __syncthreads();
-  const bool staged = s_start[kStageCells] <= kStageCap;
+  const bool staged = s_start[kStageCells] <= stage_cap;
+  if (threadIdx.x == 0) atomicMax(&status[ST_MAXSTAGE], s_start[kStageCells]);
   // FP32 reference point: centre of cell (cx0, cy, cz)
   const double rx = box.lo[0] + (cx0 + 0.5) * box.cs[0];
   const double ry = box.lo[1] + (cy + 0.5) * box.cs[1];
@@ -373,9 +381,11 @@ __global__ void __launch_bounds__(kNeighThreads) k_neigh_tiles(
   __syncthreads();
   // Warp w owns cell (cx0 + w, cy, cz); each lane takes one of its atoms.
   // The 27 neighbour cells are 9 contiguous staged ranges (3 cells along x
-  // each), scanned 32 candidates at a time: a branch-free test phase builds
-  // a 32-bit acceptance mask per lane (broadcast shared reads), then an
-  // append phase walks the set bits in candidate order.
+  // each), scanned 32 candidates at a time.  Test phase: each lane holds one
+  // candidate and the warp steps through the owned atoms (broadcast shared
+  // reads); one ballot per owned atom gives that atom's 32-bit acceptance
+  // mask, which the atom's own lane keeps.  Append phase: each lane walks the
+  // set bits of its mask in candidate order.
   if (warp >= ow) return;
   const int own_id = (warp + 1) + (kTileCells + 2) * (1 + 3 * 1);
   const int cown = cx0 + warp + ncx * (cy + ncy * cz);
@@ -387,12 +397,12 @@ __global__ void __launch_bounds__(kNeighThreads) k_neigh_tiles(
     for (int base = a0; base < a1; base += 32) {
       const int i = base + lane;
       const bool act = i < a1;
-      const double4 xi = x4[act ? i : a0];
-      const int ti = (int)xi.w;
+      // the FP64 position is read again only for a pair in the FP32 band
+      const int ti = SINGLE ? 1 : (int)x4[act ? i : a0].w;
       const int my_m = act ? o0 + (i - a0) : -1;
-      // an inactive lane sits far away and accepts no candidate
-      const float pix = act ? (float)(xi.x - rx) : 1.0e30f;
-      const float piy = (float)(xi.y - ry), piz = (float)(xi.z - rz);
+      // the owned atoms of this batch, staged as sp[ob .. ob + na) with the
+      // same FP32 offsets from the tile centre as every candidate
+      const int ob = o0 + (base - a0), na = min(32, a1 - base);
       int count = 0;
       int4 buf = make_int4(0, 0, 0, 0);
       for (int dz = -1; dz <= 1; dz++)
@@ -403,20 +413,28 @@ __global__ void __launch_bounds__(kNeighThreads) k_neigh_tiles(
           const unsigned rowadd = (unsigned)(((dy + 1) << 2) + ((dz + 1) << 4) - warp);
           for (int cb = r0; cb < r1; cb += 32) {
             const int nc = min(32, r1 - cb);
+            // this lane's candidate (the spare slots past the last row are
+            // far away, and candidates past the row end are masked below)
+            const float4 pc = sp[cb + lane];
+            const int tc = __float_as_int(pc.w) & 15;
             unsigned acc = 0u, band = 0u;
-#pragma unroll
-            for (int t = 0; t < 32; t++) {
-              const float4 pj = sp[cb + t];
-              const float ddx = pix - pj.x, ddy = piy - pj.y, ddz = piz - pj.z;
+            for (int a = 0; a < na; a++) {
+              const float4 q = sp[ob + a];
+              const float ddx = q.x - pc.x, ddy = q.y - pc.y, ddz = q.z - pc.z;
               const float r2 = ddx * ddx + ddy * ddy + ddz * ddz;
               float lo = lo1, hi = hi1;
               if (!SINGLE) {
-                const int tt = ti * ntp1 + (__float_as_int(pj.w) & 15);
+                const int tt = (__float_as_int(q.w) & 15) * ntp1 + tc;
                 lo = cns_lo[tt];
                 hi = cns_hi[tt];
               }
-              acc |= (r2 <= hi) ? (1u << t) : 0u;
-              band |= (r2 >= lo) ? (1u << t) : 0u;
+              const bool in = r2 <= hi;
+              const unsigned m = __ballot_sync(0xffffffffu, in);
+              const unsigned b = __ballot_sync(0xffffffffu, in && r2 >= lo);
+              if (lane == a) {
+                acc = m;
+                band = b;
+              }
             }
             // candidates past the row end are not neighbours
             acc &= nc == 32 ? 0xffffffffu : ((1u << nc) - 1u);
@@ -438,7 +456,7 @@ __global__ void __launch_bounds__(kNeighThreads) k_neigh_tiles(
                 // inside the FP32 uncertainty band: the reference's FP64 test
                 if ((band >> t) & 1u) {
                   const int id = idL - warp + (int)(bits & 7u);
-                  if (!exact_pair(xi, x4[md_entry_j(bits)], s_sh[id][0], s_sh[id][1], s_sh[id][2],
+                  if (!exact_pair(x4[i], x4[md_entry_j(bits)], s_sh[id][0], s_sh[id][1], s_sh[id][2],
                                   SINGLE ? cut1 : cns[ti * ntp1 + (__float_as_int(sp[m].w) & 15)]))
                     continue;
                 }
@@ -596,6 +614,36 @@ __global__ void k_prefix_ll(int n, const int *__restrict__ cnt, long long *__res
 
 }  // namespace
 
+// Staging capacity of a builder tile: 1.25 x the atoms of kStageCells cells
+// at the densest replica's mean count per cell, or the most any tile staged
+// in an earlier build if that is larger, rounded up to 128 and at most
+// kStageCapMax.  A tile that stages more atoms takes the global-memory path
+// (same list, slower); a smaller capacity leaves room for more resident
+// CTAs per SM.
+int md_stage_cap(const b200_ctx *c) {
+  double per_cell = c->ncells > 0 ? (double)c->n / c->ncells : 0.0;
+  for (int r = 0; r < c->nrep; r++) {
+    const BoxGeom &b = c->rep_box[r];
+    const double d = (double)c->rep_natoms[r] / ((double)b.ncell[0] * b.ncell[1] * b.ncell[2]);
+    per_cell = d > per_cell ? d : per_cell;
+  }
+  int cap = (int)(1.25 * kStageCells * per_cell) + 64;
+  if (c->stage_need > cap) cap = c->stage_need;
+  cap = (cap + 127) & ~127;
+  if (cap < 256) cap = 256;
+  return cap < kStageCapMax ? cap : kStageCapMax;
+}
+
+// After a build: raise the staging capacity when some tile staged more atoms
+// than the current one holds.  Returns true when the capacity changed (the
+// caller re-captures its graphs).
+bool md_stage_feedback(b200_ctx *c, int staged_max) {
+  const int cap = md_stage_cap(c);
+  if (staged_max <= cap || cap >= kStageCapMax) return false;
+  c->stage_need = staged_max + staged_max / 10;
+  return md_stage_cap(c) != cap;
+}
+
 static cudaError_t launch_scan(b200_ctx *c, int m, const int *in, int *out, const int *flag) {
   int tiles = (m + kScanTile - 1) / kScanTile;
   if (tiles > kScanTile) return cudaErrorInvalidValue;
@@ -652,17 +700,19 @@ cudaError_t md_rebuild(b200_ctx *c, const int *d_flag) {
     const int tiles = c->nrep ? c->ntiles
                               : ((c->box.ncell[0] + kTileCells - 1) / kTileCells) *
                                     c->box.ncell[1] * c->box.ncell[2];
+    const int cap = md_stage_cap(c);
+    const size_t smem = neigh_smem(cap);
 #define MD_NEIGH_ARGS                                                                         \
-  n, c->stride, c->capacity, c->box, R, c->ntypes + 1, c->cutneighsq_dev, c->x4, c->cell_start, \
-      c->nlist, c->numneigh, c->status, d_flag
+  n, c->stride, c->capacity, cap, c->box, R, c->ntypes + 1, c->cutneighsq_dev, c->x4,        \
+      c->cell_start, c->nlist, c->numneigh, c->status, d_flag
     if (c->ntypes == 1 && !c->nrep)
-      k_neigh_tiles<true, false><<<tiles, kNeighThreads, 0, c->stream>>>(MD_NEIGH_ARGS);
+      k_neigh_tiles<true, false><<<tiles, kNeighThreads, smem, c->stream>>>(MD_NEIGH_ARGS);
     else if (c->ntypes == 1)
-      k_neigh_tiles<true, true><<<tiles, kNeighThreads, 0, c->stream>>>(MD_NEIGH_ARGS);
+      k_neigh_tiles<true, true><<<tiles, kNeighThreads, smem, c->stream>>>(MD_NEIGH_ARGS);
     else if (!c->nrep)
-      k_neigh_tiles<false, false><<<tiles, kNeighThreads, 0, c->stream>>>(MD_NEIGH_ARGS);
+      k_neigh_tiles<false, false><<<tiles, kNeighThreads, smem, c->stream>>>(MD_NEIGH_ARGS);
     else
-      k_neigh_tiles<false, true><<<tiles, kNeighThreads, 0, c->stream>>>(MD_NEIGH_ARGS);
+      k_neigh_tiles<false, true><<<tiles, kNeighThreads, smem, c->stream>>>(MD_NEIGH_ARGS);
 #undef MD_NEIGH_ARGS
   }
   k_build_done<<<1, 1, 0, c->stream>>>(c->status, c->check, d_flag);
