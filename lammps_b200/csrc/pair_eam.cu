@@ -44,6 +44,18 @@ __device__ __forceinline__ void decode(unsigned int e, int &j, int &dx, int &dy,
   md_entry(e, j, dx, dy, dz);
 }
 
+// Spline knot and fraction of the mixed form from p = x * rdx + 1 >= 1:
+// m = min(floor(p), mmax), frac = min(p - m, 1) -- the reference's
+// static_cast<int> truncation (equal to floor here, p > 0) and clamps.  The
+// floor comes from a round-down add of 2^23, which leaves floor(p) in the
+// low mantissa bits (exact for p < 2^23), instead of float-to-integer and
+// integer-to-float conversions.
+__device__ __forceinline__ void knot_f(float p, int mmax, int &m, float &frac) {
+  const float t = __fadd_rd(p, 8388608.0f);
+  m = min(__float_as_int(t) - 0x4B000000, mmax);
+  frac = fminf(p - fminf(t - 8388608.0f, (float)mmax), 1.0f);
+}
+
 // Embedding F(rho) and F'(rho) of one atom, FP64, reference clamps.
 __device__ __forceinline__ void embed(const EamArgs &a, int itype_frho, double rho, double &fp,
                                       double &phi) {
@@ -58,7 +70,7 @@ __device__ __forceinline__ void embed(const EamArgs &a, int itype_frho, double r
   if (rho > a.rhomax) phi += fp * (rho - a.rhomax);
 }
 
-template <int TPA, bool EV, bool ATOM, bool MIXED>
+template <int TPA, bool EV, bool ATOM, bool MIXED, bool SINGLE>
 __global__ void __launch_bounds__(128) k_eam_rho(EamArgs a, const double4 *__restrict__ x4,
                                                  const float4 *__restrict__ xr) {
   __shared__ int s_t2rhor[TABSZ];
@@ -120,6 +132,9 @@ __global__ void __launch_bounds__(128) k_eam_rho(EamArgs a, const double4 *__res
       const float csx = (float)a.box.cs[0], csy4 = 0.25f * (float)a.box.cs[1],
                   csz16 = 0.0625f * (float)a.box.cs[2];
       const float cutf = (float)a.cutforcesq, rdrf = (float)a.rdr;
+      // one element: the density spline row of every pair
+      const float *rrow =
+          SINGLE ? a.rhor_f + (size_t)s_t2rhor[a.ntp1 + 1] * (a.nr + 1) * 8 : nullptr;
       const int4 *nl4 = reinterpret_cast<const int4 *>(a.nlist);
       for (int c4 = lane; 4 * c4 < num; c4 += TPA) {
         const int4 e4 = nl4[(size_t)c4 * a.stride + i];
@@ -138,14 +153,13 @@ __global__ void __launch_bounds__(128) k_eam_rho(EamArgs a, const double4 *__res
           const float delz = fmaf(-md_code_dz16(ee[u]), csz16, xi.z - xj.z);
           const float rsq = delx * delx + dely * dely + delz * delz;
           if (rsq < cutf) {
-            float p = sqrtf(rsq) * rdrf + 1.0f;
-            int m = (int)p;
-            m = min(m, a.nr - 1);
-            p -= (float)m;
-            p = fminf(p, 1.0f);
-            const int tab = s_t2rhor[__float_as_int(xj.w) * a.ntp1 + ti];
-            const float4 c =
-                *reinterpret_cast<const float4 *>(a.rhor_f + ((size_t)tab * (a.nr + 1) + m) * 8);
+            int m;
+            float p;
+            knot_f(rsq * rsqrtf(rsq) * rdrf + 1.0f, a.nr - 1, m, p);
+            const float *row = SINGLE ? rrow
+                                      : a.rhor_f + (size_t)s_t2rhor[__float_as_int(xj.w) * a.ntp1 + ti] *
+                                                       (a.nr + 1) * 8;
+            const float4 c = __ldg(reinterpret_cast<const float4 *>(row + (size_t)m * 8));
             crho += ((c.x * p + c.y) * p + c.z) * p + c.w;
           }
         }
@@ -169,7 +183,7 @@ __global__ void __launch_bounds__(128) k_eam_rho(EamArgs a, const double4 *__res
   if (EV) block_partials_finish<7>(acc, red, a.partial, a.counter, a.ev, false);
 }
 
-template <int TPA, bool EV, bool ATOM, bool MIXED>
+template <int TPA, bool EV, bool ATOM, bool MIXED, bool SINGLE>
 __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__restrict__ x4,
                                                    const float4 *__restrict__ xr) {
   __shared__ int s_t2rhor[TABSZ];
@@ -267,6 +281,10 @@ __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__r
       const float csx = (float)a.box.cs[0], csy4 = 0.25f * (float)a.box.cs[1],
                   csz16 = 0.0625f * (float)a.box.cs[2];
       const float cutf = (float)a.cutforcesq, rdrf = (float)a.rdr;
+      // one element: the density-derivative and pair spline rows of every pair
+      const float *drow1 =
+          SINGLE ? a.rhor_f + (size_t)s_t2rhor[a.ntp1 + 1] * (a.nr + 1) * 8 + 4 : nullptr;
+      const float *zrow1 = SINGLE ? a.z2r_f + (size_t)s_t2z2r[a.ntp1 + 1] * (a.nr + 1) * 8 : nullptr;
       const int4 *nl4 = reinterpret_cast<const int4 *>(a.nlist);
       for (int c4 = lane; 4 * c4 < num; c4 += TPA) {
        const int4 e4 = nl4[(size_t)c4 * a.stride + i];
@@ -294,23 +312,24 @@ __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__r
           const int tj = __float_as_int(xj.w);
           const float recip = rsqrtf(rsq);
           const float r = rsq * recip;
-          float p = r * rdrf + 1.0f;
-          int m = (int)p;
-          m = min(m, a.nr - 1);
-          p -= (float)m;
-          p = fminf(p, 1.0f);
-          const float4 ci = *reinterpret_cast<const float4 *>(
-              a.rhor_f + ((size_t)s_t2rhor[ti * a.ntp1 + tj] * (a.nr + 1) + m) * 8 + 4);
+          int m;
+          float p;
+          knot_f(r * rdrf + 1.0f, a.nr - 1, m, p);
+          const size_t o8 = (size_t)m * 8;
+          const float *drow =
+              SINGLE ? drow1 : a.rhor_f + (size_t)s_t2rhor[ti * a.ntp1 + tj] * (a.nr + 1) * 8 + 4;
+          const float4 ci = __ldg(reinterpret_cast<const float4 *>(drow + o8));
           const float rhoip = (ci.x * p + ci.y) * p + ci.z;
           float rhojp = rhoip;
-          if (!a.rhor_sym) {
-            const float4 cj = *reinterpret_cast<const float4 *>(
-                a.rhor_f + ((size_t)s_t2rhor[tj * a.ntp1 + ti] * (a.nr + 1) + m) * 8 + 4);
+          if (!SINGLE && !a.rhor_sym) {
+            const float4 cj = __ldg(reinterpret_cast<const float4 *>(
+                a.rhor_f + ((size_t)s_t2rhor[tj * a.ntp1 + ti] * (a.nr + 1) + m) * 8 + 4));
             rhojp = (cj.x * p + cj.y) * p + cj.z;
           }
-          const float *zb = a.z2r_f + ((size_t)s_t2z2r[ti * a.ntp1 + tj] * (a.nr + 1) + m) * 8;
-          const float4 zv = *reinterpret_cast<const float4 *>(zb);
-          const float4 zd = *reinterpret_cast<const float4 *>(zb + 4);
+          const float *zb =
+              (SINGLE ? zrow1 : a.z2r_f + (size_t)s_t2z2r[ti * a.ntp1 + tj] * (a.nr + 1) * 8) + o8;
+          const float4 zv = __ldg(reinterpret_cast<const float4 *>(zb));
+          const float4 zd = __ldg(reinterpret_cast<const float4 *>(zb + 4));
           const float z2p = (zd.x * p + zd.y) * p + zd.z;
           const float z2 = ((zv.x * p + zv.y) * p + zv.z) * p + zv.w;
           const float phi = z2 * recip;
@@ -375,27 +394,34 @@ void record_mid(b200_ctx *c, cudaEvent_t mid) {
     cudaEventRecord(mid, c->stream);
 }
 
-template <int TPA, bool EV, bool ATOM>
+template <int TPA, bool EV, bool ATOM, bool SINGLE>
 void launch_t(b200_ctx *c, const EamArgs &a, cudaEvent_t mid) {
   const int B = 128;
   const int grid = md_blocks((long long)a.n * TPA, B);
   if (c->prec == B200_PREC_MIXED) {
-    k_eam_rho<TPA, EV, ATOM, true><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
+    k_eam_rho<TPA, EV, ATOM, true, SINGLE><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
     record_mid(c, mid);
-    k_eam_force<TPA, EV, ATOM, true><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
+    k_eam_force<TPA, EV, ATOM, true, SINGLE><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
   } else {
-    k_eam_rho<TPA, EV, ATOM, false><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
+    k_eam_rho<TPA, EV, ATOM, false, SINGLE><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
     record_mid(c, mid);
-    k_eam_force<TPA, EV, ATOM, false><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
+    k_eam_force<TPA, EV, ATOM, false, SINGLE><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
   }
   c->launches += 2;
 }
 
+template <int TPA, bool SINGLE>
+void launch_ts(b200_ctx *c, const EamArgs &a, bool ev, bool atom, cudaEvent_t mid) {
+  if (!ev) launch_t<TPA, false, false, SINGLE>(c, a, mid);
+  else if (!atom) launch_t<TPA, true, false, SINGLE>(c, a, mid);
+  else launch_t<TPA, true, true, SINGLE>(c, a, mid);
+}
+
 template <int TPA>
 void launch_tpa(b200_ctx *c, const EamArgs &a, bool ev, bool atom, cudaEvent_t mid) {
-  if (!ev) launch_t<TPA, false, false>(c, a, mid);
-  else if (!atom) launch_t<TPA, true, false>(c, a, mid);
-  else launch_t<TPA, true, true>(c, a, mid);
+  // one element type: spline rows hoisted out of the pair loop (mixed form)
+  if (c->ntypes == 1) launch_ts<TPA, true>(c, a, ev, atom, mid);
+  else launch_ts<TPA, false>(c, a, ev, atom, mid);
 }
 
 }  // namespace
