@@ -58,6 +58,16 @@ def eam32k_inputs():
     return x, v, np.array([20 * 3.615] * 3)
 
 
+def eam4m_inputs():
+    """The EAM workload at 4,000,000 atoms: fcc 100^3 at a = 3.615 A, the same
+    Gaussian 1600 K velocities (seed 376847, loop geom)."""
+    from lammps_b200 import inputs
+    x = inputs.lattice("fcc", 100, 100, 100, 3.615)
+    v = inputs.velocity_create(x, np.ones(len(x), np.int32), np.array([0.0, 63.55]), 1600.0,
+                               376847, "metal", gaussian=True, loop="geom")
+    return x, v, np.array([100 * 3.615] * 3)
+
+
 def make_eam32k(precision, setfl, x, v, hi):
     from lammps_b200 import PairEAMAlloy, System
     s = System("metal", precision, device=DEVICE)
@@ -242,17 +252,30 @@ def time_form(sysm, torch, flush, K, W, start, timing=False):
     return sum(ms), ms
 
 
-def e2e_run(sysm, x_pin, v_pin, K):
-    """Public-API end to end: host buffers in, host results out, per bench step."""
+_PINNED = []  # torch tensors that own the page-locked memory of the e2e buffers
+
+
+def pinned(torch, a):
+    """A page-locked host copy of array `a` (a numpy view of a pinned torch tensor)."""
+    t = torch.empty(a.shape, dtype=getattr(torch, str(a.dtype)), pin_memory=True)
+    _PINNED.append(t)
+    out = t.numpy()
+    out[...] = a
+    return out
+
+
+def e2e_run(sysm, x_pin, v_pin, t_pin, out_pin, K):
+    """Public-API end to end: page-locked host buffers in, host results out,
+    per bench step (upload, setup, the MD steps, download)."""
     n = x_pin.shape[0]
     t0 = time.perf_counter()
     for _ in range(K):
-        sysm.set_atoms(x_pin, None, v_pin)
+        sysm.set_atoms(x_pin, t_pin, v_pin)
         sysm.setup()
         sysm.run(MD_STEPS)
-        out = sysm.download()
+        out = sysm.download(out_pin)
     t1 = time.perf_counter()
-    h2d = x_pin.nbytes + v_pin.nbytes + n * 4
+    h2d = x_pin.nbytes + v_pin.nbytes + t_pin.nbytes
     d2h = out["x"].nbytes + out["v"].nbytes + out["f"].nbytes + out["image"].nbytes
     return (t1 - t0) * 1e3, h2d, d2h
 
@@ -380,6 +403,12 @@ def profile_case(args):
     elif work == "lj4m":
         x, v, hi = lj4m_inputs()
         s = make_lj(prec, x, v, hi)
+    elif work == "eam4m":
+        tmp = tempfile.mkdtemp(prefix="b200prof_")
+        from lammps_b200.eam_synth import write_setfl
+        setfl = write_setfl(os.path.join(tmp, "Cu_synth.eam.alloy"))
+        x, v, hi = eam4m_inputs()
+        s = make_eam32k(prec, setfl, x, v, hi)
     elif work == "c3":
         from lammps_b200.replicas import make_batch, replica_batch
         batch = replica_batch(nrep=256)
@@ -502,10 +531,13 @@ def main():
                 "step": step_roofline(n, step_ms, peak, clk)}
 
     # ---- end to end through the public API --------------------------------
-    x_pin = np.ascontiguousarray(x)
-    v_pin = np.ascontiguousarray(v)
-    e2e_run(sysm, x_pin, v_pin, 1)
-    e_ms, h2d, d2h = e2e_run(sysm, x_pin, v_pin, K)
+    x_pin = pinned(torch, np.ascontiguousarray(x, dtype=np.float64))
+    v_pin = pinned(torch, np.ascontiguousarray(v, dtype=np.float64))
+    t_pin = pinned(torch, np.ones(n, np.int32))
+    out_pin = {k: pinned(torch, np.zeros((n, 3), dt)) for k, dt in
+               (("x", np.float64), ("v", np.float64), ("f", np.float64), ("image", np.int32))}
+    e2e_run(sysm, x_pin, v_pin, t_pin, out_pin, 1)
+    e_ms, h2d, d2h = e2e_run(sysm, x_pin, v_pin, t_pin, out_pin, K)
     e_ms = allmax(e_ms, ws, torch)
     e2e = {"value": ws * n * MD_STEPS * K / (e_ms * 1e3), "unit": "Matom-steps/s",
            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
@@ -544,6 +576,30 @@ def main():
         f_ms = lj["mixed_phases_ms_per_step"]["pair1"]
         lj["force_kernel_gbs"] = 48.0 * len(x4) / (f_ms * 1e-3) / 1e9
         extras["lj_4M"] = lj
+        # the EAM workload at 4M atoms: the density and force kernels at a
+        # size where they are not launch- and latency-bound
+        xe, ve, hie = eam4m_inputs()
+        em = {"atoms": len(xe), "note": "fcc 100^3 a=3.615, synthetic setfl, 1600 K, skin 1.0, "
+                                       "every 1 delay 5 check yes, 100 steps per bench step"}
+        for prec in ("mixed", "fp64"):
+            s = make_eam32k(prec, setfl, xe, ve, hie)
+            k4 = max(2, K // 3)
+            t, _ = time_form(s, torch, flush, k4, 2, (xe, ve))
+            s.set_timing(True)
+            exte = torch.cuda.ExternalStream(s.stream)
+            device_time_run(s, torch, exte, flush, MD_STEPS, (xe, ve))
+            s.timing(reset=True)
+            device_time_run(s, torch, exte, flush, MD_STEPS, (xe, ve))
+            phe = s.timing(reset=True)
+            em[prec] = len(xe) * MD_STEPS * k4 / (t * 1e3)
+            ph = {k: phe[k] / max(phe["steps"], 1) for k in s.PHASES}
+            em[prec + "_phases_ms_per_step"] = ph
+            # algorithmic bytes: density pass 40 B/atom, force pass 56 B/atom
+            em[prec + "_rho_kernel_gbs"] = 40.0 * len(xe) / (ph["pair1"] * 1e-3) / 1e9
+            em[prec + "_force_kernel_gbs"] = 56.0 * len(xe) / (ph["pair2"] * 1e-3) / 1e9
+            s.close()
+        em["mixed_over_fp64"] = em["mixed"] / em["fp64"]
+        extras["eam_4M"] = em
 
     if not args.no_extras:
         from lammps_b200.replicas import replica_batch

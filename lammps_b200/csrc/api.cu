@@ -58,6 +58,28 @@ void invalidate_graphs(b200_ctx *c) {
   c->graph_valid = false;
 }
 
+// The context's transfer staging: `parts` byte counts laid out one after
+// another (256-byte aligned) in one device buffer that only grows.  Growing
+// synchronizes the stream first, since queued copies may still use it.
+int xfer_parts(b200_ctx *c, int nparts, const size_t *bytes, char **ptrs) {
+  size_t total = 0;
+  for (int k = 0; k < nparts; k++) total += (bytes[k] + 255) & ~(size_t)255;
+  if (total > c->xfer_bytes) {
+    CK(cudaStreamSynchronize(c->stream));
+    if (c->xfer) cudaFree(c->xfer);
+    c->xfer = nullptr;
+    c->xfer_bytes = 0;
+    CK(cudaMalloc((void **)&c->xfer, total));
+    c->xfer_bytes = total;
+  }
+  size_t off = 0;
+  for (int k = 0; k < nparts; k++) {
+    ptrs[k] = bytes[k] ? c->xfer + off : nullptr;
+    off += (bytes[k] + 255) & ~(size_t)255;
+  }
+  return B200_OK;
+}
+
 // ---- kernels local to the ABI ------------------------------------------------
 
 __global__ void k_upload(int n, int stride, const double *__restrict__ x,
@@ -674,7 +696,7 @@ int b200_destroy(b200_ctx *c) {
   invalidate_graphs(c);
   dfree(c->x4); dfree(c->x4b); dfree(c->v); dfree(c->vb); dfree(c->f);
   dfree(c->orig); dfree(c->origb); dfree(c->image); dfree(c->imageb); dfree(c->cell);
-  dfree(c->xr); dfree(c->xhold); dfree(c->rho); dfree(c->fp); dfree(c->fpf); dfree(c->mass_dev);
+  dfree(c->xr); dfree(c->xhold); dfree(c->xfer); dfree(c->rho); dfree(c->fp); dfree(c->fpf); dfree(c->mass_dev);
   dfree(c->cell_count); dfree(c->cell_start); dfree(c->scan_tmp);
   dfree(c->slot); dfree(c->perm); dfree(c->cell_tmp);
   dfree(c->nlist); dfree(c->numneigh); dfree(c->partial); dfree(c->counter); dfree(c->ev);
@@ -686,7 +708,7 @@ int b200_destroy(b200_ctx *c) {
   dfree(c->snap_orig); dfree(c->snap_image); dfree(c->snap_cell); dfree(c->snap_xr);
   dfree(c->snap_status);
   dfree(c->eam.frho); dfree(c->eam.rhor); dfree(c->eam.z2r);
-  dfree(c->eam.frho_f); dfree(c->eam.rhor_f); dfree(c->eam.z2r_f);
+  dfree(c->eam.frho_f); dfree(c->eam.rhor_f); dfree(c->eam.z2r_f); dfree(c->eam.fz_f);
   for (auto &ev : c->ph_event)
     if (ev) cudaEventDestroy(ev);
   for (auto ev : c->ev_pool) cudaEventDestroy(ev);
@@ -832,6 +854,18 @@ int b200_set_eam(b200_ctx *c, int ntypes, int nrho, double drho, int nr, double 
   if (!rc) rc = pack(rhor_spline, nrhor, nr, &E.rhor, &E.rhor_f);
   if (!rc) rc = pack(z2r_spline, nz2r, nr, &E.z2r, &E.z2r_f);
   if (rc) return rc;
+  if (ntypes == 1) {
+    // one element: the z2 value and rho' coefficients of each knot in one
+    // 32-byte record for the mixed force kernel
+    const size_t ri = (size_t)E.type2rhor[ntp1 + 1], zi = (size_t)E.type2z2r[ntp1 + 1];
+    std::vector<float> fz((size_t)(nr + 1) * 8, 0.0f);
+    for (size_t m = 0; m <= (size_t)nr; m++) {
+      for (int k = 0; k < 4; k++) fz[m * 8 + k] = (float)z2r_spline[(zi * (nr + 1) + m) * 7 + 3 + k];
+      for (int k = 0; k < 3; k++) fz[m * 8 + 4 + k] = (float)rhor_spline[(ri * (nr + 1) + m) * 7 + k];
+    }
+    CK(dalloc(&E.fz_f, fz.size()));
+    CK(cudaMemcpy(E.fz_f, fz.data(), fz.size() * sizeof(float), cudaMemcpyHostToDevice));
+  }
   c->ntypes = ntypes;
   c->pstyle = B200_PAIR_EAM;
   invalidate_graphs(c);
@@ -882,11 +916,13 @@ int b200_upload_atoms(b200_ctx *c, int n, const double *x, const double *v, cons
   }
   c->n = n;
   CK(cudaMemsetAsync(c->f, 0, 3 * (size_t)c->stride * sizeof(double), c->stream));
-  double *dx = nullptr, *dv = nullptr;
-  int *dt = nullptr;
-  CK(cudaMallocAsync((void **)&dx, 3 * (size_t)n * sizeof(double), c->stream));
-  if (v) CK(cudaMallocAsync((void **)&dv, 3 * (size_t)n * sizeof(double), c->stream));
-  CK(cudaMallocAsync((void **)&dt, (size_t)n * sizeof(int), c->stream));
+  char *st[3];
+  const size_t sb[3] = {3 * (size_t)n * sizeof(double), v ? 3 * (size_t)n * sizeof(double) : 0,
+                        (size_t)n * sizeof(int)};
+  int rc = xfer_parts(c, 3, sb, st);
+  if (rc) return rc;
+  double *dx = reinterpret_cast<double *>(st[0]), *dv = reinterpret_cast<double *>(st[1]);
+  int *dt = reinterpret_cast<int *>(st[2]);
   CK(cudaMemcpyAsync(dx, x, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   if (v) CK(cudaMemcpyAsync(dv, v, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(dt, type, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, c->stream));
@@ -894,9 +930,6 @@ int b200_upload_atoms(b200_ctx *c, int n, const double *x, const double *v, cons
                                                      c->orig, c->image, c->cell);
   c->launches++;
   CK(cudaGetLastError());
-  CK(cudaFreeAsync(dx, c->stream));
-  if (dv) CK(cudaFreeAsync(dv, c->stream));
-  CK(cudaFreeAsync(dt, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->have_atoms = true;
   c->sorted_once = false;
@@ -910,12 +943,14 @@ int b200_download_atoms(b200_ctx *c, double *x, double *v, double *f, int *image
   if (!c->have_atoms) return set_err(c, B200_ERR_STATE, "no atoms uploaded");
   CK(cudaSetDevice(c->device));
   const int n = c->n;
-  double *dx = nullptr, *dv = nullptr, *df = nullptr;
-  int *di = nullptr;
-  if (x) CK(cudaMallocAsync((void **)&dx, 3 * (size_t)n * sizeof(double), c->stream));
-  if (v) CK(cudaMallocAsync((void **)&dv, 3 * (size_t)n * sizeof(double), c->stream));
-  if (f) CK(cudaMallocAsync((void **)&df, 3 * (size_t)n * sizeof(double), c->stream));
-  if (image) CK(cudaMallocAsync((void **)&di, 3 * (size_t)n * sizeof(int), c->stream));
+  char *st[4];
+  const size_t d3 = 3 * (size_t)n * sizeof(double);
+  const size_t sb[4] = {x ? d3 : 0, v ? d3 : 0, f ? d3 : 0, image ? 3 * (size_t)n * sizeof(int) : 0};
+  int rc = xfer_parts(c, 4, sb, st);
+  if (rc) return rc;
+  double *dx = reinterpret_cast<double *>(st[0]), *dv = reinterpret_cast<double *>(st[1]);
+  double *df = reinterpret_cast<double *>(st[2]);
+  int *di = reinterpret_cast<int *>(st[3]);
   k_unsort<<<md_blocks(n, 256), 256, 0, c->stream>>>(n, c->stride, c->orig, c->x4, c->v, c->f,
                                                      c->image, dx, dv, df, di);
   c->launches++;
@@ -924,10 +959,6 @@ int b200_download_atoms(b200_ctx *c, double *x, double *v, double *f, int *image
   if (v) CK(cudaMemcpyAsync(v, dv, 3 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   if (f) CK(cudaMemcpyAsync(f, df, 3 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   if (image) CK(cudaMemcpyAsync(image, di, 3 * (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-  if (dx) CK(cudaFreeAsync(dx, c->stream));
-  if (dv) CK(cudaFreeAsync(dv, c->stream));
-  if (df) CK(cudaFreeAsync(df, c->stream));
-  if (di) CK(cudaFreeAsync(di, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return B200_OK;
 }
@@ -968,21 +999,20 @@ int b200_pair_compute(b200_ctx *c, int eflag, int vflag, double *eng, double vir
   const bool vg = (vflag % 4) != 0, va = (vflag & 4) != 0;
   const bool ev = eg || ea || vg || va;
   const bool atom = ea || va;
-  double *de = nullptr, *dv = nullptr;
   const int n = c->n;
-  if (ea && eatom) {
-    CK(cudaMallocAsync((void **)&de, (size_t)n * sizeof(double), c->stream));
-    CK(cudaMemsetAsync(de, 0, (size_t)n * sizeof(double), c->stream));
-  }
-  if (va && vatom) CK(cudaMallocAsync((void **)&dv, 6 * (size_t)n * sizeof(double), c->stream));
-  int rc = pair_compute_dev(c, ev, atom, de, dv);
+  char *st[2];
+  const size_t sb[2] = {(ea && eatom) ? (size_t)n * sizeof(double) : 0,
+                        (va && vatom) ? 6 * (size_t)n * sizeof(double) : 0};
+  int rc = xfer_parts(c, 2, sb, st);
+  if (rc) return rc;
+  double *de = reinterpret_cast<double *>(st[0]), *dv = reinterpret_cast<double *>(st[1]);
+  if (de) CK(cudaMemsetAsync(de, 0, (size_t)n * sizeof(double), c->stream));
+  rc = pair_compute_dev(c, ev, atom, de, dv);
   if (rc) return rc;
   double h[8];
   if (ev) CK(cudaMemcpyAsync(h, c->ev, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   if (de) CK(cudaMemcpyAsync(eatom, de, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   if (dv) CK(cudaMemcpyAsync(vatom, dv, 6 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  if (de) CK(cudaFreeAsync(de, c->stream));
-  if (dv) CK(cudaFreeAsync(dv, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   if (ev) {
     if (eg && eng) *eng = h[0];

@@ -30,6 +30,7 @@ struct EAMDev {
   // spline tables, 8 coefficients per knot (7 used): [table][knot][8]
   double *frho = nullptr, *rhor = nullptr, *z2r = nullptr;
   float *frho_f = nullptr, *rhor_f = nullptr, *z2r_f = nullptr;
+  float *fz_f = nullptr;  // one element: [z2 c3..c6 | rho' c0..c2 | 0] per knot
   int type2frho[MD_MAXTYPES + 1];
   int type2rhor[(MD_MAXTYPES + 1) * (MD_MAXTYPES + 1)];
   int type2z2r[(MD_MAXTYPES + 1) * (MD_MAXTYPES + 1)];
@@ -96,6 +97,10 @@ struct b200_ctx {
   int *cell = nullptr;        // packed cell of each sorted atom
   float4 *xr = nullptr;       // mixed: cell-relative coordinates
   double4 *xhold = nullptr;   // positions at the last build (check yes)
+  // device staging of host transfers (upload, download, per-atom energy and
+  // virial), kept between calls so a call maps no new memory
+  char *xfer = nullptr;
+  size_t xfer_bytes = 0;
   double *rho = nullptr, *fp = nullptr;
   float *fpf = nullptr;
   double *mass_dev = nullptr; // per-type masses (device)

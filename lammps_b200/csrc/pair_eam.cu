@@ -16,7 +16,13 @@
 // so one float4 load gives a value and one a derivative; distances from the
 // FP32 cell-relative coordinates; fp_j gathered as FP32; sums in FP64.  The
 // embedding step F(rho) stays FP64 in both forms.  Each thread reads four
-// list entries with one 16-byte load and issues their gathers together.
+// list entries with one 16-byte load and issues their gathers together; the
+// mixed kernels load the next slab's entries before using the current one.
+// With one element the mixed force kernel reads each knot's z2 value and
+// rho' coefficients as one 32-byte record (fz_f) and forms the z2
+// derivative from the value coefficients, (3 c3 p^2 + 2 c4 p + c5) / dr,
+// the relation PairEAM::interpolate (:723-751) builds the stored derivative
+// coefficients from.
 #include "md_state.h"
 
 namespace {
@@ -30,6 +36,7 @@ struct EamArgs {
   double rdr, rdrho, rhomax, cutforcesq;
   const double *frho, *rhor, *z2r;
   const float *rhor_f, *z2r_f;
+  const float *fz_f;  // one element: per knot [z2 c3 c4 c5 c6 | rho' c0 c1 c2 | 0]
   const int *t2frho, *t2rhor, *t2z2r;  // device copies of the type maps
   double *rho, *fp;
   float *fpf;
@@ -136,8 +143,12 @@ __global__ void __launch_bounds__(128) k_eam_rho(EamArgs a, const double4 *__res
       const float *rrow =
           SINGLE ? a.rhor_f + (size_t)s_t2rhor[a.ntp1 + 1] * (a.nr + 1) * 8 : nullptr;
       const int4 *nl4 = reinterpret_cast<const int4 *>(a.nlist);
-      for (int c4 = lane; 4 * c4 < num; c4 += TPA) {
-        const int4 e4 = nl4[(size_t)c4 * a.stride + i];
+      const int nslab = (num + 3) >> 2;
+      int4 en = make_int4(0, 0, 0, 0);
+      if (lane < nslab) en = __ldcs(&nl4[(size_t)lane * a.stride + i]);
+      for (int c4 = lane; c4 < nslab; c4 += TPA) {
+        const int4 e4 = en;
+        if (c4 + TPA < nslab) en = __ldcs(&nl4[(size_t)(c4 + TPA) * a.stride + i]);
         // whole slabs: pad entries in the last slab fail the cutoff test
         const unsigned int ee[4] = {(unsigned int)e4.x, (unsigned int)e4.y, (unsigned int)e4.z,
                                     (unsigned int)e4.w};
@@ -282,12 +293,15 @@ __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__r
                   csz16 = 0.0625f * (float)a.box.cs[2];
       const float cutf = (float)a.cutforcesq, rdrf = (float)a.rdr;
       // one element: the density-derivative and pair spline rows of every pair
-      const float *drow1 =
-          SINGLE ? a.rhor_f + (size_t)s_t2rhor[a.ntp1 + 1] * (a.nr + 1) * 8 + 4 : nullptr;
-      const float *zrow1 = SINGLE ? a.z2r_f + (size_t)s_t2z2r[a.ntp1 + 1] * (a.nr + 1) * 8 : nullptr;
+      const float *drow1 = SINGLE ? a.fz_f + 4 : nullptr;
+      const float *zrow1 = SINGLE ? a.fz_f : nullptr;
       const int4 *nl4 = reinterpret_cast<const int4 *>(a.nlist);
-      for (int c4 = lane; 4 * c4 < num; c4 += TPA) {
-       const int4 e4 = nl4[(size_t)c4 * a.stride + i];
+      const int nslab = (num + 3) >> 2;
+      int4 en = make_int4(0, 0, 0, 0);
+      if (lane < nslab) en = __ldcs(&nl4[(size_t)lane * a.stride + i]);
+      for (int c4 = lane; c4 < nslab; c4 += TPA) {
+       const int4 e4 = en;
+       if (c4 + TPA < nslab) en = __ldcs(&nl4[(size_t)(c4 + TPA) * a.stride + i]);
        // whole slabs: pad entries in the last slab fail the cutoff test
        const unsigned int ee[4] = {(unsigned int)e4.x, (unsigned int)e4.y, (unsigned int)e4.z,
                                    (unsigned int)e4.w};
@@ -329,8 +343,15 @@ __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__r
           const float *zb =
               (SINGLE ? zrow1 : a.z2r_f + (size_t)s_t2z2r[ti * a.ntp1 + tj] * (a.nr + 1) * 8) + o8;
           const float4 zv = __ldg(reinterpret_cast<const float4 *>(zb));
-          const float4 zd = __ldg(reinterpret_cast<const float4 *>(zb + 4));
-          const float z2p = (zd.x * p + zd.y) * p + zd.z;
+          float z2p;
+          if (SINGLE) {
+            // the z2 derivative from the value coefficients:
+            // (3 c3 p^2 + 2 c4 p + c5) / dr, as PairEAM::interpolate stores it
+            z2p = (fmaf(3.0f * zv.x, p, 2.0f * zv.y) * p + zv.z) * rdrf;
+          } else {
+            const float4 zd = __ldg(reinterpret_cast<const float4 *>(zb + 4));
+            z2p = (zd.x * p + zd.y) * p + zd.z;
+          }
           const float z2 = ((zv.x * p + zv.y) * p + zv.z) * p + zv.w;
           const float phi = z2 * recip;
           const float phip = z2p * recip - phi * recip;
@@ -449,6 +470,7 @@ cudaError_t md_eam_compute(b200_ctx *c, bool ev, bool atom_ev, double *eatom, do
   a.z2r = c->eam.z2r;
   a.rhor_f = c->eam.rhor_f;
   a.z2r_f = c->eam.z2r_f;
+  a.fz_f = c->eam.fz_f;
   // type maps live right after the TAB_* tables in tables_dev (as ints)
   const int *maps = reinterpret_cast<const int *>(c->tables_dev + TAB_COUNT * TABSZ);
   a.t2frho = maps;

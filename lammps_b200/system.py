@@ -127,15 +127,26 @@ class System:
         type_ = np.ones(x.shape[0], np.int32) if type_ is None else type_
         return velocity_create(x, type_, self.mass, t, seed, self.units, gaussian, loop, mom)
 
-    def download(self):
+    def download(self, out=None):
+        """Positions, velocities, forces and image flags in the upload order.
+
+        `out` (optional) is a dict of caller-owned arrays to fill instead of
+        new ones: x, v, f as C-contiguous (n, 3) float64 and image as (n, 3)
+        int32 -- e.g. page-locked host buffers, which the device copies into
+        directly."""
         n = self.n
-        x = np.zeros((n, 3))
-        v = np.zeros((n, 3))
-        f = np.zeros((n, 3))
-        img = np.zeros((n, 3), np.int32)
-        self._ck(self._L.b200_download_atoms(self._h, _abi.dptr(x), _abi.dptr(v), _abi.dptr(f),
-                                             _abi.iptr(img)))
-        return dict(x=x, v=v, f=f, image=img)
+        if out is None:
+            out = dict(x=np.zeros((n, 3)), v=np.zeros((n, 3)), f=np.zeros((n, 3)),
+                       image=np.zeros((n, 3), np.int32))
+        else:
+            for k, dt in (("x", np.float64), ("v", np.float64), ("f", np.float64),
+                          ("image", np.int32)):
+                a = out[k]
+                if a.shape != (n, 3) or a.dtype != dt or not a.flags["C_CONTIGUOUS"]:
+                    raise ValueError(f"download: out[{k!r}] must be a C-contiguous ({n}, 3) {np.dtype(dt)}")
+        self._ck(self._L.b200_download_atoms(self._h, _abi.dptr(out["x"]), _abi.dptr(out["v"]),
+                                             _abi.dptr(out["f"]), _abi.iptr(out["image"])))
+        return out
 
     # ---- actions ---------------------------------------------------------
     def neigh_build(self):
