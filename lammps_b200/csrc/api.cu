@@ -836,11 +836,19 @@ int b200_set_eam(b200_ctx *c, int ntypes, int nrho, double drho, int nr, double 
       if (E.type2rhor[i * ntp1 + j] != E.type2rhor[j * ntp1 + i]) E.rhor_sym = false;
   // repack [table][knot][7] -> [table][knot][8]; FP32 copies reordered
   // [c3 c4 c5 c6 | c0 c1 c2 0] for one-float4 value / derivative loads
-  auto pack = [&](const double *src, int ntab, int nk, double **dd, float **df) -> int {
+  // FP64 rows: embedding [c0..c6 -]; density and pair (reorder) as the FP32
+  // rows, [c3 c4 c5 c6 | c0 c1 c2 -]
+  auto pack = [&](const double *src, int ntab, int nk, double **dd, float **df,
+                  bool reorder) -> int {
     std::vector<double> d8((size_t)ntab * (nk + 1) * 8, 0.0);
     std::vector<float> f8((size_t)ntab * (nk + 1) * 8, 0.0f);
     for (size_t r = 0; r < (size_t)ntab * (nk + 1); r++) {
-      for (int k = 0; k < 7; k++) d8[r * 8 + k] = src[r * 7 + k];
+      if (reorder) {
+        for (int k = 0; k < 4; k++) d8[r * 8 + k] = src[r * 7 + 3 + k];
+        for (int k = 0; k < 3; k++) d8[r * 8 + 4 + k] = src[r * 7 + k];
+      } else {
+        for (int k = 0; k < 7; k++) d8[r * 8 + k] = src[r * 7 + k];
+      }
       for (int k = 0; k < 4; k++) f8[r * 8 + k] = (float)src[r * 7 + 3 + k];
       for (int k = 0; k < 3; k++) f8[r * 8 + 4 + k] = (float)src[r * 7 + k];
     }
@@ -850,9 +858,9 @@ int b200_set_eam(b200_ctx *c, int ntypes, int nrho, double drho, int nr, double 
     CK(cudaMemcpy(*df, f8.data(), f8.size() * sizeof(float), cudaMemcpyHostToDevice));
     return B200_OK;
   };
-  int rc = pack(frho_spline, nfrho, nrho, &E.frho, &E.frho_f);
-  if (!rc) rc = pack(rhor_spline, nrhor, nr, &E.rhor, &E.rhor_f);
-  if (!rc) rc = pack(z2r_spline, nz2r, nr, &E.z2r, &E.z2r_f);
+  int rc = pack(frho_spline, nfrho, nrho, &E.frho, &E.frho_f, false);
+  if (!rc) rc = pack(rhor_spline, nrhor, nr, &E.rhor, &E.rhor_f, true);
+  if (!rc) rc = pack(z2r_spline, nz2r, nr, &E.z2r, &E.z2r_f, true);
   if (rc) return rc;
   if (ntypes == 1) {
     // one element: the z2 value and rho' coefficients of each knot in one

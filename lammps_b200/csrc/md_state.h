@@ -27,7 +27,8 @@ enum {
 struct EAMDev {
   int nrho = 0, nr = 0, nfrho = 0, nrhor = 0, nz2r = 0;
   double drho = 0, dr = 0, rdr = 0, rdrho = 0, rhomax = 0, cutmax = 0, cutforcesq = 0;
-  // spline tables, 8 coefficients per knot (7 used): [table][knot][8]
+  // spline tables, 8 coefficients per knot (7 used): [table][knot][8];
+  // embedding rows [c0..c6 -], density and pair rows [c3 c4 c5 c6 c0 c1 c2 -]
   double *frho = nullptr, *rhor = nullptr, *z2r = nullptr;
   float *frho_f = nullptr, *rhor_f = nullptr, *z2r_f = nullptr;
   float *fz_f = nullptr;  // one element: [z2 c3..c6 | rho' c0..c2 | 0] per knot

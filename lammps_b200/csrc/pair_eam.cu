@@ -9,7 +9,10 @@
 //   k_eam_force  pair force psi'/r using fp_i and the neighbor's own fp_j
 //                (the forward_comm_pair of fp disappears)         (:237-303)
 // Splines are the reference's 7-coefficient cubic tables
-// (PairEAM::interpolate, :723-751), stored 8 doubles per knot; the index
+// (PairEAM::interpolate, :723-751), stored 8 doubles per knot (density and
+// pair rows reordered [c3 c4 c5 c6 | c0 c1 c2 -] so the value and the
+// derivative coefficients are each 16-byte loads; embedding rows as
+// [c0..c6 -]); the index
 // clamps are the reference's: m = min(m, nr-1), p = min(p, 1) for r and
 // m = max(1, min(m, nrho-1)) for rho.
 // Mixed form: FP32 tables reordered per knot as [c3 c4 c5 c6 | c0 c1 c2 -]
@@ -63,6 +66,14 @@ __device__ __forceinline__ void knot_f(float p, int mmax, int &m, float &frac) {
   frac = fminf(p - fminf(t - 8388608.0f, (float)mmax), 1.0f);
 }
 
+// The same for the FP64 form: floor(p) from a round-down add of 2^52 (exact
+// for p < 2^52), and p - m exactly as the reference's p -= m.
+__device__ __forceinline__ void knot_d(double p, int mmax, int &m, double &frac) {
+  const double t = __dadd_rd(p, 4503599627370496.0);
+  m = min((int)(__double_as_longlong(t) - 0x4330000000000000LL), mmax);
+  frac = fmin(p - (double)m, 1.0);
+}
+
 // Embedding F(rho) and F'(rho) of one atom, FP64, reference clamps.
 __device__ __forceinline__ void embed(const EamArgs &a, int itype_frho, double rho, double &fp,
                                       double &phi) {
@@ -102,9 +113,16 @@ __global__ void __launch_bounds__(128) k_eam_rho(EamArgs a, const double4 *__res
       const Shift3 sx = shifts(cx, a.box.ncell[0], a.box.prd[0]);
       const Shift3 sy = shifts(cy, a.box.ncell[1], a.box.prd[1]);
       const Shift3 sz = shifts(cz, a.box.ncell[2], a.box.prd[2]);
+      // one element: the density spline row of every pair
+      const double *rrow =
+          SINGLE ? a.rhor + (size_t)s_t2rhor[a.ntp1 + 1] * (a.nr + 1) * 8 : nullptr;
       const int4 *nl4 = reinterpret_cast<const int4 *>(a.nlist);
-      for (int c4 = lane; 4 * c4 < num; c4 += TPA) {
-        const int4 e4 = nl4[(size_t)c4 * a.stride + i];
+      const int nslab = (num + 3) >> 2;
+      int4 en = make_int4(0, 0, 0, 0);
+      if (lane < nslab) en = __ldcs(&nl4[(size_t)lane * a.stride + i]);
+      for (int c4 = lane; c4 < nslab; c4 += TPA) {
+        const int4 e4 = en;
+        if (c4 + TPA < nslab) en = __ldcs(&nl4[(size_t)(c4 + TPA) * a.stride + i]);
         const int mm = min(4, num - 4 * c4);
         const unsigned int ee[4] = {(unsigned int)e4.x, (unsigned int)e4.y, (unsigned int)e4.z,
                                     (unsigned int)e4.w};
@@ -122,14 +140,16 @@ __global__ void __launch_bounds__(128) k_eam_rho(EamArgs a, const double4 *__res
           const double delz = __dsub_rn(xi.z, __dadd_rn(xj.z, pick(sz, dz)));
           const double rsq = dsq3(delx, dely, delz);
           if (rsq < a.cutforcesq) {
-            double p = __dadd_rn(__dmul_rn(sqrt(rsq), a.rdr), 1.0);
-            int m = (int)p;
-            m = min(m, a.nr - 1);
-            p -= m;
-            p = fmin(p, 1.0);
-            const int tab = s_t2rhor[(int)xj.w * a.ntp1 + ti];
-            const double *c = a.rhor + ((size_t)tab * (a.nr + 1) + m) * 8;
-            rho += ((c[3] * p + c[4]) * p + c[5]) * p + c[6];
+            int m;
+            double p;
+            knot_d(__dadd_rn(__dmul_rn(sqrt(rsq), a.rdr), 1.0), a.nr - 1, m, p);
+            const double *row =
+                SINGLE ? rrow : a.rhor + (size_t)s_t2rhor[(int)xj.w * a.ntp1 + ti] * (a.nr + 1) * 8;
+            // knot layout [c3 c4 c5 c6 | c0 c1 c2 -]: the value coefficients
+            // are two 16-byte loads
+            const double2 v01 = __ldg(reinterpret_cast<const double2 *>(row + (size_t)m * 8));
+            const double2 v23 = __ldg(reinterpret_cast<const double2 *>(row + (size_t)m * 8 + 2));
+            rho += ((v01.x * p + v01.y) * p + v23.x) * p + v23.y;
           }
         }
       }
@@ -222,9 +242,17 @@ __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__r
       const Shift3 sx = shifts(cx, a.box.ncell[0], a.box.prd[0]);
       const Shift3 sy = shifts(cy, a.box.ncell[1], a.box.prd[1]);
       const Shift3 sz = shifts(cz, a.box.ncell[2], a.box.prd[2]);
+      // one element: the density and pair spline rows of every pair
+      const double *rrow1 =
+          SINGLE ? a.rhor + (size_t)s_t2rhor[a.ntp1 + 1] * (a.nr + 1) * 8 : nullptr;
+      const double *zrow1 = SINGLE ? a.z2r + (size_t)s_t2z2r[a.ntp1 + 1] * (a.nr + 1) * 8 : nullptr;
       const int4 *nl4 = reinterpret_cast<const int4 *>(a.nlist);
-      for (int c4 = lane; 4 * c4 < num; c4 += TPA) {
-       const int4 e4 = nl4[(size_t)c4 * a.stride + i];
+      const int nslab = (num + 3) >> 2;
+      int4 en = make_int4(0, 0, 0, 0);
+      if (lane < nslab) en = __ldcs(&nl4[(size_t)lane * a.stride + i]);
+      for (int c4 = lane; c4 < nslab; c4 += TPA) {
+       const int4 e4 = en;
+       if (c4 + TPA < nslab) en = __ldcs(&nl4[(size_t)(c4 + TPA) * a.stride + i]);
        const int mm = min(4, num - 4 * c4);
        const unsigned int ee[4] = {(unsigned int)e4.x, (unsigned int)e4.y, (unsigned int)e4.z,
                                    (unsigned int)e4.w};
@@ -249,21 +277,28 @@ __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__r
         if (rsq < a.cutforcesq) {
           const int tj = (int)xj.w;
           const double r = sqrt(rsq);
-          double p = __dadd_rn(__dmul_rn(r, a.rdr), 1.0);
-          int m = (int)p;
-          m = min(m, a.nr - 1);
-          p -= m;
-          p = fmin(p, 1.0);
-          const double *ci = a.rhor + ((size_t)s_t2rhor[ti * a.ntp1 + tj] * (a.nr + 1) + m) * 8;
-          const double rhoip = (ci[0] * p + ci[1]) * p + ci[2];
+          int m;
+          double p;
+          knot_d(__dadd_rn(__dmul_rn(r, a.rdr), 1.0), a.nr - 1, m, p);
+          const size_t o8 = (size_t)m * 8;
+          // knot layout [c3 c4 c5 c6 | c0 c1 c2 -]
+          const double *ci =
+              (SINGLE ? rrow1 : a.rhor + (size_t)s_t2rhor[ti * a.ntp1 + tj] * (a.nr + 1) * 8) + o8;
+          const double2 d01 = __ldg(reinterpret_cast<const double2 *>(ci + 4));
+          const double rhoip = (d01.x * p + d01.y) * p + __ldg(ci + 6);
           double rhojp = rhoip;
-          if (!a.rhor_sym) {
+          if (!SINGLE && !a.rhor_sym) {
             const double *cj = a.rhor + ((size_t)s_t2rhor[tj * a.ntp1 + ti] * (a.nr + 1) + m) * 8;
-            rhojp = (cj[0] * p + cj[1]) * p + cj[2];
+            const double2 e01 = __ldg(reinterpret_cast<const double2 *>(cj + 4));
+            rhojp = (e01.x * p + e01.y) * p + __ldg(cj + 6);
           }
-          const double *cz2 = a.z2r + ((size_t)s_t2z2r[ti * a.ntp1 + tj] * (a.nr + 1) + m) * 8;
-          const double z2p = (cz2[0] * p + cz2[1]) * p + cz2[2];
-          const double z2 = ((cz2[3] * p + cz2[4]) * p + cz2[5]) * p + cz2[6];
+          const double *cz2 =
+              (SINGLE ? zrow1 : a.z2r + (size_t)s_t2z2r[ti * a.ntp1 + tj] * (a.nr + 1) * 8) + o8;
+          const double2 z01 = __ldg(reinterpret_cast<const double2 *>(cz2));
+          const double2 z23 = __ldg(reinterpret_cast<const double2 *>(cz2 + 2));
+          const double2 zd01 = __ldg(reinterpret_cast<const double2 *>(cz2 + 4));
+          const double z2p = (zd01.x * p + zd01.y) * p + __ldg(cz2 + 6);
+          const double z2 = ((z01.x * p + z01.y) * p + z23.x) * p + z23.y;
           const double recip = rcp_nr(r);
           const double phi = z2 * recip;
           const double phip = z2p * recip - phi * recip;
