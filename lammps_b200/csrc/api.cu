@@ -510,9 +510,10 @@ cudaError_t launch_piece(b200_ctx *c, int kind, double dtv, double dtf, cudaEven
       }
     }
     if (e == cudaSuccess && ev) e = record(c, ev[2]);
+    // the fused half-steps also record the thermo row and make the next
+    // step's rebuild decision (in their last block)
     if (e == cudaSuccess) e = fused ? md_nve_fused(c, dtv, dtf, out) : md_nve_final(c, dtf, out);
-    if (e == cudaSuccess && out) e = md_record_row(c);
-    if (e == cudaSuccess && fused) e = md_decide(c);
+    if (e == cudaSuccess && out && !fused) e = md_record_row(c);
     if (e == cudaSuccess && ev) e = record(c, ev[3]);
   }
   return e;

@@ -11,6 +11,54 @@
 
 namespace {
 
+// Neighbor::decide (src/neighbor.cpp:1294-1309) on the device: the host
+// mirrors the same schedule and reads ST_REBUILD only when the distance
+// criterion decides.
+__device__ __forceinline__ void decide_dev(int *status, int every, int delay, int check) {
+  const int ago = status[ST_AGO] + 1;
+  status[ST_AGO] = ago;
+  int rebuild = 0;
+  if (ago >= delay && ago % every == 0) {
+    if (!check) rebuild = 1;
+    else {
+      rebuild = status[ST_MOVED] != 0;
+      if (rebuild && ago == (every > delay ? every : delay)) status[ST_NDANGER] += 1;
+    }
+  }
+  if (status[ST_FORCE_BUILD]) {  // replay after a list overflow: lists are stale
+    rebuild = 1;
+    status[ST_FORCE_BUILD] = 0;
+  }
+  status[ST_MOVED] = 0;
+  status[ST_REBUILD] = rebuild;
+  unsigned int lo = (unsigned int)status[ST_STEP_LO] + 1u;
+  if (lo == 0u) status[ST_STEP_HI] += 1;
+  status[ST_STEP_LO] = (int)lo;
+}
+
+__device__ __forceinline__ void record_row_dev(int *status, const double *ev, double *rows,
+                                               int cap) {
+  const int r = status[ST_ROW];
+  if (r < cap) {
+    double *row = rows + 9 * (size_t)r;
+    const long long step = ((long long)(unsigned int)status[ST_STEP_HI] << 32) |
+                           (long long)(unsigned int)status[ST_STEP_LO];
+    row[0] = (double)step;
+    row[1] = ev[7];
+    row[2] = ev[0];
+    for (int k = 0; k < 6; k++) row[3 + k] = ev[1 + k];
+  }
+  status[ST_ROW] = r + 1;
+}
+
+__global__ void k_decide(int *status, int every, int delay, int check) {
+  decide_dev(status, every, delay, check);
+}
+
+__global__ void k_record_row(int *status, const double *ev, double *rows, int cap) {
+  record_row_dev(status, ev, rows, cap);
+}
+
 template <bool BATCH>
 __global__ void __launch_bounds__(256) k_nve_initial(int n, int stride, double dtv, double dtf,
                                                       const double *__restrict__ mass,
@@ -86,7 +134,10 @@ __global__ void __launch_bounds__(256) k_nve_final(int n, int stride, double dtf
 // FixNVE::final_integrate of this step, the kinetic-energy term of the
 // thermo output (KE), then FixNVE::initial_integrate of the next step: the
 // same rounded operations as k_nve_final followed by k_nve_initial, with v, f
-// and x read once.
+// and x read once.  The last block to finish then completes the step on the
+// device: the kinetic-energy sum (block partials added in block order), the
+// thermo row (KE), and the next step's rebuild decision (Neighbor::decide),
+// which sees every block's displacement flag.
 template <bool KE, bool BATCH>
 __global__ void __launch_bounds__(256) k_nve_fused(int n, int stride, double dtv, double dtf,
                                                     const double *__restrict__ mass,
@@ -98,8 +149,10 @@ __global__ void __launch_bounds__(256) k_nve_fused(int n, int stride, double dtv
                                                     Reps reps, const double4 *__restrict__ xhold,
                                                     double triggersq, int *__restrict__ status,
                                                     double *partial, unsigned int *counter,
-                                                    double *out) {
+                                                    double *ev, double *rows, int rows_cap,
+                                                    int every, int delay, int check) {
   __shared__ double red[8];
+  __shared__ bool last;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double acc[1] = {0.0};
   bool moved = false;
@@ -139,9 +192,32 @@ __global__ void __launch_bounds__(256) k_nve_fused(int n, int stride, double dtv
       moved = rsq > triggersq;
     }
   }
-  if (xhold && __any_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0)
+  if (xhold && __any_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0) {
     atomicExch(&status[ST_MOVED], 1);
-  if (KE) block_partials_finish<1>(acc, red, partial, counter, out, false);
+    __threadfence();  // the flag is visible before this block counts itself done
+  }
+  if (KE) block_sum<1>(acc, red);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (KE) partial[blockIdx.x] = acc[0];
+    __threadfence();
+    last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (KE) {
+    double s[1] = {0.0};
+    for (unsigned int b = threadIdx.x; b < gridDim.x; b += blockDim.x) s[0] += __ldcg(&partial[b]);
+    __syncthreads();
+    block_sum<1>(s, red);
+    if (threadIdx.x == 0) ev[7] = s[0];
+  }
+  if (threadIdx.x == 0) {
+    if (KE) record_row_dev(status, ev, rows, rows_cap);
+    decide_dev(status, every, delay, check);
+    *counter = 0u;
+  }
 }
 
 __global__ void __launch_bounds__(256) k_ke(int n, int stride, const double *__restrict__ mass,
@@ -157,45 +233,6 @@ __global__ void __launch_bounds__(256) k_ke(int n, int stride, const double *__r
     acc[0] = (vx * vx + vy * vy + vz * vz) * m;
   }
   block_partials_finish<1>(acc, red, partial, counter, out, false);
-}
-
-// Neighbor::decide (src/neighbor.cpp:1294-1309) on the device: the host
-// mirrors the same schedule and reads ST_REBUILD only when the distance
-// criterion decides.
-__global__ void k_decide(int *status, int every, int delay, int check) {
-  const int ago = status[ST_AGO] + 1;
-  status[ST_AGO] = ago;
-  int rebuild = 0;
-  if (ago >= delay && ago % every == 0) {
-    if (!check) rebuild = 1;
-    else {
-      rebuild = status[ST_MOVED] != 0;
-      if (rebuild && ago == (every > delay ? every : delay)) status[ST_NDANGER] += 1;
-    }
-  }
-  if (status[ST_FORCE_BUILD]) {  // replay after a list overflow: lists are stale
-    rebuild = 1;
-    status[ST_FORCE_BUILD] = 0;
-  }
-  status[ST_MOVED] = 0;
-  status[ST_REBUILD] = rebuild;
-  unsigned int lo = (unsigned int)status[ST_STEP_LO] + 1u;
-  if (lo == 0u) status[ST_STEP_HI] += 1;
-  status[ST_STEP_LO] = (int)lo;
-}
-
-__global__ void k_record_row(int *status, const double *ev, double *rows, int cap) {
-  const int r = status[ST_ROW];
-  if (r < cap) {
-    double *row = rows + 9 * (size_t)r;
-    const long long step = ((long long)(unsigned int)status[ST_STEP_HI] << 32) |
-                           (long long)(unsigned int)status[ST_STEP_LO];
-    row[0] = (double)step;
-    row[1] = ev[7];
-    row[2] = ev[0];
-    for (int k = 0; k < 6; k++) row[3 + k] = ev[1 + k];
-  }
-  status[ST_ROW] = r + 1;
 }
 
 }  // namespace
@@ -235,7 +272,8 @@ cudaError_t md_nve_fused(b200_ctx *c, double dtv, double dtf, bool ke) {
 #define MD_FUSED_ARGS                                                                           \
   c->n, c->stride, dtv, dtf, c->mass_dev, c->x4, c->v, c->f,                                  \
       c->prec == B200_PREC_MIXED ? c->xr : nullptr, c->cell, c->box, c->reps(),               \
-      c->check ? c->xhold : nullptr, triggersq, c->status, c->partial, c->counter, c->ev + 7
+      c->check ? c->xhold : nullptr, triggersq, c->status, c->partial, c->counter, c->ev,     \
+      c->rows, c->rows_cap, c->every, c->delay, c->check
   const int grid = md_blocks(c->n, B);
   if (ke && c->nrep) k_nve_fused<true, true><<<grid, B, 0, c->stream>>>(MD_FUSED_ARGS);
   else if (ke) k_nve_fused<true, false><<<grid, B, 0, c->stream>>>(MD_FUSED_ARGS);
