@@ -373,13 +373,26 @@ def dist_setup():
     return ws, rank, local
 
 
-def allmax(val, ws, torch):
+def _reduce(val, ws, torch, op):
     if ws == 1:
         return val
     import torch.distributed as dist
-    t = torch.tensor([val], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([val], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=op)
     return float(t.item())
+
+
+def allmax(val, ws, torch):
+    """The maximum of `val` over the ranks (device times: the slowest rank)."""
+    import torch.distributed as dist
+    return _reduce(val, ws, torch, dist.ReduceOp.MAX if ws > 1 else None)
+
+
+def allsum(val, ws, torch):
+    """The sum of `val` over the ranks (work done by all ranks)."""
+    import torch.distributed as dist
+    return _reduce(val, ws, torch, dist.ReduceOp.SUM if ws > 1 else None)
 
 
 def barrier(ws):
@@ -503,7 +516,8 @@ def main():
     barrier(ws)
     clk = clocks.stop()
     total_ms = allmax(sum(per), ws, torch)
-    value = ws * n * MD_STEPS * K / (total_ms * 1e3)
+    atoms_all = allsum(n, ws, torch)  # every rank advances its own box
+    value = atoms_all * MD_STEPS * K / (total_ms * 1e3)
 
     # ---- per-phase device timers over the same number of bench steps ------
     sysm.set_timing(True)
@@ -539,7 +553,7 @@ def main():
     e2e_run(sysm, x_pin, v_pin, t_pin, out_pin, 1)
     e_ms, h2d, d2h = e2e_run(sysm, x_pin, v_pin, t_pin, out_pin, K)
     e_ms = allmax(e_ms, ws, torch)
-    e2e = {"value": ws * n * MD_STEPS * K / (e_ms * 1e3), "unit": "Matom-steps/s",
+    e2e = {"value": atoms_all * MD_STEPS * K / (e_ms * 1e3), "unit": "Matom-steps/s",
            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
 
     extras = {}
@@ -602,16 +616,28 @@ def main():
         extras["eam_4M"] = em
 
     if not args.no_extras:
-        from lammps_b200.replicas import replica_batch
-        batch = replica_batch(nrep=256)
-        rep = {"replicas": 256, "atoms": int(batch["natoms"].sum()),
-               "natoms_min": int(batch["natoms"].min()), "natoms_max": int(batch["natoms"].max()),
-               "steps": 1000, "note": "256 fcc LJ boxes, 4n^3 atoms with n = 5..12 from log-uniform "
-                                      "500-8000, rho* U(0.70,0.95), T* U(0.8,2.0), rc 2.5 skin 0.3 "
-                                      "every 20; one set of launches per step for all replicas; "
-                                      "p50/p99 with phase events recorded in the step graphs"}
+        from lammps_b200.replicas import replica_batch, shard_batch
+        full = replica_batch(nrep=256)
+        # under torchrun the 256 replicas are sharded across the ranks (no
+        # exchange); throughput is all replicas over the slowest rank's time
+        batch = shard_batch(full, rank, ws) if ws > 1 else full
+        rep = {"replicas": 256, "atoms": int(full["natoms"].sum()),
+               "natoms_min": int(full["natoms"].min()), "natoms_max": int(full["natoms"].max()),
+               "ranks": ws, "steps": 1000,
+               "note": "256 fcc LJ boxes, 4n^3 atoms with n = 5..12 from log-uniform "
+                       "500-8000, rho* U(0.70,0.95), T* U(0.8,2.0), rc 2.5 skin 0.3 "
+                       "every 20; one set of launches per step for all replicas; "
+                       "p50/p99 with phase events recorded in the step graphs"}
         for prec in ("mixed", "fp64"):
-            rep[prec] = replica_bench(prec, batch, torch)
+            r = replica_bench(prec, batch, torch)
+            if ws > 1:
+                ms = allmax(r["ms_per_step"], ws, torch)
+                r["ms_per_step"] = ms
+                r["replica_steps_per_s"] = 256 / (ms * 1e-3)
+                r["matom_steps_per_s"] = float(full["natoms"].sum()) / (ms * 1e3)
+                r["step_ms_p50"] = allmax(r["step_ms_p50"], ws, torch)
+                r["step_ms_p99"] = allmax(r["step_ms_p99"], ws, torch)
+            rep[prec] = r
         rep["mixed_over_fp64"] = rep["mixed"]["replica_steps_per_s"] / rep["fp64"]["replica_steps_per_s"]
         extras["replicas_256"] = rep
         from lammps_b200.forcematch import force_matching_case, gradient_check

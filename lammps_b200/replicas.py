@@ -49,6 +49,36 @@ def replica_batch(nrep: int = 256, seed: int = 20140808, nmin: int = 500, nmax: 
                 seeds=seeds)
 
 
+def shard_batch(batch: dict, rank: int, world: int) -> dict:
+    """The replicas of `batch` that rank `rank` of `world` advances: a
+    contiguous block of replicas, the blocks cut where the running atom count
+    crosses k / world of the total, so every rank gets about the same number
+    of atoms.  Replicas are independent, so the shards need no exchange.
+    Returns a batch of the same form plus `replicas`, the replica indices."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError(f"rank {rank} of world {world}")
+    nat = np.asarray(batch["natoms"], dtype=np.int64)
+    cum = np.concatenate([[0], np.cumsum(nat)])
+    # replica r goes to the rank whose share contains the midpoint of its atoms
+    mid = (cum[:-1] + cum[1:]) / 2.0
+    owner = np.minimum((mid * world / cum[-1]).astype(int), world - 1)
+    idx = np.nonzero(owner == rank)[0]
+    out = {"replicas": idx}
+    if len(idx) == 0:
+        out.update(x=np.zeros((0, 3)), v=np.zeros((0, 3)), natoms=np.zeros(0, np.int32))
+        for k in ("lo", "hi"):
+            out[k] = np.zeros((0, 3))
+        return out
+    a0, a1 = int(cum[idx[0]]), int(cum[idx[-1] + 1])
+    out.update(x=batch["x"][a0:a1], v=batch["v"][a0:a1])
+    for k, val in batch.items():
+        if k in ("x", "v"):
+            continue
+        arr = np.asarray(val)
+        out[k] = arr[idx] if arr.ndim >= 1 and len(arr) == len(nat) else val
+    return out
+
+
 def make_batch(batch: dict, precision: str = "fp64", cut: float = 2.5, skin: float = 0.3,
                every: int = 20, device: int = 0, tpa: int = 0) -> System:
     """A System advancing every replica of `batch` (lj units, eps = sigma = 1,
