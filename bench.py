@@ -128,6 +128,70 @@ def make_lj(precision, x, v, hi):
 # ---------------------------------------------------------------------------
 # clocks during the timed region
 
+class NvmlClockSampler:
+    """SM clock and clock-event reasons sampled in-process through NVML every
+    `period` seconds while the timed region runs (the bench's timed region is
+    tens of milliseconds, too short for nvidia-smi's 200 ms loop).  Reads
+    only; changes no GPU setting."""
+
+    def __init__(self, device, period=0.005):
+        import pynvml
+        import torch
+        self.nv = pynvml
+        pynvml.nvmlInit()
+        pr = torch.cuda.get_device_properties(device)
+        bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+        try:
+            self.h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(device)
+        self.period = period
+        self.samples = []
+        self.stop_ev = threading.Event()
+        self.t = None
+
+    def _run(self):
+        nv = self.nv
+        while not self.stop_ev.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                self.samples.append((sm, rs))
+            except Exception:
+                pass
+            self.stop_ev.wait(self.period)
+
+    def start(self):
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
+
+    def stop(self):
+        self.stop_ev.set()
+        if self.t:
+            self.t.join(timeout=2)
+        nv = self.nv
+        try:
+            mx = float(nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM))
+        except Exception:
+            mx = None
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        reasons = sorted({k for _, r in self.samples for k, b in bits.items() if r & b})
+        sm = [float(c) for c, _ in self.samples]
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": reasons, "samples": len(sm), "source": "nvml"}
+
+
+def clock_sampler(device):
+    """NVML sampler when NVML loads, else the nvidia-smi loop."""
+    try:
+        return NvmlClockSampler(device)
+    except Exception:
+        return ClockSampler(device)
+
+
 class ClockSampler:
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -507,7 +571,7 @@ def main():
         device_time_run(sysm, torch, ext, flush, MD_STEPS, start)
     barrier(ws)
     torch.cuda.synchronize()
-    clocks = ClockSampler(dev)
+    clocks = clock_sampler(dev)
     clocks.start()
     launches0 = sysm.kernel_launches
     per = [device_time_run(sysm, torch, ext, flush, MD_STEPS, start) for _ in range(K)]
