@@ -16,10 +16,13 @@
 // Memory-level parallelism: each thread reads four list entries with one
 // 16-byte load (slab layout, md_slab).  The FP64 kernel issues a slab's four
 // neighbor gathers before using any of them and forms 1/rsq by Newton's
-// method from the hardware reciprocal (rcp_nr).  The mixed kernel works on
+// method from the hardware reciprocal (rcp_nr); for an atom away from the
+// box faces it skips the periodic-shift decode.  The mixed kernel works on
 // four slabs at a time with the next four already loading, evaluates every
 // entry branch-free with the one-instruction FP32 reciprocal, and adds the
 // FP32 force sum of each eight entries to the FP64 accumulator.
+#include <type_traits>
+
 #include "md_state.h"
 
 namespace {
@@ -77,6 +80,13 @@ __global__ void __launch_bounds__(128) k_lj_fp64(PairArgs a, const double4 *__re
     const Shift3 sz = shifts(cz, box.ncell[2], box.prd[2]);
     const int num = a.numneigh[i];
     const int4 *nl4 = reinterpret_cast<const int4 *>(a.nlist);
+    // An atom whose 27 neighbour cells all lie inside the box has no
+    // periodic image among its neighbours: x_j + 0.0 is x_j exactly, so the
+    // offset decode and the shift are skipped (same results bit for bit).
+    const bool interior = cx >= 1 && cx + 2 <= box.ncell[0] && cy >= 1 &&
+                          cy + 2 <= box.ncell[1] && cz >= 1 && cz + 2 <= box.ncell[2];
+    auto slabs = [&](auto wrap_tag) {
+    constexpr bool WRAP = decltype(wrap_tag)::value;
     for (int c4 = lane; 4 * c4 < num; c4 += TPA) {
       const int4 e4 = nl4[(size_t)c4 * a.stride + i];
       const int m = min(4, num - 4 * c4);
@@ -88,11 +98,18 @@ __global__ void __launch_bounds__(128) k_lj_fp64(PairArgs a, const double4 *__re
 #pragma unroll
       for (int u = 0; u < 4; u++) {
         if (u >= m) break;
-        int j, dx, dy, dz;
-        decode(ee[u], j, dx, dy, dz);
-        const double delx = __dsub_rn(xi.x, __dadd_rn(xj[u].x, pick(sx, dx)));
-        const double dely = __dsub_rn(xi.y, __dadd_rn(xj[u].y, pick(sy, dy)));
-        const double delz = __dsub_rn(xi.z, __dadd_rn(xj[u].z, pick(sz, dz)));
+        double delx, dely, delz;
+        if (WRAP) {
+          int j, dx, dy, dz;
+          decode(ee[u], j, dx, dy, dz);
+          delx = __dsub_rn(xi.x, __dadd_rn(xj[u].x, pick(sx, dx)));
+          dely = __dsub_rn(xi.y, __dadd_rn(xj[u].y, pick(sy, dy)));
+          delz = __dsub_rn(xi.z, __dadd_rn(xj[u].z, pick(sz, dz)));
+        } else {
+          delx = __dsub_rn(xi.x, xj[u].x);
+          dely = __dsub_rn(xi.y, xj[u].y);
+          delz = __dsub_rn(xi.z, xj[u].z);
+        }
         const double rsq = dsq3(delx, dely, delz);
         const int tt = ti * a.ntp1 + (int)xj[u].w;
         const double cs = SINGLE ? cutsq1 : tab[0 * nt2 + tt];
@@ -123,6 +140,9 @@ __global__ void __launch_bounds__(128) k_lj_fp64(PairArgs a, const double4 *__re
         }
       }
     }
+    };
+    if (interior) slabs(std::false_type{});
+    else slabs(std::true_type{});
   }
   fx = lane_sum<TPA>(fx);
   fy = lane_sum<TPA>(fy);
