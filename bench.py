@@ -653,6 +653,22 @@ def main():
         lj["mixed_over_fp64"] = lj["mixed"] / lj["fp64"]
         f_ms = lj["mixed_phases_ms_per_step"]["pair1"]
         lj["force_kernel_gbs"] = 48.0 * len(x4) / (f_ms * 1e-3) / 1e9
+        # NVE energy conservation over 1000 steps (thermo every 100), both
+        # forms from the same state: TotEng per atom, its least-squares slope
+        # per step, and the largest mixed - FP64 difference along the run
+        etot = {}
+        for prec in ("mixed", "fp64"):
+            s = make_lj(prec, x4, v4, hi4)
+            s.set_thermo(100)
+            r0 = s.setup()
+            rows = [r0] + s.run(1000)
+            st = np.array([r["Step"] for r in rows], dtype=float)
+            e = np.array([r["TotEng"] for r in rows])
+            etot[prec] = e
+            lj[prec + "_nve_1000"] = {"etot_first": float(e[0]), "etot_last": float(e[-1]),
+                                      "slope_per_step": float(np.polyfit(st, e, 1)[0])}
+            s.close()
+        lj["nve_1000_max_abs_etot_diff"] = float(np.max(np.abs(etot["mixed"] - etot["fp64"])))
         extras["lj_4M"] = lj
         # the EAM workload at 4M atoms: the density and force kernels at a
         # size where they are not launch- and latency-bound
