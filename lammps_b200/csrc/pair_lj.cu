@@ -85,10 +85,15 @@ __global__ void __launch_bounds__(128) k_lj_fp64(PairArgs a, const double4 *__re
     // offset decode and the shift are skipped (same results bit for bit).
     const bool interior = cx >= 1 && cx + 2 <= box.ncell[0] && cy >= 1 &&
                           cy + 2 <= box.ncell[1] && cz >= 1 && cz + 2 <= box.ncell[2];
+    const int nslab = (num + 3) >> 2;
     auto slabs = [&](auto wrap_tag) {
     constexpr bool WRAP = decltype(wrap_tag)::value;
-    for (int c4 = lane; 4 * c4 < num; c4 += TPA) {
-      const int4 e4 = nl4[(size_t)c4 * a.stride + i];
+    // the next slab's entries load (streaming) while this slab is used
+    int4 en = make_int4(0, 0, 0, 0);
+    if (lane < nslab) en = __ldcs(&nl4[(size_t)lane * a.stride + i]);
+    for (int c4 = lane; c4 < nslab; c4 += TPA) {
+      const int4 e4 = en;
+      if (c4 + TPA < nslab) en = __ldcs(&nl4[(size_t)(c4 + TPA) * a.stride + i]);
       const int m = min(4, num - 4 * c4);
       const unsigned int ee[4] = {(unsigned int)e4.x, (unsigned int)e4.y, (unsigned int)e4.z,
                                   (unsigned int)e4.w};
