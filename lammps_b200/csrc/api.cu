@@ -8,6 +8,9 @@
 #include <new>
 #include <vector>
 
+#include <atomic>
+#include <chrono>
+
 #include "md_state.h"
 
 namespace {
@@ -555,6 +558,35 @@ int capture_piece(b200_ctx *c, int kind, double dtv, double dtf) {
   return B200_OK;
 }
 
+// The rebuild decision of the last piece launched: wait until the device's
+// decision count in the mailbox reaches the host's, then read the flag.  If
+// that takes longer than 0.2 s, read the status word after a stream
+// synchronize instead (which also reports a CUDA error) and take the
+// device's count as the host's.
+int wait_decision(b200_ctx *c, bool *rebuild) {
+  volatile int *m = c->mail_host;
+  const int want = (int)c->decisions;
+  const auto t0 = std::chrono::steady_clock::now();
+  for (unsigned it = 1;; it++) {
+    if (m[1] == want) {
+      std::atomic_thread_fence(std::memory_order_acquire);
+      *rebuild = m[0] != 0;
+      return B200_OK;
+    }
+    if ((it & 4095u) == 0u &&
+        std::chrono::steady_clock::now() - t0 > std::chrono::milliseconds(200))
+      break;
+  }
+  CK(cudaMemcpyAsync(&c->status_host[ST_REBUILD], c->status + ST_REBUILD, sizeof(int),
+                     cudaMemcpyDeviceToHost, c->stream));
+  int dc = 0;
+  CK(cudaMemcpyAsync(&dc, c->dec_count, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->decisions = (unsigned int)dc;
+  *rebuild = c->status_host[ST_REBUILD] != 0;
+  return B200_OK;
+}
+
 // run one piece: graph replay, or the kernels themselves with graphs off
 int run_piece(b200_ctx *c, int kind, double dtv, double dtf, cudaEvent_t *ev) {
   if (!c->use_graphs) {
@@ -676,6 +708,13 @@ int b200_create(int device, int precision, b200_ctx **out) {
   if (e == cudaSuccess) e = cudaMalloc((void **)&c->status, ST_COUNT * sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(c->status, 0, ST_COUNT * sizeof(int));
   if (e == cudaSuccess) e = cudaMallocHost((void **)&c->status_host, ST_COUNT * sizeof(int));
+  if (e == cudaSuccess) e = cudaHostAlloc((void **)&c->mail_host, 4 * sizeof(int), cudaHostAllocMapped);
+  if (e == cudaSuccess) {
+    c->mail_host[0] = c->mail_host[1] = 0;
+    e = cudaHostGetDevicePointer((void **)&c->mail_dev, c->mail_host, 0);
+  }
+  if (e == cudaSuccess) e = cudaMalloc((void **)&c->dec_count, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(c->dec_count, 0, sizeof(int));
   if (e == cudaSuccess) e = cudaMalloc((void **)&c->ev, 8 * sizeof(double));
   if (e == cudaSuccess) e = cudaMemset(c->ev, 0, 8 * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc((void **)&c->counter, sizeof(unsigned int));
@@ -703,7 +742,7 @@ int b200_destroy(b200_ctx *c) {
   dfree(c->nlist); dfree(c->numneigh); dfree(c->partial); dfree(c->counter); dfree(c->ev);
   dfree(c->adj_gs); dfree(c->adj_gtab);
   dfree(c->d_rep_box); dfree(c->d_rep_of_atom); dfree(c->d_rep_cell_base); dfree(c->d_tile_rep);
-  dfree(c->d_rep_tile_base); dfree(c->rep_eatom); dfree(c->rep_vatom); dfree(c->rep_rows);
+  dfree(c->d_rep_tile_base); 
   dfree(c->status); dfree(c->rows); dfree(c->tables_dev);
   dfree(c->snap_x4); dfree(c->snap_xhold); dfree(c->snap_v); dfree(c->snap_f);
   dfree(c->snap_orig); dfree(c->snap_image); dfree(c->snap_cell); dfree(c->snap_xr);
@@ -714,6 +753,8 @@ int b200_destroy(b200_ctx *c) {
     if (ev) cudaEventDestroy(ev);
   for (auto ev : c->ev_pool) cudaEventDestroy(ev);
   if (c->status_host) cudaFreeHost(c->status_host);
+  if (c->mail_host) cudaFreeHost(c->mail_host);
+  dfree(c->dec_count);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return B200_OK;
@@ -1152,11 +1193,11 @@ int b200_run(b200_ctx *c, int nsteps, double dt, double ftm2v, int thermo_every,
         if (!c->check) {
           rebuild = true;
         } else {
-          // distance criterion: the decision the device just made
-          CK(cudaMemcpyAsync(&c->status_host[ST_REBUILD], c->status + ST_REBUILD, sizeof(int),
-                             cudaMemcpyDeviceToHost, c->stream));
-          CK(cudaStreamSynchronize(c->stream));
-          rebuild = c->status_host[ST_REBUILD] != 0;
+          // distance criterion: the decision the device just made (it
+          // posts to the mailbox exactly on these steps)
+          c->decisions++;
+          rc = wait_decision(c, &rebuild);
+          if (rc) return rc;
         }
       }
       if (rebuild) {
@@ -1269,14 +1310,17 @@ int b200_neigh_stats(b200_ctx *c, long long *full_total, int *ncalls, int *ndang
   if (!c) return B200_ERR_ARG;
   if (!c->sorted_once) return set_err(c, B200_ERR_STATE, "neighbor list not built");
   CK(cudaSetDevice(c->device));
-  unsigned long long *d = nullptr, h = 0;
-  CK(cudaMallocAsync((void **)&d, sizeof(unsigned long long), c->stream));
+  unsigned long long h = 0;
+  char *st[1];
+  const size_t sb[1] = {sizeof(unsigned long long)};
+  int rc = xfer_parts(c, 1, sb, st);
+  if (rc) return rc;
+  unsigned long long *d = reinterpret_cast<unsigned long long *>(st[0]);
   CK(cudaMemsetAsync(d, 0, sizeof(unsigned long long), c->stream));
   k_full_total<<<md_blocks(c->n, 256), 256, 0, c->stream>>>(c->n, c->numneigh, d);
   c->launches++;
   CK(cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaFreeAsync(d, c->stream));
-  int rc = read_status(c);
+  rc = read_status(c);
   if (rc) return rc;
   if (full_total) *full_total = (long long)h;
   if (ncalls) *ncalls = c->status_host[ST_NCALLS];
@@ -1292,8 +1336,11 @@ int b200_get_rho_fp(b200_ctx *c, double *rho, double *fp) {
   if (!c->sorted_once) return set_err(c, B200_ERR_STATE, "neighbor list not built");
   CK(cudaSetDevice(c->device));
   const int n = c->n;
-  double *d = nullptr;
-  CK(cudaMallocAsync((void **)&d, (size_t)n * sizeof(double), c->stream));
+  char *st[1];
+  const size_t sb[1] = {(size_t)n * sizeof(double)};
+  int rc = xfer_parts(c, 1, sb, st);
+  if (rc) return rc;
+  double *d = reinterpret_cast<double *>(st[0]);
   if (rho) {
     k_unsort_scalar<<<md_blocks(n, 256), 256, 0, c->stream>>>(n, c->orig, c->rho, d);
     CK(cudaMemcpyAsync(rho, d, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -1303,7 +1350,6 @@ int b200_get_rho_fp(b200_ctx *c, double *rho, double *fp) {
     CK(cudaMemcpyAsync(fp, d, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   }
   c->launches += 2;
-  CK(cudaFreeAsync(d, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return B200_OK;
 }
@@ -1483,21 +1529,24 @@ int b200_replica_thermo(b200_ctx *c, double *rows) {
   if (!c->sorted_once) return set_err(c, B200_ERR_STATE, "neighbor list not built");
   CK(cudaSetDevice(c->device));
   const int n = c->n, R = c->nrep;
-  CK(cudaMallocAsync((void **)&c->rep_eatom, (size_t)n * sizeof(double), c->stream));
-  CK(cudaMallocAsync((void **)&c->rep_vatom, 6 * (size_t)n * sizeof(double), c->stream));
-  CK(cudaMallocAsync((void **)&c->rep_rows, 9 * (size_t)R * sizeof(double), c->stream));
-  int rc = pair_compute_dev(c, true, true, c->rep_eatom, c->rep_vatom);
+  char *st[4];
+  const size_t sb[4] = {(size_t)n * sizeof(double), 6 * (size_t)n * sizeof(double),
+                        9 * (size_t)R * sizeof(double), ((size_t)R + 1) * sizeof(int)};
+  int rc = xfer_parts(c, 4, sb, st);
+  if (rc) return rc;
+  double *eatom = reinterpret_cast<double *>(st[0]), *vatom = reinterpret_cast<double *>(st[1]);
+  double *drows = reinterpret_cast<double *>(st[2]);
+  int *d_start = reinterpret_cast<int *>(st[3]);
+  CK(cudaMemcpyAsync(d_start, c->rep_atom_start.data(), ((size_t)R + 1) * sizeof(int),
+                     cudaMemcpyHostToDevice, c->stream));
+  rc = pair_compute_dev(c, true, true, eatom, vatom);
   if (!rc) {
-    cudaError_t e = md_rep_rows(c, c->rep_eatom, c->rep_vatom, c->rep_rows);
+    cudaError_t e = md_rep_rows(c, d_start, eatom, vatom, drows);
     if (e != cudaSuccess) rc = set_err(c, B200_ERR_CUDA, "replica rows: %s", cudaGetErrorString(e));
   }
   if (!rc)
-    CK(cudaMemcpyAsync(rows, c->rep_rows, 9 * (size_t)R * sizeof(double), cudaMemcpyDeviceToHost,
+    CK(cudaMemcpyAsync(rows, drows, 9 * (size_t)R * sizeof(double), cudaMemcpyDeviceToHost,
                        c->stream));
-  CK(cudaFreeAsync(c->rep_eatom, c->stream));
-  CK(cudaFreeAsync(c->rep_vatom, c->stream));
-  CK(cudaFreeAsync(c->rep_rows, c->stream));
-  c->rep_eatom = c->rep_vatom = c->rep_rows = nullptr;
   CK(cudaStreamSynchronize(c->stream));
   return rc;
 }

@@ -14,19 +14,23 @@ namespace {
 // Neighbor::decide (src/neighbor.cpp:1294-1309) on the device: the host
 // mirrors the same schedule and reads ST_REBUILD only when the distance
 // criterion decides.
-__device__ __forceinline__ void decide_dev(int *status, int every, int delay, int check) {
+__device__ __forceinline__ void decide_dev(int *status, int every, int delay, int check,
+                                           int *dcount, volatile int *mail) {
   const int ago = status[ST_AGO] + 1;
   status[ST_AGO] = ago;
   int rebuild = 0;
-  if (ago >= delay && ago % every == 0) {
+  const bool candidate = ago >= delay && ago % every == 0;
+  if (candidate) {
     if (!check) rebuild = 1;
     else {
       rebuild = status[ST_MOVED] != 0;
       if (rebuild && ago == (every > delay ? every : delay)) status[ST_NDANGER] += 1;
     }
   }
+  bool forced = false;
   if (status[ST_FORCE_BUILD]) {  // replay after a list overflow: lists are stale
     rebuild = 1;
+    forced = true;
     status[ST_FORCE_BUILD] = 0;
   }
   status[ST_MOVED] = 0;
@@ -34,6 +38,15 @@ __device__ __forceinline__ void decide_dev(int *status, int every, int delay, in
   unsigned int lo = (unsigned int)status[ST_STEP_LO] + 1u;
   if (lo == 0u) status[ST_STEP_HI] += 1;
   status[ST_STEP_LO] = (int)lo;
+  if (check && candidate && !forced) {
+    // a decision the host waits for (the distance criterion): the flag
+    // first, then, after a system-wide fence, the new decision count
+    const int k = *dcount + 1;
+    *dcount = k;
+    mail[0] = rebuild;
+    __threadfence_system();
+    mail[1] = k;
+  }
 }
 
 __device__ __forceinline__ void record_row_dev(int *status, const double *ev, double *rows,
@@ -51,8 +64,8 @@ __device__ __forceinline__ void record_row_dev(int *status, const double *ev, do
   status[ST_ROW] = r + 1;
 }
 
-__global__ void k_decide(int *status, int every, int delay, int check) {
-  decide_dev(status, every, delay, check);
+__global__ void k_decide(int *status, int every, int delay, int check, int *dcount, int *mail) {
+  decide_dev(status, every, delay, check, dcount, mail);
 }
 
 __global__ void k_record_row(int *status, const double *ev, double *rows, int cap) {
@@ -150,7 +163,8 @@ __global__ void __launch_bounds__(256) k_nve_fused(int n, int stride, double dtv
                                                     double triggersq, int *__restrict__ status,
                                                     double *partial, unsigned int *counter,
                                                     double *ev, double *rows, int rows_cap,
-                                                    int every, int delay, int check) {
+                                                    int every, int delay, int check, int *dcount,
+                                                    int *mail) {
   __shared__ double red[8];
   __shared__ bool last;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -215,7 +229,7 @@ __global__ void __launch_bounds__(256) k_nve_fused(int n, int stride, double dtv
   }
   if (threadIdx.x == 0) {
     if (KE) record_row_dev(status, ev, rows, rows_cap);
-    decide_dev(status, every, delay, check);
+    decide_dev(status, every, delay, check, dcount, mail);
     *counter = 0u;
   }
 }
@@ -273,7 +287,7 @@ cudaError_t md_nve_fused(b200_ctx *c, double dtv, double dtf, bool ke) {
   c->n, c->stride, dtv, dtf, c->mass_dev, c->x4, c->v, c->f,                                  \
       c->prec == B200_PREC_MIXED ? c->xr : nullptr, c->cell, c->box, c->reps(),               \
       c->check ? c->xhold : nullptr, triggersq, c->status, c->partial, c->counter, c->ev,     \
-      c->rows, c->rows_cap, c->every, c->delay, c->check
+      c->rows, c->rows_cap, c->every, c->delay, c->check, c->dec_count, c->mail_dev
   const int grid = md_blocks(c->n, B);
   if (ke && c->nrep) k_nve_fused<true, true><<<grid, B, 0, c->stream>>>(MD_FUSED_ARGS);
   else if (ke) k_nve_fused<true, false><<<grid, B, 0, c->stream>>>(MD_FUSED_ARGS);
@@ -293,7 +307,8 @@ cudaError_t md_ke(b200_ctx *c) {
 }
 
 cudaError_t md_decide(b200_ctx *c) {
-  k_decide<<<1, 1, 0, c->stream>>>(c->status, c->every, c->delay, c->check);
+  k_decide<<<1, 1, 0, c->stream>>>(c->status, c->every, c->delay, c->check, c->dec_count,
+                                   c->mail_dev);
   c->launches++;
   return cudaGetLastError();
 }

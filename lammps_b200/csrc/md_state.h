@@ -68,7 +68,6 @@ struct b200_ctx {
   int *d_rep_of_atom = nullptr, *d_rep_cell_base = nullptr, *d_tile_rep = nullptr,
       *d_rep_tile_base = nullptr;
   int rep_dev_n = 0, rep_dev_tiles = 0, rep_dev_r = 0;
-  double *rep_eatom = nullptr, *rep_vatom = nullptr, *rep_rows = nullptr;
   Reps reps() const { return Reps{d_rep_box, d_rep_of_atom, d_rep_cell_base, d_tile_rep,
                                   d_rep_tile_base}; }
 
@@ -137,6 +136,16 @@ struct b200_ctx {
   double *ev = nullptr;          // [0] eng, [1..6] virial, [7] sum m v^2
   int *status = nullptr;         // ST_* words
   int *status_host = nullptr;    // pinned mirror
+  // decision mailbox: mapped page-locked words that the device's rebuild
+  // decision writes on the steps where the distance criterion decides ([0]
+  // the decision, [1] the number of such decisions so far), so the host
+  // reads a decision by waiting on memory instead of a copy and a stream
+  // synchronize; dec_count is the device's count (kept apart from the status
+  // words, which run-chunk snapshots restore) and decisions the host's count
+  // of the decisions it has waited for
+  int *mail_host = nullptr, *mail_dev = nullptr;
+  int *dec_count = nullptr;
+  unsigned int decisions = 0;
   double *rows = nullptr;        // device thermo rows (9 doubles each)
   int rows_cap = 0;
 
@@ -204,7 +213,8 @@ cudaError_t md_adj_positions(b200_ctx *c, const double *x);
 // ---- replicas (replica.cu) ------------------------------------------------------
 // per-replica thermo rows {natoms, sum m v^2, eng_vdwl, virial[6]} from the
 // per-atom energy/virial of the last compute (eatom, vatom in caller order)
-cudaError_t md_rep_rows(b200_ctx *c, const double *eatom, const double *vatom, double *rows);
+cudaError_t md_rep_rows(b200_ctx *c, const int *d_start, const double *eatom, const double *vatom,
+                        double *rows);
 
 inline int md_blocks(long long work, int block) {
   return (int)((work + block - 1) / block);

@@ -44,19 +44,11 @@ __global__ void __launch_bounds__(kRepThreads)
 
 }  // namespace
 
-cudaError_t md_rep_rows(b200_ctx *c, const double *eatom, const double *vatom, double *rows) {
-  int *d_start = nullptr;
-  cudaError_t e = cudaMallocAsync((void **)&d_start, (c->nrep + 1) * sizeof(int), c->stream);
-  if (e != cudaSuccess) return e;
-  e = cudaMemcpyAsync(d_start, c->rep_atom_start.data(), (c->nrep + 1) * sizeof(int),
-                      cudaMemcpyHostToDevice, c->stream);
-  if (e == cudaSuccess) {
-    k_rep_rows<<<c->nrep, kRepThreads, 0, c->stream>>>(d_start, c->stride, c->mass_dev, c->x4,
-                                                       c->v, eatom, vatom, rows);
-    c->launches++;
-    e = cudaGetLastError();
-  }
-  cudaError_t e2 = cudaStreamSynchronize(c->stream);
-  cudaFreeAsync(d_start, c->stream);
-  return e != cudaSuccess ? e : e2;
+cudaError_t md_rep_rows(b200_ctx *c, const int *d_start, const double *eatom, const double *vatom,
+                        double *rows) {
+  // d_start: device copy of the replica atom ranges (nrep + 1 ints)
+  k_rep_rows<<<c->nrep, kRepThreads, 0, c->stream>>>(d_start, c->stride, c->mass_dev, c->x4, c->v,
+                                                     eatom, vatom, rows);
+  c->launches++;
+  return cudaGetLastError();
 }
