@@ -329,6 +329,8 @@ int alloc_cells(b200_ctx *c) {
     invalidate_graphs(c);
     int m = c->ncells + 1;
     CK(dalloc(&c->cell_count, (size_t)m));
+    // zero once here: each build's scatter zeroes the counts for the next
+    CK(cudaMemsetAsync(c->cell_count, 0, (size_t)m * sizeof(int), c->stream));
     CK(dalloc(&c->cell_start, (size_t)m));
     CK(dalloc(&c->scan_tmp, (size_t)4096 + 1));
     c->ncell_alloc = m;

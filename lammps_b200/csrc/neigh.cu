@@ -7,10 +7,10 @@
 // and Neighbor::build -> half_bin_newton (src/neigh_half_bin.cpp:285-419):
 //   1 k_wrap_bin    wrap into the box (image flags), count atoms per cell
 //   2 k_scan_*      exclusive scan of the counts -> cell_start
-//   3 k_scatter     counting-sort scatter of atom indices
+//   3 k_scatter     counting-sort scatter of atom indices; zeroes the counts
 //   4 k_sort_cells  order each cell by caller index (deterministic order)
 //   5 k_gather      permute x, v, ids; cell-relative FP32 copy; xhold
-//   6 k_copyback    permuted arrays back into the primary buffers
+//   6 k_copyback    permuted arrays back into the primary buffers; ago = 0
 //   7 k_neigh_tiles full list over the 27 neighbor cells (cell >= rc+skin),
 //                   neighbor-cell tiles staged in shared memory
 // The pair test is the reference's, bit for bit: the periodic image is
@@ -135,11 +135,15 @@ __global__ void k_scan_add(int m, int *__restrict__ out, const int *__restrict__
   }
 }
 
+// Scatter each atom to its slot in the cell-sorted order.  The scan has
+// consumed the m cell counts by now, so this kernel also zeroes them for the
+// next build (the counts start at zero when they are allocated).
 __global__ void k_scatter(int n, const int *__restrict__ cell_tmp, const int *__restrict__ slot,
-                          const int *__restrict__ cell_start, int *__restrict__ perm,
-                          const int *flag) {
+                          const int *__restrict__ cell_start, int *__restrict__ perm, int m,
+                          int *__restrict__ cell_count, const int *flag) {
   if (!rebuild_on(flag)) return;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  for (int k = i; k < m; k += gridDim.x * blockDim.x) cell_count[k] = 0;
   if (i >= n) return;
   perm[cell_start[cell_tmp[i]] + slot[i]] = i;
 }
@@ -224,9 +228,14 @@ __global__ void k_copyback(int n, int stride, const double4 *__restrict__ x4b,
                            double4 *__restrict__ x4, const double *__restrict__ vb,
                            double *__restrict__ v, const int *__restrict__ origb,
                            int *__restrict__ orig, const int *__restrict__ imageb,
-                           int *__restrict__ image, const int *flag) {
+                           int *__restrict__ image, int *__restrict__ status, const int *flag) {
   if (!rebuild_on(flag)) return;
   int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k == 0) {
+    // Neighbor::build bookkeeping: ago = 0, ncalls++ (src/neighbor.cpp:1384-1386)
+    status[ST_AGO] = 0;
+    status[ST_NCALLS] += 1;
+  }
   if (k >= n) return;
   x4[k] = x4b[k];
   v[k] = vb[k];
@@ -505,13 +514,6 @@ __global__ void __launch_bounds__(kNeighThreads, 8) k_neigh_tiles(
   }
 }
 
-__global__ void k_build_done(int *status, int check, const int *flag) {
-  if (!rebuild_on(flag)) return;
-  // Neighbor::build bookkeeping: ago = 0, ncalls++ (src/neighbor.cpp:1384-1386)
-  status[ST_AGO] = 0;
-  status[ST_NCALLS] += 1;
-}
-
 // ---------------------------------------------------------------------------
 // Export of Neighbor::half_bin_newton's half list from the full list.
 struct HalfBins {
@@ -658,16 +660,9 @@ static cudaError_t launch_scan(b200_ctx *c, int m, const int *in, int *out, cons
   return cudaGetLastError();
 }
 
-__global__ void k_zero_counts(int m, int *cnt, const int *flag) {
-  if (flag && !*flag) return;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < m) cnt[i] = 0;
-}
-
 cudaError_t md_rebuild(b200_ctx *c, const int *d_flag) {
   const int n = c->n, B = 256;
   const int m = c->ncells + 1;
-  k_zero_counts<<<md_blocks(m, B), B, 0, c->stream>>>(m, c->cell_count, d_flag);
   const Reps R = c->reps();
   if (c->nrep)
     k_wrap_bin<true><<<md_blocks(n, B), B, 0, c->stream>>>(n, c->box, R, c->x4, c->image,
@@ -677,11 +672,11 @@ cudaError_t md_rebuild(b200_ctx *c, const int *d_flag) {
     k_wrap_bin<false><<<md_blocks(n, B), B, 0, c->stream>>>(n, c->box, R, c->x4, c->image,
                                                             c->cell_count, c->slot, c->cell_tmp,
                                                             c->status, d_flag);
-  c->launches += 2;
+  c->launches += 1;
   cudaError_t e = launch_scan(c, m, c->cell_count, c->cell_start, d_flag);
   if (e != cudaSuccess) return e;
   k_scatter<<<md_blocks(n, B), B, 0, c->stream>>>(n, c->cell_tmp, c->slot, c->cell_start, c->perm,
-                                                  d_flag);
+                                                  m, c->cell_count, d_flag);
   k_sort_cells<<<md_blocks(c->ncells, kSortWarps), kSortWarps * 32, 0, c->stream>>>(
       c->ncells, c->cell_start, c->perm, c->slot, c->orig, d_flag);
   if (c->nrep)
@@ -695,7 +690,8 @@ cudaError_t md_rebuild(b200_ctx *c, const int *d_flag) {
         c->imageb, c->cell_tmp, c->cell, c->prec == 1 ? c->xr : nullptr,
         c->check ? c->xhold : nullptr, d_flag);
   k_copyback<<<md_blocks(n, B), B, 0, c->stream>>>(n, c->stride, c->x4b, c->x4, c->vb, c->v,
-                                                   c->origb, c->orig, c->imageb, c->image, d_flag);
+                                                   c->origb, c->orig, c->imageb, c->image,
+                                                   c->status, d_flag);
   {
     const int tiles = c->nrep ? c->ntiles
                               : ((c->box.ncell[0] + kTileCells - 1) / kTileCells) *
@@ -715,8 +711,7 @@ cudaError_t md_rebuild(b200_ctx *c, const int *d_flag) {
       k_neigh_tiles<false, true><<<tiles, kNeighThreads, smem, c->stream>>>(MD_NEIGH_ARGS);
 #undef MD_NEIGH_ARGS
   }
-  k_build_done<<<1, 1, 0, c->stream>>>(c->status, c->check, d_flag);
-  c->launches += 5;
+  c->launches += 4;
   return cudaGetLastError();
 }
 
