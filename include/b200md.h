@@ -197,6 +197,39 @@ long long b200_kernel_launches(const b200_ctx *ctx);
 /* CUDA stream of the context, as a void* (cudaStream_t). */
 void *b200_stream(const b200_ctx *ctx);
 
+/* ---- spatial decomposition (one brick of a box per rank) ------------------- */
+
+/* A rank's context holds the whole periodic box with its own atoms and, as
+   ghosts, the atoms of other ranks within the ghost depth of its brick, at
+   their own (unshifted) coordinates; the builder forms periodic images as for
+   a single box.  These calls carry the per-rank parts of CommBrick and
+   Neighbor::decide; the exchange between ranks is the caller's (NCCL or any
+   transport).
+
+   Mark the ghosts of the current atoms: ghost[i] != 0 for caller index i
+   (upload order), n ints on the host; NULL clears.  Ghosts are not
+   integrated by b200_nve_initial / b200_nve_final, are left out of the
+   distance check and of the kinetic energy, and get their positions from
+   b200_halo_unpack.  Cleared by every b200_upload_atoms.  b200_run refuses a
+   context with ghosts (it decides rebuilds alone; a decomposed box decides
+   them across ranks).  The borders step, CommBrick::borders
+   (src/comm_brick.cpp:696-864), is the caller's choice of ghosts. */
+int b200_set_ghosts(b200_ctx *ctx, const int *ghost);
+/* The local half of Neighbor::check_distance (src/neighbor.cpp:1322-1372):
+   *moved = 1 if some owned atom moved more than half the skin since the last
+   build, as tested by the b200_nve_initial calls since the last check (the
+   flag is cleared).  The caller reduces it over ranks (MPI_Allreduce MAX,
+   src/neighbor.cpp:1369).  Needs check yes (b200_set_neighbor). */
+int b200_neigh_check(b200_ctx *ctx, int *moved);
+/* CommBrick::forward_comm with AtomVecAtomic::pack_comm / unpack_comm
+   (src/comm_brick.cpp:444-511, src/atom_vec_atomic.cpp:105-217), local
+   halves.  idx[m] are caller indices and buf[3m] the coordinates, both
+   DEVICE pointers on the context's device; the calls are ordered on the
+   context's stream and return after it completes.  pack: buf[3i..3i+2] = x
+   of atom idx[i].  unpack: x of atom idx[i] = buf[3i..3i+2]. */
+int b200_halo_pack(b200_ctx *ctx, int m, const int *idx, double *buf);
+int b200_halo_unpack(b200_ctx *ctx, int m, const int *idx, const double *buf);
+
 /* ---- batched replicas ---------------------------------------------------- */
 
 /* No counterpart in the reference (which runs one box per process): make the

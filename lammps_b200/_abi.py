@@ -56,6 +56,10 @@ SIGNATURES = {
     "b200_get_timing": (C.c_int, [_vp, _dp, C.POINTER(C.c_longlong), C.c_int]),
     "b200_stream": (_vp, [_vp]),
     "b200_get_step_times": (C.c_int, [_vp, _dp, C.c_int, _ip, C.c_int]),
+    "b200_set_ghosts": (C.c_int, [_vp, _ip]),
+    "b200_neigh_check": (C.c_int, [_vp, _ip]),
+    "b200_halo_pack": (C.c_int, [_vp, C.c_int, C.c_void_p, C.c_void_p]),
+    "b200_halo_unpack": (C.c_int, [_vp, C.c_int, C.c_void_p, C.c_void_p]),
     "b200_set_replicas": (C.c_int, [_vp, C.c_int, _ip, _dp, _dp]),
     "b200_replica_count": (C.c_int, [_vp]),
     "b200_replica_thermo": (C.c_int, [_vp, _dp]),

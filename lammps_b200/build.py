@@ -7,7 +7,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libb200md.so")
-SOURCES = ["api.cu", "neigh.cu", "pair_lj.cu", "pair_eam.cu", "integrate.cu", "noalloc.cu", "adjoint.cu", "replica.cu"]
+SOURCES = ["api.cu", "neigh.cu", "pair_lj.cu", "pair_eam.cu", "integrate.cu", "noalloc.cu", "adjoint.cu", "replica.cu", "halo.cu"]
 HEADERS = ["md_common.cuh", "md_state.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]

@@ -673,6 +673,7 @@ int snapshot(b200_ctx *c, bool save) {
   if (c->check) CK(cp(c->xhold, c->snap_xhold, n * sizeof(double4)));
   if (c->prec == B200_PREC_MIXED) CK(cp(c->xr, c->snap_xr, n * sizeof(float4)));
   CK(cp(c->status, c->snap_status, ST_COUNT * sizeof(int)));
+  if (!save) CK(md_where(c));
   return B200_OK;
 }
 
@@ -738,6 +739,7 @@ int b200_destroy(b200_ctx *c) {
   invalidate_graphs(c);
   dfree(c->x4); dfree(c->x4b); dfree(c->v); dfree(c->vb); dfree(c->f);
   dfree(c->orig); dfree(c->origb); dfree(c->image); dfree(c->imageb); dfree(c->cell);
+  dfree(c->where); dfree(c->ghost);
   dfree(c->xr); dfree(c->xhold); dfree(c->xfer); dfree(c->rho); dfree(c->fp); dfree(c->fpf); dfree(c->mass_dev);
   dfree(c->cell_count); dfree(c->cell_start); dfree(c->scan_tmp);
   dfree(c->slot); dfree(c->perm); dfree(c->cell_tmp);
@@ -948,6 +950,8 @@ int b200_upload_atoms(b200_ctx *c, int n, const double *x, const double *v, cons
     CK(dalloc(&c->image, stride));
     CK(dalloc(&c->imageb, stride));
     CK(dalloc(&c->cell, stride));
+    CK(dalloc(&c->where, stride));
+    CK(dalloc(&c->ghost, stride));
     CK(dalloc(&c->xr, stride));
     CK(dalloc(&c->xhold, stride));
     CK(dalloc(&c->rho, stride));
@@ -982,6 +986,8 @@ int b200_upload_atoms(b200_ctx *c, int n, const double *x, const double *v, cons
                                                      c->orig, c->image, c->cell);
   c->launches++;
   CK(cudaGetLastError());
+  CK(md_where(c));
+  c->ghosts_on = false;  // a new atom set: the caller marks its ghosts again
   CK(cudaStreamSynchronize(c->stream));
   c->have_atoms = true;
   c->sorted_once = false;
@@ -1129,6 +1135,10 @@ int b200_run(b200_ctx *c, int nsteps, double dt, double ftm2v, int thermo_every,
              int maxrows, int *nrows) {
   if (!c || nsteps < 0) return B200_ERR_ARG;
   if (!c->sorted_once) return set_err(c, B200_ERR_STATE, "b200_setup not called");
+  if (c->ghosts_on)
+    return set_err(c, B200_ERR_STATE,
+                   "b200_run with ghost atoms: a decomposed box steps through the per-call entry "
+                   "points and the halo exchange");
   CK(cudaSetDevice(c->device));
   const double dtv = dt, dtf = 0.5 * dt * ftm2v;  // FixNVE::init (src/fix_nve.cpp:52-59)
   // thermo rows: room for every output step of this run
@@ -1490,6 +1500,62 @@ int b200_adj_backward(b200_ctx *c, const double *lj1, const double *lj2, const d
 }
 
 // ---- replicas --------------------------------------------------------------
+
+// ---- spatial decomposition: ghosts, distance check, halo ----------------------
+
+int b200_set_ghosts(b200_ctx *c, const int *ghost) {
+  if (!c) return B200_ERR_ARG;
+  if (!c->have_atoms) return set_err(c, B200_ERR_STATE, "no atoms uploaded");
+  if (c->nrep) return set_err(c, B200_ERR_STATE, "ghost atoms with replicas");
+  CK(cudaSetDevice(c->device));
+  if (!ghost) {
+    c->ghosts_on = false;
+    return B200_OK;
+  }
+  CK(cudaMemcpyAsync(c->ghost, ghost, (size_t)c->n * sizeof(int), cudaMemcpyHostToDevice,
+                     c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->ghosts_on = true;
+  return B200_OK;
+}
+
+int b200_neigh_check(b200_ctx *c, int *moved) {
+  if (!c || !moved) return B200_ERR_ARG;
+  if (!c->sorted_once) return set_err(c, B200_ERR_STATE, "neighbor list not built");
+  CK(cudaSetDevice(c->device));
+  CK(cudaMemcpyAsync(c->status_host + ST_MOVED, c->status + ST_MOVED, sizeof(int),
+                     cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemsetAsync(c->status + ST_MOVED, 0, sizeof(int), c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *moved = c->status_host[ST_MOVED] != 0;
+  return B200_OK;
+}
+
+static int halo_call(b200_ctx *c, int m, const int *idx, const double *buf, bool pack) {
+  if (!c || m < 0 || (m > 0 && (!idx || !buf))) return B200_ERR_ARG;
+  if (!c->sorted_once) return set_err(c, B200_ERR_STATE, "neighbor list not built");
+  CK(cudaSetDevice(c->device));
+  if (m == 0) return B200_OK;
+  CK(cudaMemsetAsync(c->status + ST_HALO_BAD, 0, sizeof(int), c->stream));
+  if (pack)
+    CK(md_halo_pack(c, m, idx, const_cast<double *>(buf)));
+  else
+    CK(md_halo_unpack(c, m, idx, buf));
+  int rc = read_status(c);
+  if (rc) return rc;
+  if (c->status_host[ST_HALO_BAD])
+    return set_err(c, B200_ERR_ARG, "halo %s: an atom index is outside [0, %d)",
+                   pack ? "pack" : "unpack", c->n);
+  return B200_OK;
+}
+
+int b200_halo_pack(b200_ctx *c, int m, const int *idx, double *buf) {
+  return halo_call(c, m, idx, buf, true);
+}
+
+int b200_halo_unpack(b200_ctx *c, int m, const int *idx, const double *buf) {
+  return halo_call(c, m, idx, buf, false);
+}
 
 int b200_set_replicas(b200_ctx *c, int nrep, const int *natoms, const double *lo,
                       const double *hi) {

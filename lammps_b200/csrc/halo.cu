@@ -1,0 +1,92 @@
+// halo.cu -- per-step forward communication of ghost positions for a
+// spatially decomposed box.
+//
+// A rank's context holds its own atoms and, as ghosts, copies of the atoms of
+// other ranks that lie within the ghost depth of its brick, all in the one
+// periodic box.  Between rebuilds the ghost set is fixed and each step only
+// refreshes ghost positions from their owners, as CommBrick::forward_comm
+// does with AtomVecAtomic::pack_comm / unpack_comm
+// (src/comm_brick.cpp:444-511, src/atom_vec_atomic.cpp:105-217).  The atoms
+// are addressed by caller index (upload order); `where` maps a caller index
+// to the atom's current slot in the cell-sorted order.  A ghost is a copy of
+// the owner's coordinates, not a periodic image: the builder forms the images.
+#include "md_state.h"
+
+namespace {
+
+__global__ void k_where(int n, const int *__restrict__ orig, int *__restrict__ where) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) where[orig[k]] = k;
+}
+
+__global__ void k_halo_pack(int m, int n, const int *__restrict__ idx,
+                            const int *__restrict__ where, const double4 *__restrict__ x4,
+                            double *__restrict__ buf, int *__restrict__ status) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const int j = idx[i];
+  if (j < 0 || j >= n) {
+    atomicExch(&status[ST_HALO_BAD], 1);
+    return;
+  }
+  const double4 p = x4[where[j]];
+  buf[3 * (size_t)i] = p.x;
+  buf[3 * (size_t)i + 1] = p.y;
+  buf[3 * (size_t)i + 2] = p.z;
+}
+
+__global__ void k_halo_unpack(int m, int n, const int *__restrict__ idx,
+                              const int *__restrict__ where, const double *__restrict__ buf,
+                              double4 *__restrict__ x4, float4 *__restrict__ xr,
+                              const int *__restrict__ cell, BoxGeom box,
+                              int *__restrict__ status) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const int j = idx[i];
+  if (j < 0 || j >= n) {
+    atomicExch(&status[ST_HALO_BAD], 1);
+    return;
+  }
+  const int k = where[j];
+  double4 p = x4[k];
+  p.x = buf[3 * (size_t)i];
+  p.y = buf[3 * (size_t)i + 1];
+  p.z = buf[3 * (size_t)i + 2];
+  x4[k] = p;
+  if (xr) {
+    // the cell-relative FP32 copy, formed as the integrator forms it
+    int cx, cy, cz;
+    md_cell_unpack(cell[k], cx, cy, cz);
+    const double ox = box.lo[0] + (cx + 0.5) * box.cs[0];
+    const double oy = box.lo[1] + (cy + 0.5) * box.cs[1];
+    const double oz = box.lo[2] + (cz + 0.5) * box.cs[2];
+    xr[k] = make_float4((float)(p.x - ox), (float)(p.y - oy), (float)(p.z - oz),
+                        __int_as_float((int)p.w));
+  }
+}
+
+}  // namespace
+
+cudaError_t md_where(b200_ctx *c) {
+  if (c->n < 1) return cudaSuccess;
+  k_where<<<md_blocks(c->n, 256), 256, 0, c->stream>>>(c->n, c->orig, c->where);
+  c->launches++;
+  return cudaGetLastError();
+}
+
+cudaError_t md_halo_pack(b200_ctx *c, int m, const int *idx, double *buf) {
+  if (m < 1) return cudaSuccess;
+  k_halo_pack<<<md_blocks(m, 256), 256, 0, c->stream>>>(m, c->n, idx, c->where, c->x4, buf,
+                                                        c->status);
+  c->launches++;
+  return cudaGetLastError();
+}
+
+cudaError_t md_halo_unpack(b200_ctx *c, int m, const int *idx, const double *buf) {
+  if (m < 1) return cudaSuccess;
+  k_halo_unpack<<<md_blocks(m, 256), 256, 0, c->stream>>>(
+      m, c->n, idx, c->where, buf, c->x4, c->prec == B200_PREC_MIXED ? c->xr : nullptr, c->cell,
+      c->box, c->status);
+  c->launches++;
+  return cudaGetLastError();
+}

@@ -82,10 +82,14 @@ __global__ void __launch_bounds__(256) k_nve_initial(int n, int stride, double d
                                                       const int *__restrict__ cell, BoxGeom box1,
                                                       Reps reps,
                                                       const double4 *__restrict__ xhold,
-                                                      double triggersq, int *__restrict__ status) {
+                                                      double triggersq, int *__restrict__ status,
+                                                      const int *__restrict__ ghost,
+                                                      const int *__restrict__ orig) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   bool moved = false;
-  if (i < n) {
+  // a ghost (an atom another rank owns) is neither moved nor checked here:
+  // the halo unpack overwrites its position with the owner's
+  if (i < n && !(ghost && ghost[orig[i]])) {
     double4 p = x4[i];
     const double dtfm = dtf / mass[(int)p.w];
     double vx = __dadd_rn(v[i], __dmul_rn(dtfm, f[i]));
@@ -125,11 +129,12 @@ __global__ void __launch_bounds__(256) k_nve_final(int n, int stride, double dtf
                                                     double *__restrict__ v,
                                                     const double *__restrict__ f,
                                                     double *partial, unsigned int *counter,
-                                                    double *out) {
+                                                    double *out, const int *__restrict__ ghost,
+                                                    const int *__restrict__ orig) {
   __shared__ double red[8];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double acc[1] = {0.0};
-  if (i < n) {
+  if (i < n && !(ghost && ghost[orig[i]])) {
     const double m = mass[(int)x4[i].w];
     const double dtfm = dtf / m;
     const double vx = __dadd_rn(v[i], __dmul_rn(dtfm, f[i]));
@@ -258,24 +263,29 @@ cudaError_t md_nve_initial(b200_ctx *c, double dtv, double dtf) {
     k_nve_initial<true><<<md_blocks(c->n, B), B, 0, c->stream>>>(
         c->n, c->stride, dtv, dtf, c->mass_dev, c->x4, c->v, c->f,
         c->prec == B200_PREC_MIXED ? c->xr : nullptr, c->cell, c->box, c->reps(),
-        c->check ? c->xhold : nullptr, triggersq, c->status);
+        c->check ? c->xhold : nullptr, triggersq, c->status, c->ghosts_on ? c->ghost : nullptr,
+        c->orig);
   else
     k_nve_initial<false><<<md_blocks(c->n, B), B, 0, c->stream>>>(
         c->n, c->stride, dtv, dtf, c->mass_dev, c->x4, c->v, c->f,
         c->prec == B200_PREC_MIXED ? c->xr : nullptr, c->cell, c->box, c->reps(),
-        c->check ? c->xhold : nullptr, triggersq, c->status);
+        c->check ? c->xhold : nullptr, triggersq, c->status, c->ghosts_on ? c->ghost : nullptr,
+        c->orig);
   c->launches++;
   return cudaGetLastError();
 }
 
 cudaError_t md_nve_final(b200_ctx *c, double dtf, bool ke) {
   const int B = 256;
+  const int *gh = c->ghosts_on ? c->ghost : nullptr;
   if (ke)
     k_nve_final<true><<<md_blocks(c->n, B), B, 0, c->stream>>>(
-        c->n, c->stride, dtf, c->mass_dev, c->x4, c->v, c->f, c->partial, c->counter, c->ev + 7);
+        c->n, c->stride, dtf, c->mass_dev, c->x4, c->v, c->f, c->partial, c->counter, c->ev + 7,
+        gh, c->orig);
   else
     k_nve_final<false><<<md_blocks(c->n, B), B, 0, c->stream>>>(
-        c->n, c->stride, dtf, c->mass_dev, c->x4, c->v, c->f, c->partial, c->counter, c->ev + 7);
+        c->n, c->stride, dtf, c->mass_dev, c->x4, c->v, c->f, c->partial, c->counter, c->ev + 7,
+        gh, c->orig);
   c->launches++;
   return cudaGetLastError();
 }

@@ -40,6 +40,7 @@ enum {
   ST_STEP_HI = 10,
   ST_FORCE_BUILD = 11,  // rebuild on the next step regardless of the schedule
   ST_MAXSTAGE = 12,     // most atoms staged by one neighbor-builder tile since setup
+  ST_HALO_BAD = 13,     // a halo pack/unpack index was outside [0, n)
   ST_COUNT = 16
 };
 

@@ -95,6 +95,11 @@ struct b200_ctx {
   int *orig = nullptr, *origb = nullptr;
   int *image = nullptr, *imageb = nullptr;
   int *cell = nullptr;        // packed cell of each sorted atom
+  int *where = nullptr;       // sorted slot of each caller index (inverse of orig)
+  // ghost atoms (b200_set_ghosts): per caller index, nonzero for an atom that
+  // another rank owns; such atoms are neither integrated nor distance-checked
+  int *ghost = nullptr;
+  bool ghosts_on = false;
   float4 *xr = nullptr;       // mixed: cell-relative coordinates
   double4 *xhold = nullptr;   // positions at the last build (check yes)
   // device staging of host transfers (upload, download, per-atom energy and
@@ -184,6 +189,13 @@ bool md_stage_feedback(b200_ctx *c, int staged_max);
 // LAMMPS half list derived from the full list; returns entry count via *total
 cudaError_t md_half_list(b200_ctx *c, int *d_num, int *d_jowner, int *d_jimage, long long cap,
                          long long *total);
+// ---- halo (halo.cu) ---------------------------------------------------------
+// where[orig[k]] = k for the n sorted atoms
+cudaError_t md_where(b200_ctx *c);
+// buf[3i..3i+2] = x of caller atom idx[i]; idx, buf on the device
+cudaError_t md_halo_pack(b200_ctx *c, int m, const int *idx, double *buf);
+// x of caller atom idx[i] = buf[3i..3i+2] (and its cell-relative FP32 copy)
+cudaError_t md_halo_unpack(b200_ctx *c, int m, const int *idx, const double *buf);
 // ---- pair kernels (pair_lj.cu, pair_eam.cu) --------------------------------
 cudaError_t md_lj_compute(b200_ctx *c, bool ev, bool atom_ev, double *eatom, double *vatom);
 // `mid`, when given, is recorded between the density and the force kernel

@@ -10,7 +10,8 @@
 //   3 k_scatter     counting-sort scatter of atom indices; zeroes the counts
 //   4 k_sort_cells  order each cell by caller index (deterministic order)
 //   5 k_gather      permute x, v, ids; cell-relative FP32 copy; xhold
-//   6 k_copyback    permuted arrays back into the primary buffers; ago = 0
+//   6 k_copyback    permuted arrays back into the primary buffers, the
+//                   caller-index -> slot map; ago = 0
 //   7 k_neigh_tiles full list over the 27 neighbor cells (cell >= rc+skin),
 //                   neighbor-cell tiles staged in shared memory
 // The pair test is the reference's, bit for bit: the periodic image is
@@ -228,7 +229,8 @@ __global__ void k_copyback(int n, int stride, const double4 *__restrict__ x4b,
                            double4 *__restrict__ x4, const double *__restrict__ vb,
                            double *__restrict__ v, const int *__restrict__ origb,
                            int *__restrict__ orig, const int *__restrict__ imageb,
-                           int *__restrict__ image, int *__restrict__ status, const int *flag) {
+                           int *__restrict__ image, int *__restrict__ where,
+                           int *__restrict__ status, const int *flag) {
   if (!rebuild_on(flag)) return;
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k == 0) {
@@ -241,7 +243,9 @@ __global__ void k_copyback(int n, int stride, const double4 *__restrict__ x4b,
   v[k] = vb[k];
   v[stride + k] = vb[stride + k];
   v[2 * stride + k] = vb[2 * stride + k];
-  orig[k] = origb[k];
+  const int o = origb[k];
+  orig[k] = o;
+  where[o] = k;  // caller index -> sorted slot, for the halo pack / unpack
   image[k] = imageb[k];
 }
 
@@ -691,7 +695,7 @@ cudaError_t md_rebuild(b200_ctx *c, const int *d_flag) {
         c->check ? c->xhold : nullptr, d_flag);
   k_copyback<<<md_blocks(n, B), B, 0, c->stream>>>(n, c->stride, c->x4b, c->x4, c->vb, c->v,
                                                    c->origb, c->orig, c->imageb, c->image,
-                                                   c->status, d_flag);
+                                                   c->where, c->status, d_flag);
   {
     const int tiles = c->nrep ? c->ntiles
                               : ((c->box.ncell[0] + kTileCells - 1) / kTileCells) *

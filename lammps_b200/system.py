@@ -26,6 +26,7 @@ class System:
         self.units = units
         self.u = UNITS[units]
         self.precision = precision
+        self.device = f"cuda:{device}"
         h = C.c_void_p()
         rc = self._L.b200_create(device, _abi.PREC[precision], C.byref(h))
         self._h = h
@@ -66,6 +67,7 @@ class System:
     def set_neighbor(self, skin=None, every=1, delay=10, check=True, one=0):
         skin = self.u["skin"] if skin is None else skin
         self.skin = skin
+        self.every, self.delay, self.check = int(every), int(delay), bool(check)
         self._ck(self._L.b200_set_neighbor(self._h, skin, every, delay, int(check), one))
 
     def set_pair(self, pair):
@@ -147,6 +149,50 @@ class System:
         self._ck(self._L.b200_download_atoms(self._h, _abi.dptr(out["x"]), _abi.dptr(out["v"]),
                                              _abi.dptr(out["f"]), _abi.iptr(out["image"])))
         return out
+
+    def cutforce(self):
+        """Largest force cutoff of the pair style (Pair::cutforce)."""
+        if isinstance(self.pair, PairEAM):
+            return float(self.tables["cutmax"])
+        return float(np.sqrt(np.max(self.tables["cutsq"])))
+
+    # ---- spatial decomposition (lammps_b200.brick) -----------------------
+    def set_ghosts(self, ghost):
+        """Mark ghost atoms (caller order; None clears): not integrated, not
+        distance-checked, positions set by halo_unpack."""
+        g = None if ghost is None else np.ascontiguousarray(ghost, dtype=np.int32)
+        if g is not None and g.shape != (self.n,):
+            raise ValueError(f"set_ghosts: need {self.n} flags")
+        self._ck(self._L.b200_set_ghosts(self._h, _abi.iptr(g)))
+
+    def neigh_check(self):
+        """The local half of Neighbor::check_distance since the last call."""
+        m = C.c_int(0)
+        self._ck(self._L.b200_neigh_check(self._h, C.byref(m)))
+        return bool(m.value)
+
+    def nve_initial(self):
+        self._ck(self._L.b200_nve_initial(self._h, self.dt, 0.5 * self.dt * self.u["ftm2v"]))
+
+    def nve_final(self):
+        self._ck(self._L.b200_nve_final(self._h, 0.5 * self.dt * self.u["ftm2v"]))
+
+    @staticmethod
+    def _dev_args(idx, buf):
+        if not (idx.is_cuda and buf.is_cuda and idx.dtype.itemsize == 4 and buf.is_contiguous()
+                and idx.is_contiguous() and buf.numel() == 3 * idx.numel()):
+            raise ValueError("halo: idx (m int32) and buf (3m float64) must be contiguous CUDA tensors")
+        return idx.numel(), C.c_void_p(idx.data_ptr()), C.c_void_p(buf.data_ptr())
+
+    def halo_pack(self, idx, buf):
+        """buf[i] = x of atom idx[i] (device tensors)."""
+        m, pi, pb = self._dev_args(idx, buf)
+        self._ck(self._L.b200_halo_pack(self._h, m, pi, pb))
+
+    def halo_unpack(self, idx, buf):
+        """x of atom idx[i] = buf[i] (device tensors)."""
+        m, pi, pb = self._dev_args(idx, buf)
+        self._ck(self._L.b200_halo_unpack(self._h, m, pi, pb))
 
     # ---- actions ---------------------------------------------------------
     def neigh_build(self):

@@ -1,0 +1,131 @@
+"""The brick decomposition on the device: bricks of one box as separate
+engine contexts on one GPU, stepped together in one process (`LocalComm`;
+the halo exchange is a device copy and no kernel waits on another).  Each
+owned atom sees the same neighbors in the same order as in the single box,
+so a decomposed run must reproduce the single-box trajectory bit for bit --
+for lj/cut and EAM, FP64 and mixed, through rebuilds (check yes) with
+exchange and borders, and the per-step halo pack / unpack in between."""
+import os
+
+import numpy as np
+import pytest
+
+from lammps_b200 import PairEAM, PairLJCut, System, inputs
+from lammps_b200._abi import B200Error
+from lammps_b200.brick import BrickRun, LocalComm
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+TPA = 4
+
+
+def _lj(precision):
+    a = inputs.lj_lattice_constant("fcc", 0.8442)
+    x = inputs.lattice("fcc", 10, 10, 10, a)
+    L = 10 * a
+
+    def make():
+        s = System("lj", precision)
+        s.set_box([0.0] * 3, [L] * 3)
+        p = PairLJCut(2.5)
+        p.coeff(1, 1, 1.0, 1.0, 2.5)
+        s.set_pair(p)
+        s.set_mass([1.0])
+        s.set_neighbor(0.3, every=1, delay=0, check=True)
+        s.set_launch(TPA, 128)
+        return s
+
+    v = make().create_velocity(x, 1.44, 87287, gaussian=True)
+    return make, x, v, 200
+
+
+def _eam(precision):
+    x = inputs.lattice("fcc", 10, 10, 10, 3.615)
+    L = 10 * 3.615
+
+    def make():
+        s = System("metal", precision)
+        s.set_box([0.0] * 3, [L] * 3)
+        p = PairEAM(1)
+        p.coeff(1, os.path.join(ROOT, "tests", "golden", "Cu_u3.eam"))
+        s.set_pair(p)
+        s.set_neighbor(1.0, every=1, delay=5, check=True)
+        s.set_timestep(0.005)
+        s.set_launch(TPA, 128)
+        return s
+
+    v = make().create_velocity(x, 1600.0, 376847, gaussian=True)
+    return make, x, v, 100
+
+
+def _brick(case, grid):
+    make, x, v, steps = case
+    comm = LocalComm(int(np.prod(grid)))
+    b = BrickRun(comm, {r: make() for r in comm.ranks}, grid)
+    b.set_atoms(x, None, v)
+    b.setup()
+    rows = b.run(steps, thermo_every=steps // 2)
+    return b, rows, b.gather()
+
+
+@pytest.mark.parametrize("style", ["lj", "eam"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_bricks_reproduce_single_box(style, precision):
+    case = (_lj if style == "lj" else _eam)(precision)
+    b1, rows1, ref = _brick(case, (1, 1, 1))
+    assert b1.ncalls >= 2
+    for grid in ((2, 1, 1), (2, 2, 1)):
+        b, rows, got = _brick(case, grid)
+        assert b.ncalls == b1.ncalls, grid
+        for k in ("x", "v", "image"):
+            assert np.array_equal(got[k], ref[k]), (grid, k, float(np.abs(got[k] - ref[k]).max()))
+        assert all(s["ghost"] > 0 for s in b.stats().values())
+        for r1, r2 in zip(rows1, rows):
+            for k in ("Temp", "E_pair", "Press"):
+                assert r2[k] == pytest.approx(r1[k], rel=1e-11, abs=1e-11), (grid, k)
+
+
+@pytest.mark.parametrize("style", ["lj", "eam"])
+def test_one_brick_matches_graph_run(style):
+    """The per-call path of one brick and b200_run's step graphs take the same
+    rounded steps: same trajectory, same thermo."""
+    make, x, v, steps = (_lj if style == "lj" else _eam)("fp64")
+    b1, rows1, ref = _brick((make, x, v, steps), (1, 1, 1))
+    s = make()
+    s.set_atoms(x, None, v)
+    s.set_thermo(steps // 2)
+    s.setup()
+    rows = s.run(steps)
+    d = s.download()
+    assert np.array_equal(d["x"], ref["x"])
+    assert np.array_equal(d["v"], ref["v"])
+    assert np.array_equal(d["image"], ref["image"])
+    assert s.neigh_stats()["ncalls"] == b1.ncalls
+    by_step = {r["Step"]: r for r in rows}
+    assert steps in by_step
+    for r1 in rows1:
+        r2 = by_step[r1["Step"]]
+        for k in ("Temp", "E_pair", "Press"):
+            assert r2[k] == pytest.approx(r1[k], rel=1e-11, abs=1e-11), k
+
+
+def test_halo_index_errors_are_reported():
+    make, x, v, _ = _lj("fp64")
+    s = make()
+    s.set_atoms(x, None, v)
+    s.neigh_build()
+    idx = torch.tensor([0, len(x)], dtype=torch.int32, device="cuda")
+    buf = torch.zeros((2, 3), dtype=torch.float64, device="cuda")
+    with pytest.raises(B200Error, match="outside"):
+        s.halo_pack(idx, buf)
+    # the context stays usable
+    s.halo_pack(idx[:1], buf[:1])
+    assert buf[0].cpu().numpy().tolist() == list(x[0])
+    # b200_run decides rebuilds alone: it refuses a context with ghosts
+    s.set_ghosts(np.ones(len(x)))
+    s.setup()
+    with pytest.raises(B200Error, match="ghost"):
+        s.run(1)
