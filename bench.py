@@ -110,7 +110,7 @@ def lj4m_inputs():
     return x, v, np.array([100 * a] * 3)
 
 
-def make_lj(precision, x, v, hi):
+def make_lj(precision, x, v, hi, atoms=True):
     from lammps_b200 import PairLJCut, System
     s = System("lj", precision, device=DEVICE)
     s.set_box([0.0, 0.0, 0.0], hi)
@@ -121,7 +121,8 @@ def make_lj(precision, x, v, hi):
     s.set_neighbor(0.3, every=20, delay=0, check=False)
     s.set_timestep(0.005)
     s.set_thermo(0)
-    s.set_atoms(x, None, v)
+    if atoms:
+        s.set_atoms(x, None, v)
     return s
 
 
@@ -422,6 +423,42 @@ def replica_bench(prec, batch, torch, steps=1000, lat_steps=200):
     return out
 
 
+def brick_bench(torch, x, v, hi, steps=40, warm=20):
+    """One box split into bricks (lammps_b200.brick) on this one GPU: the
+    per-call step of one brick, and of 2 bricks (2 x 1 x 1) as separate
+    contexts whose halo exchange is a device copy.  The bricks of a step run
+    one after the other here; on N GPUs they run side by side.  Wall time
+    around host-synchronous steps (each entry point returns after its
+    stream)."""
+    from lammps_b200.brick import BrickRun, LocalComm
+    out = {"atoms": len(x), "steps": steps,
+           "note": "LJ fcc 4M, rc 2.5, skin 0.3, every 20 check no; per-call steps with "
+                   "rebuild (exchange + borders) every 20 steps and a halo exchange on the others"}
+    for prec in ("fp64", "mixed"):
+        for grid in ((1, 1, 1), (2, 1, 1)):
+            comm = LocalComm(int(np.prod(grid)))
+            b = BrickRun(comm, {r: make_lj(prec, x, v, hi, atoms=False) for r in comm.ranks}, grid)
+            b.set_atoms(x, None, v)
+            b.setup()
+            b.run(warm)
+            torch.cuda.synchronize()
+            b.timers = {k: 0.0 for k in b.timers}
+            t0 = time.perf_counter()
+            b.run(steps)
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+            key = f"{prec}_{'x'.join(map(str, grid))}"
+            st = b.stats()
+            out[key] = {"ms_per_step": dt / steps * 1e3,
+                        "matom_steps_per_s": len(x) * steps / dt / 1e6,
+                        "ghost_atoms": sum(q["ghost"] for q in st.values()),
+                        "rebuilds": b.ncalls,
+                        "ms_per_step_by_phase": {k: t / steps * 1e3 for k, t in b.timers.items()}}
+            for e in b.st.values():
+                e.engine.close()
+    return out
+
+
 def dist_setup():
     import torch
     ws = int(os.environ.get("WORLD_SIZE", "1"))
@@ -694,6 +731,7 @@ def main():
             s.close()
         em["mixed_over_fp64"] = em["mixed"] / em["fp64"]
         extras["eam_4M"] = em
+        extras["bricks_lj_4M"] = brick_bench(torch, x4, v4, hi4)
 
     if not args.no_extras:
         from lammps_b200.replicas import replica_batch, shard_batch

@@ -108,7 +108,10 @@ int b200_set_eam(b200_ctx *ctx, int ntypes, int nrho, double drho, int nr, doubl
 /* ---- atoms ----------------------------------------------------------------- */
 
 /* Copy n atoms to the device (AtomVec x, v, type, tag; ljl_gpu_compute's x
-   upload, lib/gpu/lal_base_atomic.cpp:176-241).  v may be NULL (zero). */
+   upload, lib/gpu/lal_base_atomic.cpp:176-241).  v may be NULL (zero).  The
+   arrays may be host or device memory (unified addressing), as may the
+   destinations of b200_download_atoms and the per-atom arrays of
+   b200_pair_compute. */
 int b200_upload_atoms(b200_ctx *ctx, int n, const double *x, const double *v, const int *type,
                       const int *tag);
 /* Copy positions, velocities, forces and image flags back, in the caller's
@@ -207,7 +210,7 @@ void *b200_stream(const b200_ctx *ctx);
    transport).
 
    Mark the ghosts of the current atoms: ghost[i] != 0 for caller index i
-   (upload order), n ints on the host; NULL clears.  Ghosts are not
+   (upload order), n ints in host or device memory; NULL clears.  Ghosts are not
    integrated by b200_nve_initial / b200_nve_final, are left out of the
    distance check and of the kinetic energy, and get their positions from
    b200_halo_unpack.  Cleared by every b200_upload_atoms.  b200_run refuses a

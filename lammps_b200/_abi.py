@@ -102,6 +102,16 @@ def iptr(a):
     return None if a is None else a.ctypes.data_as(_ip)
 
 
+def tdptr(t):
+    """double* of a contiguous float64 torch tensor (host or device)."""
+    return None if t is None else C.cast(C.c_void_p(t.data_ptr()), _dp)
+
+
+def tiptr(t):
+    """int* of a contiguous int32 torch tensor (host or device)."""
+    return None if t is None else C.cast(C.c_void_p(t.data_ptr()), _ip)
+
+
 class B200Error(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"{STATUS_NAMES.get(code, code)}: {msg}")

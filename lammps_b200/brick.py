@@ -23,10 +23,11 @@ How it differs from the reference, and why:
   each cell by caller index, so every owned atom's neighbor list holds the
   same entries in the same order as in the single box: forces, and with them
   whole trajectories, are bit-identical to the single-box run.
-- The exchange and borders steps (src/comm_brick.cpp:573-864) run at each
-  rebuild through host memory; the per-step forward communication of ghost
-  positions (src/comm_brick.cpp:444-511) stays on the device
-  (b200_halo_pack / b200_halo_unpack and one all-to-all).
+- Atom data stays on the rank's device.  The exchange and borders steps
+  (src/comm_brick.cpp:573-864) at each rebuild are tensor operations there
+  plus two all-to-alls; the per-step forward communication of ghost
+  positions (src/comm_brick.cpp:444-511) is b200_halo_pack, one all-to-all
+  and b200_halo_unpack.
 
 The ranks may all live in one process (`LocalComm`: one engine per rank, the
 exchange a copy) or one per process (`DistComm`: torch.distributed, NCCL for
@@ -38,28 +39,53 @@ from __future__ import annotations
 import numpy as np
 import torch
 
+import time
+
 from .pair import PairEAM
 
-# record columns of an atom sent between ranks
+# record columns of an atom sent between ranks (float64 rows: ids, types and
+# image flags are exact)
 _GID, _TYPE, _IMG, _X, _V, _W = 0, 1, 2, 5, 8, 11
 
 
 def pbc(x, image, lo, hi):
     """Domain::pbc for an orthogonal box (src/domain.cpp:478-560): x < lo ->
     x + prd, image - 1; x >= hi -> x - prd, max(x, lo), image + 1.  Same
-    rounded operations as the device's wrap."""
-    x = np.array(x, dtype=np.float64, copy=True)
-    image = np.array(image, dtype=np.int64, copy=True)
-    prd = hi - lo
+    rounded operations as the device's wrap.  Torch tensors (any device) or
+    numpy arrays."""
+    as_np = isinstance(x, np.ndarray)
+    xt = torch.from_numpy(np.array(x, dtype=np.float64)) if as_np else x.clone()
+    it = (torch.from_numpy(np.array(image, dtype=np.int64)) if as_np
+          else image.to(torch.int64).clone())
     for d in range(3):
-        xd = x[:, d]
-        m = xd < lo[d]
-        xd[m] = xd[m] + prd[d]
-        image[m, d] -= 1
-        m = xd >= hi[d]
-        xd[m] = np.maximum(xd[m] - prd[d], lo[d])
-        image[m, d] += 1
-    return x, image
+        lo_d, hi_d = float(lo[d]), float(hi[d])
+        prd = hi_d - lo_d
+        xd = xt[:, d]
+        m = xd < lo_d
+        xd = torch.where(m, xd + prd, xd)
+        it[:, d] -= m.to(torch.int64)
+        m = xd >= hi_d
+        xd = torch.where(m, torch.clamp_min(xd - prd, lo_d), xd)
+        it[:, d] += m.to(torch.int64)
+        xt[:, d] = xd
+    return (xt.numpy(), it.numpy()) if as_np else (xt, it)
+
+
+def _merge_by_gid(a, b):
+    """Rows of a (sorted by global id) and b (any order) in one array sorted by
+    global id, with the positions the rows of a and of b went to.  b is the
+    small side (ghosts, migrants): only b is sorted."""
+    ob = torch.argsort(b[:, _GID], stable=True)
+    b = b[ob]
+    ga, gb = a[:, _GID].contiguous(), b[:, _GID].contiguous()
+    pa = torch.arange(len(a), device=a.device) + torch.searchsorted(gb, ga)
+    pb = torch.arange(len(b), device=a.device) + torch.searchsorted(ga, gb)
+    out = torch.empty((len(a) + len(b), a.shape[1]), dtype=a.dtype, device=a.device)
+    out[pa] = a
+    out[pb] = b
+    posb = torch.empty_like(pb)
+    posb[ob] = pb
+    return out, pa, posb
 
 
 class BrickGrid:
@@ -77,8 +103,8 @@ class BrickGrid:
         self.splits = []
         for d in range(3):
             p = self.grid[d]
-            s = np.array([self.lo[d] + self.prd[d] * (i * 1.0 / p) for i in range(p)] + [self.hi[d]])
-            self.splits.append(s)
+            sp = np.array([self.lo[d] + self.prd[d] * (i * 1.0 / p) for i in range(p)] + [self.hi[d]])
+            self.splits.append(sp)
 
     def coords(self, rank):
         px, py, _ = self.grid
@@ -91,26 +117,35 @@ class BrickGrid:
         return blo, bhi
 
     def owner(self, x):
-        """Rank owning each (wrapped) position."""
-        c = [np.searchsorted(self.splits[d][1:-1], x[:, d], side="right") for d in range(3)]
+        """Rank owning each (wrapped) position (torch or numpy)."""
+        as_np = isinstance(x, np.ndarray)
+        xt = torch.from_numpy(x) if as_np else x
+        c = []
+        for d in range(3):
+            inner = torch.tensor(self.splits[d][1:-1], dtype=torch.float64, device=xt.device)
+            c.append(torch.searchsorted(inner, xt[:, d].contiguous(), right=True))
         px, py, _ = self.grid
-        return (c[0] + px * (c[1] + py * c[2])).astype(np.int64)
+        r = (c[0] + px * (c[1] + py * c[2])).to(torch.int64)
+        return r.numpy() if as_np else r
 
     def near(self, x, rank, depth):
         """Atoms whose periodic distance to brick `rank` is at most `depth` in
         every dimension (a superset of those within `depth` in space)."""
+        as_np = isinstance(x, np.ndarray)
+        xt = torch.from_numpy(x) if as_np else x
         blo, bhi = self.bounds(rank)
-        ok = np.ones(len(x), dtype=bool)
+        ok = torch.ones(len(xt), dtype=torch.bool, device=xt.device)
         tol = depth * (1.0 + 1e-12) + 1e-12 * float(np.max(self.prd))
         for d in range(3):
             if self.grid[d] == 1:
                 continue
-            xd = x[:, d]
-            inside = (xd >= blo[d]) & (xd < bhi[d])
-            L = self.prd[d]
-            dist = np.minimum(np.mod(blo[d] - xd, L), np.mod(xd - bhi[d], L))
+            xd = xt[:, d]
+            inside = (xd >= float(blo[d])) & (xd < float(bhi[d]))
+            L = float(self.prd[d])
+            dist = torch.minimum(torch.remainder(float(blo[d]) - xd, L),
+                                 torch.remainder(xd - float(bhi[d]), L))
             ok &= inside | (dist <= tol)
-        return ok
+        return ok.numpy() if as_np else ok
 
 
 # ---- communicators ------------------------------------------------------------
@@ -184,10 +219,10 @@ class _Rank:
 
 
 def _records(gid, typ, img, x, v):
-    r = np.zeros((len(gid), _W))
-    r[:, _GID] = gid
-    r[:, _TYPE] = typ
-    r[:, _IMG:_IMG + 3] = img
+    r = torch.zeros((len(gid), _W), dtype=torch.float64, device=x.device)
+    r[:, _GID] = gid.to(torch.float64)
+    r[:, _TYPE] = typ.to(torch.float64)
+    r[:, _IMG:_IMG + 3] = img.to(torch.float64)
     r[:, _X:_X + 3] = x
     r[:, _V:_V + 3] = v
     return r
@@ -200,7 +235,9 @@ class BrickRun:
 
     `engines` maps each rank of `comm.ranks` to a configured engine
     (`System`: box, pair style, masses, neighbor settings and timestep set;
-    no atoms).  All engines must share those settings."""
+    no atoms).  All engines must share those settings.  Atom data stays on
+    each rank's device: the rebuild's exchange and borders are tensor
+    operations there, and the engine takes and returns device tensors."""
 
     def __init__(self, comm, engines, grid):
         self.comm = comm
@@ -221,8 +258,11 @@ class BrickRun:
         self.ago = 0
         self.ncalls = 0
         self.ndanger = 0
-        self.thermo_every = 0
         self.thermo_rows = []
+        # wall seconds per Timer category of the reference (src/timer.h:19-20):
+        # the entry points return after their stream, so host time is device
+        # time plus launch overhead
+        self.timers = dict(pair=0.0, neigh=0.0, comm=0.0, modify=0.0, output=0.0)
 
     @staticmethod
     def _box(engines):
@@ -237,54 +277,59 @@ class BrickRun:
         n = len(x)
         typ = np.ones(n, np.int64) if type_ is None else np.asarray(type_, dtype=np.int64)
         v = np.zeros((n, 3)) if v is None else np.asarray(v, dtype=np.float64)
-        xw, img = pbc(x, np.zeros((n, 3), np.int64), self.grid.lo, self.grid.hi)
-        own = self.grid.owner(xw)
-        gid = np.arange(n, dtype=np.int64)
         owned = {}
-        for r in self.comm.ranks:
-            m = own == r
-            owned[r] = _records(gid[m], typ[m], img[m], xw[m], v[m])
+        for r, s in self.st.items():
+            xt = torch.from_numpy(x).to(s.dev)
+            xw, img = pbc(xt, torch.zeros((n, 3), dtype=torch.int64, device=s.dev),
+                          self.grid.lo, self.grid.hi)
+            m = self.grid.owner(xw) == r
+            gid = torch.arange(n, dtype=torch.int64, device=s.dev)
+            owned[r] = _records(gid[m], torch.from_numpy(typ).to(s.dev)[m], img[m], xw[m],
+                                torch.from_numpy(v).to(s.dev)[m])
         self.natoms = n
         self._borders(owned)
 
     def gather(self):
         """Positions, velocities and image flags of all atoms by global id, on
-        every rank (for checks and output)."""
+        every rank, as numpy arrays (for checks and output)."""
         send, cnt = {}, {}
         for r, s in self.st.items():
             own = self._owned_records(s, wrap=False)
-            send[r] = torch.from_numpy(np.tile(own, (self.comm.world, 1)))
+            send[r] = own.repeat(self.comm.world, 1)
             cnt[r] = [len(own)] * self.comm.world
         got = self.comm.alltoall_rows(send, cnt)
         rows = got[self.comm.ranks[0]][0].cpu().numpy()
-        order = np.argsort(rows[:, _GID], kind="stable")
-        rows = rows[order]
+        rows = rows[np.argsort(rows[:, _GID], kind="stable")]
         return dict(x=rows[:, _X:_X + 3].copy(), v=rows[:, _V:_V + 3].copy(),
                     image=rows[:, _IMG:_IMG + 3].astype(np.int64), type=rows[:, _TYPE].astype(np.int64))
 
     def _owned_records(self, s, wrap):
-        d = s.engine.download()
+        d = s.engine.download_dev()
         own = ~s.ghost
         x = d["x"][own]
-        img = s.image[own] + d["image"][own]
+        img = s.image[own] + d["image"][own].to(torch.int64)
         if wrap:
             x, img = pbc(x, img, self.grid.lo, self.grid.hi)
         return _records(s.gid[own], s.type[own], img, x, d["v"][own])
 
     # ---- CommBrick::exchange + borders ---------------------------------------
     def _exchange(self, owned):
-        """Send every owned atom to the rank whose brick holds it."""
-        send, cnt = {}, {}
+        """Send every atom that left the brick to the rank whose brick holds it
+        (CommBrick::exchange); the atoms that stay keep their order."""
+        send, cnt, keep = {}, {}, {}
         for r, rec in owned.items():
             dest = self.grid.owner(rec[:, _X:_X + 3])
-            order = np.argsort(dest, kind="stable")
-            send[r] = torch.from_numpy(np.ascontiguousarray(rec[order]))
-            cnt[r] = np.bincount(dest, minlength=self.comm.world).tolist()
+            stay = dest == r
+            keep[r] = rec[stay]
+            go = ~stay
+            dg = dest[go]
+            order = torch.argsort(dg, stable=True)
+            send[r] = rec[go][order]
+            cnt[r] = torch.bincount(dg, minlength=self.comm.world).tolist()
         got = self.comm.alltoall_rows(send, cnt)
         out = {}
         for r, (rows, _) in got.items():
-            rows = rows.cpu().numpy()
-            out[r] = rows[np.argsort(rows[:, _GID], kind="stable")]
+            out[r] = _merge_by_gid(keep[r], rows.to(keep[r].device))[0] if len(rows) else keep[r]
         return out
 
     def _borders(self, owned):
@@ -294,42 +339,38 @@ class BrickRun:
         send, cnt, sel = {}, {}, {}
         for r, rec in owned.items():
             x = rec[:, _X:_X + 3]
-            parts, c, ss = [], [], []
+            parts, ss = [], []
             for q in range(self.comm.world):
-                k = (np.zeros(0, np.int64) if q == r
-                     else np.nonzero(self.grid.near(x, q, self.depth))[0])
-                g = rec[k].copy()
+                k = (torch.zeros(0, dtype=torch.int64, device=rec.device) if q == r
+                     else torch.nonzero(self.grid.near(x, q, self.depth)).flatten())
+                g = rec[k].clone()
                 g[:, _IMG:_IMG + 3] = 0
                 g[:, _V:_V + 3] = 0
                 parts.append(g)
-                c.append(len(k))
                 ss.append(k)
-            send[r] = torch.from_numpy(np.concatenate(parts) if parts else np.zeros((0, _W)))
-            cnt[r] = c
+            send[r] = torch.cat(parts)
+            cnt[r] = [len(k) for k in ss]
             sel[r] = ss
         got = self.comm.alltoall_rows(send, cnt)
         for r, (grec, rc) in got.items():
             s = self.st[r]
             own = owned[r]
-            grec = grec.cpu().numpy()
-            allr = np.concatenate([own, grec])
-            order = np.argsort(allr[:, _GID], kind="stable")
-            pos = np.empty(len(allr), np.int64)
-            pos[order] = np.arange(len(allr))
-            rows = allr[order]
-            s.gid = rows[:, _GID].astype(np.int64)
-            s.type = rows[:, _TYPE].astype(np.int64)
-            s.image = rows[:, _IMG:_IMG + 3].astype(np.int64)
-            s.ghost = np.zeros(len(rows), dtype=bool)
-            s.ghost[pos[len(own):]] = True
+            nown = len(own)
+            rows, pown, pgh = _merge_by_gid(own, grec.to(s.dev))
+            s.gid = rows[:, _GID].to(torch.int64)
+            s.type = rows[:, _TYPE].to(torch.int64)
+            s.image = rows[:, _IMG:_IMG + 3].to(torch.int64)
+            s.ghost = torch.zeros(len(rows), dtype=torch.bool, device=s.dev)
+            s.ghost[pgh] = True
+            s.nghost = len(rows) - nown
             s.send_counts = list(cnt[r])
             s.recv_counts = list(rc)
-            s.send_idx = torch.from_numpy(
-                np.concatenate([pos[k] for k in sel[r]]).astype(np.int32)).to(s.dev)
-            s.recv_idx = torch.from_numpy(pos[len(own):].astype(np.int32)).to(s.dev)
+            s.send_idx = torch.cat([pown[k] for k in sel[r]]).to(torch.int32)
+            s.recv_idx = pgh.to(torch.int32)
             e = s.engine
-            e.set_atoms(rows[:, _X:_X + 3], s.type.astype(np.int32), rows[:, _V:_V + 3])
-            e.set_ghosts(s.ghost.astype(np.int32) if s.ghost.any() else None)
+            e.set_atoms_dev(rows[:, _X:_X + 3].contiguous(), s.type.to(torch.int32),
+                            rows[:, _V:_V + 3].contiguous())
+            e.set_ghosts(s.ghost.to(torch.int32) if s.nghost else None)
             e.neigh_build()
 
     def _rebuild(self):
@@ -340,6 +381,8 @@ class BrickRun:
 
     # ---- CommBrick::forward_comm ---------------------------------------------
     def _forward(self):
+        if self.comm.world == 1:
+            return  # one brick holds no ghosts
         send, cnt, rcnt = {}, {}, {}
         for r, s in self.st.items():
             buf = torch.empty((len(s.send_idx), 3), dtype=torch.float64, device=s.dev)
@@ -369,26 +412,37 @@ class BrickRun:
         rows = {}
         for r, s in self.st.items():
             if thermo:
-                o = s.engine.compute(1, 1, per_atom=True)
+                o = s.engine.compute_dev()
                 own = ~s.ghost
-                rows[r] = np.concatenate([[0.0, o["eatom"][own].sum()], o["vatom"][own].sum(axis=0)])
+                rows[r] = torch.cat([torch.zeros(1, dtype=torch.float64, device=s.dev),
+                                     o["eatom"][own].sum().reshape(1),
+                                     o["vatom"][own].sum(dim=0)])
             else:
                 s.engine.compute(0, 0)
         return rows
 
     def _thermo_row(self, rows):
+        vals = {}
         for r, s in self.st.items():
-            d = s.engine.download()
+            d = s.engine.download_dev()
             own = ~s.ghost
             v = d["v"][own]
-            rows[r][0] = float(np.sum(self.mass[s.type[own]] * np.sum(v * v, axis=1)))
-        tot = self.comm.allreduce(rows, "sum")
+            m = torch.from_numpy(self.mass).to(s.dev)[s.type[own]]
+            row = rows[r].clone()
+            row[0] = torch.sum(m * torch.sum(v * v, dim=1))
+            vals[r] = row.cpu().numpy()
+        tot = self.comm.allreduce(vals, "sum")
         row = np.concatenate([[float(self.ntimestep)], tot])
         vol = float(np.prod(self.grid.prd))
         return self.e0._thermo(row, self.natoms, vol)
 
     # ---- Verlet ------------------------------------------------------------------
     def setup(self):
+        for s in self.st.values():
+            # an engine without a launch shape picks one by timing its own
+            # pair kernel on its atoms (b200_setup's search)
+            if hasattr(s.engine, "launch") and s.engine.launch()[0] == 0:
+                s.engine.setup()
         rows = self._force(True)
         r = self._thermo_row(rows)
         self.thermo_rows = [r]
@@ -398,25 +452,39 @@ class BrickRun:
 
     def run(self, nsteps, thermo_every=0):
         out = []
+        T = self.timers
+        clock = time.perf_counter
         for k in range(1, nsteps + 1):
             self.ntimestep += 1
             thermo = (thermo_every > 0 and k % thermo_every == 0) or k == nsteps
+            t0 = clock()
             for s in self.st.values():
                 s.engine.nve_initial()
             moved = {r: (s.engine.neigh_check() if self.check else False) for r, s in self.st.items()}
+            t1 = clock()
+            T["modify"] += t1 - t0
             if self._decide(moved):
                 self._rebuild()
+                t2 = clock()
+                T["neigh"] += t2 - t1
             else:
                 self._forward()
+                t2 = clock()
+                T["comm"] += t2 - t1
             rows = self._force(thermo)
+            t3 = clock()
+            T["pair"] += t3 - t2
             for s in self.st.values():
                 s.engine.nve_final()
+            t4 = clock()
+            T["modify"] += t4 - t3
             if thermo:
                 out.append(self._thermo_row(rows))
+                T["output"] += clock() - t4
         self.thermo_rows.extend(out)
         return out
 
     def stats(self):
         """Atoms held per rank: owned and ghost."""
-        return {r: dict(owned=int((~s.ghost).sum()), ghost=int(s.ghost.sum()))
+        return {r: dict(owned=int(len(s.gid) - s.nghost), ghost=int(s.nghost))
                 for r, s in self.st.items()}

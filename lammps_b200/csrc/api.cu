@@ -61,6 +61,16 @@ void invalidate_graphs(b200_ctx *c) {
   c->graph_valid = false;
 }
 
+// true for device (or managed) memory, false for host memory of any kind
+bool is_device_ptr(const void *p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
 // The context's transfer staging: `parts` byte counts laid out one after
 // another (256-byte aligned) in one device buffer that only grows.  Growing
 // synchronizes the stream first, since queued copies may still use it.
@@ -85,14 +95,19 @@ int xfer_parts(b200_ctx *c, int nparts, const size_t *bytes, char **ptrs) {
 
 // ---- kernels local to the ABI ------------------------------------------------
 
-__global__ void k_upload(int n, int stride, const double *__restrict__ x,
+__global__ void k_upload(int n, int stride, int ntypes, const double *__restrict__ x,
                          const double *__restrict__ v, const int *__restrict__ type,
                          double4 *__restrict__ x4, double *__restrict__ vd,
                          int *__restrict__ orig, int *__restrict__ image,
-                         int *__restrict__ cell) {
+                         int *__restrict__ cell, int *__restrict__ status) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  x4[i] = make_double4(x[3 * i], x[3 * i + 1], x[3 * i + 2], (double)type[i]);
+  int t = type[i];
+  if (t < 1 || t > ntypes) {  // recorded for the host (one offending index), kept in range
+    atomicCAS(&status[ST_BADTYPE], 0, i + 1);
+    t = 1;
+  }
+  x4[i] = make_double4(x[3 * i], x[3 * i + 1], x[3 * i + 2], (double)t);
   vd[i] = v ? v[3 * i] : 0.0;
   vd[stride + i] = v ? v[3 * i + 1] : 0.0;
   vd[2 * stride + i] = v ? v[3 * i + 2] : 0.0;
@@ -932,14 +947,22 @@ int b200_upload_atoms(b200_ctx *c, int n, const double *x, const double *v, cons
   if (!c || n < 1 || !x || !type) return set_err(c, B200_ERR_ARG, "Illegal atoms");
   if (n > MD_MAX_ATOMS) return set_err(c, B200_ERR_ARG, "too many atoms (%d > %d)", n, MD_MAX_ATOMS);
   if (c->ntypes < 1) return set_err(c, B200_ERR_STATE, "set masses or a pair style before atoms");
-  for (int i = 0; i < n; i++)
-    if (type[i] < 1 || type[i] > c->ntypes)
-      return set_err(c, B200_ERR_ARG, "Invalid atom type %d of atom %d", type[i], i);
   CK(cudaSetDevice(c->device));
+  // host arrays are checked here, device arrays by the upload kernel
+  const bool dev_type = is_device_ptr(type);
+  if (!dev_type)
+    for (int i = 0; i < n; i++)
+      if (type[i] < 1 || type[i] > c->ntypes)
+        return set_err(c, B200_ERR_ARG, "Invalid atom type %d of atom %d", type[i], i);
   // step graphs bake the atom count and the buffer addresses
   if (n != c->n || n > c->nalloc) invalidate_graphs(c);
   if (n > c->nalloc) {
-    const int stride = (n + 31) & ~31;
+    // a count that grows again (a decomposed box's owned + ghost atoms
+    // between rebuilds) gets 1/16 headroom, so it does not reallocate at
+    // every small growth
+    long long cap = c->nalloc > 0 ? (long long)n + n / 16 : n;
+    if (cap > MD_MAX_ATOMS) cap = MD_MAX_ATOMS;
+    const int stride = (int)((cap + 31) & ~31LL);
     CK(dalloc(&c->x4, stride));
     CK(dalloc(&c->x4b, stride));
     CK(dalloc(&c->v, 3 * (size_t)stride));
@@ -965,7 +988,7 @@ int b200_upload_atoms(b200_ctx *c, int n, const double *x, const double *v, cons
     // 128 threads per block)
     c->partial_blocks = stride / 4 + 64;
     CK(dalloc(&c->partial, (size_t)c->partial_blocks * 8));
-    c->nalloc = n;
+    c->nalloc = (int)cap;
     c->stride = stride;
     c->nlist_alloc = 0;
     dfree(c->nlist);
@@ -979,15 +1002,25 @@ int b200_upload_atoms(b200_ctx *c, int n, const double *x, const double *v, cons
   if (rc) return rc;
   double *dx = reinterpret_cast<double *>(st[0]), *dv = reinterpret_cast<double *>(st[1]);
   int *dt = reinterpret_cast<int *>(st[2]);
-  CK(cudaMemcpyAsync(dx, x, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  if (v) CK(cudaMemcpyAsync(dv, v, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  CK(cudaMemcpyAsync(dt, type, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, c->stream));
-  k_upload<<<md_blocks(n, 256), 256, 0, c->stream>>>(n, c->stride, dx, dv, dt, c->x4, c->v,
-                                                     c->orig, c->image, c->cell);
+  // host or device sources (unified addressing)
+  CK(cudaMemcpyAsync(dx, x, 3 * (size_t)n * sizeof(double), cudaMemcpyDefault, c->stream));
+  if (v) CK(cudaMemcpyAsync(dv, v, 3 * (size_t)n * sizeof(double), cudaMemcpyDefault, c->stream));
+  CK(cudaMemcpyAsync(dt, type, (size_t)n * sizeof(int), cudaMemcpyDefault, c->stream));
+  CK(cudaMemsetAsync(c->status + ST_BADTYPE, 0, sizeof(int), c->stream));
+  k_upload<<<md_blocks(n, 256), 256, 0, c->stream>>>(n, c->stride, c->ntypes, dx, dv, dt, c->x4,
+                                                     c->v, c->orig, c->image, c->cell, c->status);
   c->launches++;
   CK(cudaGetLastError());
   CK(md_where(c));
   c->ghosts_on = false;  // a new atom set: the caller marks its ghosts again
+  if (dev_type) {
+    int rc2 = read_status(c);
+    if (rc2) return rc2;
+    if (c->status_host[ST_BADTYPE]) {
+      c->have_atoms = false;
+      return set_err(c, B200_ERR_ARG, "Invalid atom type of atom %d", c->status_host[ST_BADTYPE] - 1);
+    }
+  }
   CK(cudaStreamSynchronize(c->stream));
   c->have_atoms = true;
   c->sorted_once = false;
@@ -1013,10 +1046,11 @@ int b200_download_atoms(b200_ctx *c, double *x, double *v, double *f, int *image
                                                      c->image, dx, dv, df, di);
   c->launches++;
   CK(cudaGetLastError());
-  if (x) CK(cudaMemcpyAsync(x, dx, 3 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  if (v) CK(cudaMemcpyAsync(v, dv, 3 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  if (f) CK(cudaMemcpyAsync(f, df, 3 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  if (image) CK(cudaMemcpyAsync(image, di, 3 * (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  // host or device destinations (unified addressing)
+  if (x) CK(cudaMemcpyAsync(x, dx, 3 * (size_t)n * sizeof(double), cudaMemcpyDefault, c->stream));
+  if (v) CK(cudaMemcpyAsync(v, dv, 3 * (size_t)n * sizeof(double), cudaMemcpyDefault, c->stream));
+  if (f) CK(cudaMemcpyAsync(f, df, 3 * (size_t)n * sizeof(double), cudaMemcpyDefault, c->stream));
+  if (image) CK(cudaMemcpyAsync(image, di, 3 * (size_t)n * sizeof(int), cudaMemcpyDefault, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return B200_OK;
 }
@@ -1069,8 +1103,8 @@ int b200_pair_compute(b200_ctx *c, int eflag, int vflag, double *eng, double vir
   if (rc) return rc;
   double h[8];
   if (ev) CK(cudaMemcpyAsync(h, c->ev, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  if (de) CK(cudaMemcpyAsync(eatom, de, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  if (dv) CK(cudaMemcpyAsync(vatom, dv, 6 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (de) CK(cudaMemcpyAsync(eatom, de, (size_t)n * sizeof(double), cudaMemcpyDefault, c->stream));
+  if (dv) CK(cudaMemcpyAsync(vatom, dv, 6 * (size_t)n * sizeof(double), cudaMemcpyDefault, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   if (ev) {
     if (eg && eng) *eng = h[0];
@@ -1512,8 +1546,7 @@ int b200_set_ghosts(b200_ctx *c, const int *ghost) {
     c->ghosts_on = false;
     return B200_OK;
   }
-  CK(cudaMemcpyAsync(c->ghost, ghost, (size_t)c->n * sizeof(int), cudaMemcpyHostToDevice,
-                     c->stream));
+  CK(cudaMemcpyAsync(c->ghost, ghost, (size_t)c->n * sizeof(int), cudaMemcpyDefault, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->ghosts_on = true;
   return B200_OK;

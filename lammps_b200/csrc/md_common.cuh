@@ -41,6 +41,7 @@ enum {
   ST_FORCE_BUILD = 11,  // rebuild on the next step regardless of the schedule
   ST_MAXSTAGE = 12,     // most atoms staged by one neighbor-builder tile since setup
   ST_HALO_BAD = 13,     // a halo pack/unpack index was outside [0, n)
+  ST_BADTYPE = 14,      // 1 + index of an uploaded atom with a type outside [1, ntypes]
   ST_COUNT = 16
 };
 

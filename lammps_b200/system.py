@@ -18,6 +18,11 @@ from .inputs import UNITS, velocity_create
 from .pair import PairEAM, PairLJCut
 
 
+def _torch():
+    import torch
+    return torch
+
+
 class System:
     def __init__(self, units: str = "lj", precision: str = "fp64", device: int = 0):
         if units not in UNITS:
@@ -159,11 +164,57 @@ class System:
     # ---- spatial decomposition (lammps_b200.brick) -----------------------
     def set_ghosts(self, ghost):
         """Mark ghost atoms (caller order; None clears): not integrated, not
-        distance-checked, positions set by halo_unpack."""
-        g = None if ghost is None else np.ascontiguousarray(ghost, dtype=np.int32)
-        if g is not None and g.shape != (self.n,):
+        distance-checked, positions set by halo_unpack.  A numpy array or an
+        int32 torch tensor (host or device)."""
+        if ghost is None:
+            self._ck(self._L.b200_set_ghosts(self._h, None))
+            return
+        if hasattr(ghost, "data_ptr"):
+            g = ghost.contiguous()
+            if g.dtype.itemsize != 4 or tuple(g.shape) != (self.n,):
+                raise ValueError(f"set_ghosts: need {self.n} int32 flags")
+            self._ck(self._L.b200_set_ghosts(self._h, _abi.tiptr(g)))
+            return
+        g = np.ascontiguousarray(ghost, dtype=np.int32)
+        if g.shape != (self.n,):
             raise ValueError(f"set_ghosts: need {self.n} flags")
         self._ck(self._L.b200_set_ghosts(self._h, _abi.iptr(g)))
+
+    # device-tensor forms of set_atoms / download / compute (torch tensors on
+    # this context's device; no host copy)
+    def set_atoms_dev(self, x, type_, v=None):
+        """x (n, 3) float64, type_ (n,) int32, v (n, 3) float64 or None."""
+        x = x.contiguous()
+        t = type_.contiguous()
+        vv = None if v is None else v.contiguous()
+        n = int(x.shape[0])
+        if x.dtype != _torch().float64 or t.dtype != _torch().int32 or tuple(t.shape) != (n,):
+            raise ValueError("set_atoms_dev: x float64 (n, 3), type int32 (n,)")
+        self.n = n
+        self.type = None
+        self._ck(self._L.b200_upload_atoms(self._h, n, _abi.tdptr(x), _abi.tdptr(vv),
+                                           _abi.tiptr(t), None))
+
+    def download_dev(self, f=False):
+        torch = _torch()
+        n, dev = self.n, self.device
+        out = dict(x=torch.empty((n, 3), dtype=torch.float64, device=dev),
+                   v=torch.empty((n, 3), dtype=torch.float64, device=dev),
+                   image=torch.empty((n, 3), dtype=torch.int32, device=dev))
+        if f:
+            out["f"] = torch.empty((n, 3), dtype=torch.float64, device=dev)
+        self._ck(self._L.b200_download_atoms(self._h, _abi.tdptr(out["x"]), _abi.tdptr(out["v"]),
+                                             _abi.tdptr(out.get("f")), _abi.tiptr(out["image"])))
+        return out
+
+    def compute_dev(self):
+        """Forces with per-atom energy (n,) and virial (n, 6) as device tensors."""
+        torch = _torch()
+        ea = torch.empty(self.n, dtype=torch.float64, device=self.device)
+        va = torch.empty((self.n, 6), dtype=torch.float64, device=self.device)
+        self._ck(self._L.b200_pair_compute(self._h, 2, 4, None, None, _abi.tdptr(ea),
+                                           _abi.tdptr(va)))
+        return dict(eatom=ea, vatom=va)
 
     def neigh_check(self):
         """The local half of Neighbor::check_distance since the last call."""

@@ -48,7 +48,19 @@ class NumpyLJ:
         self.ghost = np.zeros(len(self.x), dtype=bool)
 
     def set_ghosts(self, g):
+        if g is not None and hasattr(g, "numpy"):
+            g = g.numpy()
         self.ghost = np.zeros(len(self.x), dtype=bool) if g is None else np.asarray(g) != 0
+
+    def set_atoms_dev(self, x, type_, v=None):
+        self.set_atoms(x.numpy(), type_.numpy(), np.zeros(tuple(x.shape)) if v is None else v.numpy())
+
+    def download_dev(self):
+        return {k: torch.from_numpy(a) for k, a in self.download().items() if k != "f"}
+
+    def compute_dev(self):
+        o = self.compute(1, 1, per_atom=True)
+        return dict(eatom=torch.from_numpy(o["eatom"]), vatom=torch.from_numpy(o["vatom"]))
 
     def neigh_build(self):
         self.xhold = self.x.copy()

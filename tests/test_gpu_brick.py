@@ -6,13 +6,14 @@ so a decomposed run must reproduce the single-box trajectory bit for bit --
 for lj/cut and EAM, FP64 and mixed, through rebuilds (check yes) with
 exchange and borders, and the per-step halo pack / unpack in between."""
 import os
+import socket
 
 import numpy as np
 import pytest
 
 from lammps_b200 import PairEAM, PairLJCut, System, inputs
 from lammps_b200._abi import B200Error
-from lammps_b200.brick import BrickRun, LocalComm
+from lammps_b200.brick import BrickRun, DistComm, LocalComm
 
 pytestmark = pytest.mark.gpu
 
@@ -129,3 +130,46 @@ def test_halo_index_errors_are_reported():
     s.setup()
     with pytest.raises(B200Error, match="ghost"):
         s.run(1)
+
+
+def _nccl_worker(port, out):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", rank=0, world_size=1)
+    try:
+        make, x, v, steps = _lj("fp64")
+        b = BrickRun(DistComm(), {0: make()}, (1, 1, 1))
+        b.set_atoms(x, None, v)
+        b.setup()
+        rows = b.run(steps // 4, thermo_every=steps // 8)
+        g = b.gather()
+        np.savez(out, x=g["x"], v=g["v"], ncalls=b.ncalls, temp=[r["Temp"] for r in rows])
+    finally:
+        dist.destroy_process_group()
+
+
+def test_nccl_transport_one_rank(tmp_path):
+    """DistComm over NCCL (one rank: the all-to-alls of the exchange and
+    borders, the MAX and SUM all-reduces) gives the in-process result."""
+    import torch.multiprocessing as mp
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    out = str(tmp_path / "nccl.npz")
+    p = mp.get_context("spawn").Process(target=_nccl_worker, args=(port, out))
+    p.start()
+    p.join(timeout=300)
+    assert p.exitcode == 0, p.exitcode
+    make, x, v, steps = _lj("fp64")
+    b = BrickRun(LocalComm(1), {0: make()}, (1, 1, 1))
+    b.set_atoms(x, None, v)
+    b.setup()
+    rows = b.run(steps // 4, thermo_every=steps // 8)
+    ref = b.gather()
+    res = np.load(out)
+    assert int(res["ncalls"]) == b.ncalls
+    assert np.array_equal(res["x"], ref["x"])
+    assert np.array_equal(res["v"], ref["v"])
+    assert np.allclose(res["temp"], [r["Temp"] for r in rows], rtol=1e-13)
