@@ -7,6 +7,7 @@ import numpy as np
 import pytest
 
 from lammps_b200 import PairLJCut, System, inputs
+from lammps_b200._abi import B200Error
 
 pytestmark = pytest.mark.gpu
 
@@ -63,4 +64,28 @@ def test_download_into_page_locked_buffers():
         assert np.array_equal(out[k], ref[k]), k
     with pytest.raises(ValueError):
         s.download({"x": np.zeros((n, 2)), "v": out["v"], "f": out["f"], "image": out["image"]})
+    s.close()
+
+
+def test_device_pointer_upload_download():
+    """Upload from and download into device memory (unified addressing): same
+    atoms as the host path; an out-of-range type in a device array is found by
+    the upload kernel and reported with its index."""
+    s = _system()
+    rng = np.random.default_rng(3)
+    n = 3000
+    x = rng.uniform(0.0, 20.0, size=(n, 3))
+    v = rng.normal(size=(n, 3))
+    xt = torch.from_numpy(x).cuda()
+    vt = torch.from_numpy(v).cuda()
+    tt = torch.ones(n, dtype=torch.int32, device="cuda")
+    s.set_atoms_dev(xt, tt, vt)
+    d = s.download_dev()
+    assert torch.equal(d["x"], xt) and torch.equal(d["v"], vt)
+    assert not d["image"].any()
+    h = s.download()
+    assert np.array_equal(h["x"], x) and np.array_equal(h["v"], v)
+    tt[1234] = 7
+    with pytest.raises(B200Error, match="atom 1234"):
+        s.set_atoms_dev(xt, tt, vt)
     s.close()
