@@ -135,3 +135,17 @@ def test_two_gloo_ranks_match_single_box(tmp_path):
             assert np.array_equal(res[k], ref[k]), k
         assert np.allclose(res["temp"], [q["Temp"] for q in rows1], rtol=1e-12)
         assert np.allclose(res["epair"], [q["E_pair"] for q in rows1], rtol=1e-12)
+
+
+def test_merge_by_gid():
+    from lammps_b200.brick import _merge_by_gid, _W, _GID
+    rng = np.random.default_rng(9)
+    gid = rng.permutation(1000)
+    for na, nb in ((600, 400), (0, 1000), (1000, 0), (999, 1)):
+        a = np.zeros((na, _W)); a[:, _GID] = np.sort(gid[:na]); a[:, 5] = rng.normal(size=na)
+        b = np.zeros((nb, _W)); b[:, _GID] = gid[na:na + nb]; b[:, 5] = rng.normal(size=nb)
+        out, pa, pb = _merge_by_gid(torch.from_numpy(a), torch.from_numpy(b))
+        out = out.numpy()
+        assert np.array_equal(out[:, _GID], np.arange(na + nb) if na + nb == 1000 else np.sort(gid[:na + nb]))
+        assert np.array_equal(out[pa.numpy()], a)
+        assert np.array_equal(out[pb.numpy()], b)
