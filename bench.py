@@ -423,7 +423,7 @@ def replica_bench(prec, batch, torch, steps=1000, lat_steps=200):
     return out
 
 
-def brick_bench(torch, x, v, hi, steps=40, warm=20):
+def brick_bench(torch, x, v, hi, steps=40, warm=40):
     """One box split into bricks (lammps_b200.brick) on this one GPU: the
     per-call step of one brick, and of 2 bricks (2 x 1 x 1) as separate
     contexts whose halo exchange is a device copy.  The bricks of a step run
