@@ -118,6 +118,14 @@ int b200_upload_atoms(b200_ctx *ctx, int n, const double *x, const double *v, co
    order (NULL pointers are skipped; image is 3 ints per atom). */
 int b200_download_atoms(b200_ctx *ctx, double *x, double *v, double *f, int *image);
 int b200_natoms(const b200_ctx *ctx);
+/* New positions x[3n] (caller order, host or device memory) for the atoms of
+   the last upload, keeping their cells and the neighbor list of the last
+   build: the per-step position refresh of a Pair::compute between
+   reneighborings, when the host integrates and Neighbor::decide
+   (src/neighbor.cpp:1294-1320) has not asked for a rebuild.  Like the
+   reference, forces use the list as built; the caller rebuilds (upload +
+   b200_neigh_build) on its reneighbor steps. */
+int b200_update_positions(b200_ctx *ctx, const double *x);
 
 /* ---- per-step entry points ------------------------------------------------- */
 
@@ -229,7 +237,9 @@ int b200_neigh_check(b200_ctx *ctx, int *moved);
    halves.  idx[m] are caller indices and buf[3m] the coordinates, both
    DEVICE pointers on the context's device; the calls are ordered on the
    context's stream and return after it completes.  pack: buf[3i..3i+2] = x
-   of atom idx[i].  unpack: x of atom idx[i] = buf[3i..3i+2]. */
+   of atom idx[i].  unpack: x of atom idx[i] = buf[3i..3i+2].  An index
+   outside [0, n) -- or, when ghosts are marked (b200_set_ghosts), an index
+   of an owned atom -- is not written and the call returns B200_ERR_ARG. */
 int b200_halo_pack(b200_ctx *ctx, int m, const int *idx, double *buf);
 int b200_halo_unpack(b200_ctx *ctx, int m, const int *idx, const double *buf);
 
@@ -286,7 +296,9 @@ int b200_adj_backward(b200_ctx *ctx, const double *lj1, const double *lj2, const
    graph by stream capture (where cudaMalloc is not allowed) or a host whose
    device memory belongs to another allocator.  No context is needed; v
    (3n doubles, xyz interleaved), type (n ints, each in 1..ntypes), mass
-   (ntypes+1 doubles) and out are device pointers, and the call is ordered
+   (ntypes+1 doubles) and out are device pointers (an atom whose type lies
+   outside 1..ntypes is not looked up in mass; it makes out[0] NaN, which the
+   caller sees when it reads the result), and the call is ordered
    on `stream` (a cudaStream_t; NULL = the legacy default stream).  It
    allocates nothing: its reduction scratch is a fixed static device array
    (1184 block partials and a counter, about 9.5 KB per device) whose address

@@ -39,6 +39,7 @@ SIGNATURES = {
     "b200_upload_atoms": (C.c_int, [_vp, C.c_int, _dp, _dp, _ip, _ip]),
     "b200_download_atoms": (C.c_int, [_vp, _dp, _dp, _dp, _ip]),
     "b200_natoms": (C.c_int, [_vp]),
+    "b200_update_positions": (C.c_int, [_vp, _dp]),
     "b200_neigh_build": (C.c_int, [_vp]),
     "b200_pair_compute": (C.c_int, [_vp, C.c_int, C.c_int, _dp, _dp, _dp, _dp]),
     "b200_nve_initial": (C.c_int, [_vp, C.c_double, C.c_double]),

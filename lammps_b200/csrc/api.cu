@@ -1029,6 +1029,25 @@ int b200_upload_atoms(b200_ctx *c, int n, const double *x, const double *v, cons
 
 int b200_natoms(const b200_ctx *c) { return c ? c->n : 0; }
 
+int b200_update_positions(b200_ctx *c, const double *x) {
+  if (!c || !x) return B200_ERR_ARG;
+  if (!c->sorted_once) return set_err(c, B200_ERR_STATE, "neighbor list not built");
+  CK(cudaSetDevice(c->device));
+  const size_t bytes = 3 * (size_t)c->n * sizeof(double);
+  const double *dx = x;
+  if (!is_device_ptr(x)) {
+    char *st[1];
+    const size_t sb[1] = {bytes};
+    int rc = xfer_parts(c, 1, sb, st);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(st[0], x, bytes, cudaMemcpyHostToDevice, c->stream));
+    dx = reinterpret_cast<const double *>(st[0]);
+  }
+  CK(md_set_positions(c, dx));
+  CK(cudaStreamSynchronize(c->stream));
+  return B200_OK;
+}
+
 int b200_download_atoms(b200_ctx *c, double *x, double *v, double *f, int *image) {
   if (!c) return B200_ERR_ARG;
   if (!c->have_atoms) return set_err(c, B200_ERR_STATE, "no atoms uploaded");
@@ -1576,6 +1595,8 @@ static int halo_call(b200_ctx *c, int m, const int *idx, const double *buf, bool
     CK(md_halo_unpack(c, m, idx, buf));
   int rc = read_status(c);
   if (rc) return rc;
+  if (c->status_host[ST_HALO_BAD] == 2)
+    return set_err(c, B200_ERR_ARG, "halo unpack: an index names an owned atom, not a ghost");
   if (c->status_host[ST_HALO_BAD])
     return set_err(c, B200_ERR_ARG, "halo %s: an atom index is outside [0, %d)",
                    pack ? "pack" : "unpack", c->n);

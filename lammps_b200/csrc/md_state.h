@@ -196,6 +196,8 @@ cudaError_t md_where(b200_ctx *c);
 cudaError_t md_halo_pack(b200_ctx *c, int m, const int *idx, double *buf);
 // x of caller atom idx[i] = buf[3i..3i+2] (and its cell-relative FP32 copy)
 cudaError_t md_halo_unpack(b200_ctx *c, int m, const int *idx, const double *buf);
+// x of every atom from x[3n] in caller order (device), keeping cells and list
+cudaError_t md_set_positions(b200_ctx *c, const double *x);
 // ---- pair kernels (pair_lj.cu, pair_eam.cu) --------------------------------
 cudaError_t md_lj_compute(b200_ctx *c, bool ev, bool atom_ev, double *eatom, double *vatom);
 // `mid`, when given, is recorded between the density and the force kernel

@@ -48,16 +48,20 @@ cudaError_t scratch_address(int device, NoAllocScratch **out) {
 }
 
 // sum over atoms of (vx^2 + vy^2 + vz^2) * mass[type] (the term of
-// ComputeTemp::compute_scalar); grid-stride, deterministic two-level sum
+// ComputeTemp::compute_scalar); grid-stride, deterministic two-level sum.
+// An atom whose type lies outside 1..ntypes never indexes mass[]: it adds a
+// NaN instead, so the result the caller reads is NaN.
 __global__ void __launch_bounds__(kNoAllocThreads)
     k_kinetic_noalloc(int n, const double *__restrict__ v, const int *__restrict__ type,
-                      const double *__restrict__ mass, NoAllocScratch *scratch,
+                      const double *__restrict__ mass, int ntypes, NoAllocScratch *scratch,
                       double *__restrict__ out) {
   __shared__ double red[kNoAllocThreads / 32];
   double acc[1] = {0.0};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const double vx = v[3 * i], vy = v[3 * i + 1], vz = v[3 * i + 2];
-    acc[0] += (vx * vx + vy * vy + vz * vz) * mass[type[i]];
+    const int t = type[i];
+    acc[0] += (t >= 1 && t <= ntypes) ? (vx * vx + vy * vy + vz * vz) * mass[t]
+                                      : __longlong_as_double(0x7ff8000000000000LL);
   }
   block_partials_finish<1>(acc, red, scratch->partial, &scratch->counter, out, false);
 }
@@ -81,6 +85,7 @@ extern "C" int b200_kinetic_sum_noalloc(int n, const double *v, const int *type,
     return B200_ERR_CUDA;
   int blocks = (n + kNoAllocThreads - 1) / kNoAllocThreads;
   if (blocks > kNoAllocBlocks) blocks = kNoAllocBlocks;
-  k_kinetic_noalloc<<<blocks, kNoAllocThreads, 0, s>>>(n, v, type, mass, scratch, out);
+  k_kinetic_noalloc<<<blocks, kNoAllocThreads, 0, s>>>(n, v, type, mass, ntypes, scratch,
+                                                        out);
   return cudaGetLastError() == cudaSuccess ? B200_OK : B200_ERR_CUDA;
 }

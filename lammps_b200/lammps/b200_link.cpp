@@ -48,6 +48,8 @@ B200Link::B200Link(LAMMPS *lmp) : Pointers(lmp) {
   ctx_precision = -1;
   tables_dirty = 1;
   refs = 0;
+  built = 0;
+  nbuilt = -1;
   fbuf = NULL;
   ibuf = NULL;
   nbuf = 0;
@@ -101,7 +103,18 @@ b200_ctx *B200Link::context(int precision) {
   }
   ctx_precision = precision;
   tables_dirty = 1;
+  built = 0;
+  char msg[128];
+  snprintf(msg, sizeof(msg), "B200: libb200md context on CUDA device %d, %s precision",
+           dev ? atoi(dev) : 0, precision == B200_PREC_MIXED ? "mixed" : "fp64");
+  banner(msg);
   return ctx;
+}
+
+void B200Link::banner(const char *text) {
+  if (comm->me != 0) return;
+  if (screen) fprintf(screen, "%s\n", text);
+  if (logfile) fprintf(logfile, "%s\n", text);
 }
 
 void B200Link::check(int status, const char *where) {
@@ -145,12 +158,26 @@ void B200Link::upload_atoms(int with_velocities) {
   check(b200_upload_atoms(ctx, n, x, v, atom->type, ibuf), "upload_atoms");
 }
 
-void B200Link::pair_compute(Pair *pair, int eflag, int vflag) {
-  check(b200_neigh_build(ctx), "neigh_build");
-  long long total = 0;
-  int ncalls = 0, ndanger = 0, maxneigh = 0, cap = 0;
-  check(b200_neigh_stats(ctx, &total, &ncalls, &ndanger, &maxneigh, &cap), "neigh_stats");
-  if (maxneigh > neighbor->oneatom) check(B200_ERR_NEIGH_OVERFLOW, "neigh_build");
+void B200Link::pair_compute(Pair *pair, B200PairTables *tables, int eflag, int vflag) {
+  const int n = atom->nlocal;
+  // LAMMPS reorders and wraps atoms only when it reneighbors (pbc, exchange,
+  // Atom::sort, borders in Verlet::run, src/verlet.cpp:250-270); between
+  // those steps the atom set and order are fixed and the list stays valid
+  const int rebuild = !ctx || ctx_precision != tables->b200_precision() || tables_dirty ||
+                      !built || neighbor->ago == 0 || n != nbuilt;
+  if (rebuild) {
+    sync_settings(tables);
+    upload_atoms(0);
+    check(b200_neigh_build(ctx), "neigh_build");
+    built = 1;
+    nbuilt = n;
+    long long total = 0;
+    int ncalls = 0, ndanger = 0, maxneigh = 0, cap = 0;
+    check(b200_neigh_stats(ctx, &total, &ncalls, &ndanger, &maxneigh, &cap), "neigh_stats");
+    if (maxneigh > neighbor->oneatom) check(B200_ERR_NEIGH_OVERFLOW, "neigh_build");
+  } else if (n > 0) {
+    check(b200_update_positions(ctx, &atom->x[0][0]), "update_positions");
+  }
 
   double eng = 0.0, vir[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   double *eatom = (pair->eflag_atom && pair->eatom) ? pair->eatom : NULL;
@@ -158,7 +185,6 @@ void B200Link::pair_compute(Pair *pair, int eflag, int vflag) {
   check(b200_pair_compute(ctx, eflag, vflag, pair->eflag_global ? &eng : NULL,
                           pair->vflag_global ? vir : NULL, eatom, vatom),
         "pair_compute");
-  const int n = atom->nlocal;
   grow(n);
   check(b200_download_atoms(ctx, NULL, NULL, fbuf, NULL), "download forces");
   double **f = atom->f;

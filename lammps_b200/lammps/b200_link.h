@@ -6,11 +6,14 @@
    device context (atoms, cell-sorted neighbor list and potential tables on
    the GPU).  Two ways of driving it:
 
-   - per call (any run style): Pair::compute uploads the owned atoms, builds
-     the list on the device, evaluates forces/energy/virial and copies the
-     forces back into atom->f -- the contract of Pair::compute(eflag,vflag)
-     in src/pair.h:135 with the GPU package's device-neighbor mode as the
-     model (src/GPU/pair_lj_cut_gpu.cpp:97-140);
+   - per call (any run style): Pair::compute evaluates forces/energy/virial
+     on the device and copies the forces back into atom->f -- the contract
+     of Pair::compute(eflag,vflag) in src/pair.h:135 with the GPU package's
+     device-neighbor mode as the model (src/GPU/pair_lj_cut_gpu.cpp:97-140).
+     It follows LAMMPS's own reneighbor schedule: on a step where Neighbor
+     has just rebuilt (neighbor->ago == 0, after pbc, exchange, sort and
+     borders) it uploads the owned atoms and builds the device list;
+     on the other steps it only refreshes their positions;
    - resident (run_style verlet/b200 with fix nve/b200): the whole run
      advances on the device through b200_run and host arrays are refreshed
      only on output steps.
@@ -57,11 +60,15 @@ class B200Link : protected Pointers {
   /* map a B200_* status to error->all with the library's message */
   void check(int status, const char *where);
 
-  /* per-call mode: box, neighbor settings and tables, then owned atoms */
+  /* box, neighbor settings and tables, then owned atoms */
   void sync_settings(B200PairTables *tables);
   void upload_atoms(int with_velocities);
-  /* per-call Pair::compute: build + forces, energy and virial */
-  void pair_compute(class Pair *pair, int eflag, int vflag);
+  /* per-call Pair::compute: (re)build on reneighbor steps, else refresh
+     positions; then forces, energy and virial */
+  void pair_compute(class Pair *pair, B200PairTables *tables, int eflag, int vflag);
+  /* one line on screen and in the log file (proc 0), as the GPU package
+     reports its acceleration at init */
+  void banner(const char *text);
 
   /* resident mode: host x, v, f and image flags from the device */
   void download_state();
@@ -70,6 +77,8 @@ class B200Link : protected Pointers {
   int ctx_precision;
   int tables_dirty;   // tables must be re-uploaded before the next compute
   int refs;           // styles holding this link
+  int built;          // the device list belongs to the current atom set
+  int nbuilt;         // nlocal of that atom set
 
  private:
   double *fbuf;       // nlocal*3 forces in caller order

@@ -3,6 +3,7 @@
    evaluated by libb200md.
 ------------------------------------------------------------------------- */
 
+#include <cstdio>
 #include <cstring>
 
 #include "b200md.h"
@@ -43,6 +44,10 @@ void PairEAMB200::init_style() {
   file2array();
   array2spline();
   link->tables_dirty = 1;
+  char msg[160];
+  snprintf(msg, sizeof(msg), "B200: pair_style %s (%s), device neighbor list", b200_style(),
+           b200_class());
+  link->banner(msg);
 }
 
 double PairEAMB200::init_one(int i, int j) {
@@ -61,7 +66,5 @@ int PairEAMB200::b200_upload_tables(b200_ctx *ctx) {
 void PairEAMB200::compute(int eflag, int vflag) {
   if (eflag || vflag) ev_setup(eflag, vflag);
   else evflag = vflag_fdotr = 0;
-  link->sync_settings(this);
-  link->upload_atoms(0);
-  link->pair_compute(this, eflag, vflag);
+  link->pair_compute(this, this, eflag, vflag);
 }

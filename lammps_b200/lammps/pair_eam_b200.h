@@ -40,6 +40,9 @@ class PairEAMB200 : virtual public PairEAM, public B200PairTables {
   double init_one(int, int);
   int b200_upload_tables(b200_ctx *);
   int b200_precision() const { return precision; }
+  // the style name and class for the init banner
+  virtual const char *b200_style() const { return "eam/b200"; }
+  virtual const char *b200_class() const { return "PairEAMB200"; }
 
  protected:
   int precision;
@@ -50,12 +53,16 @@ class PairEAMAlloyB200 : public PairEAMB200, public PairEAMAlloy {
  public:
   PairEAMAlloyB200(class LAMMPS *);
   virtual ~PairEAMAlloyB200() {}
+  const char *b200_style() const { return "eam/alloy/b200"; }
+  const char *b200_class() const { return "PairEAMAlloyB200"; }
 };
 
 class PairEAMFSB200 : public PairEAMB200, public PairEAMFS {
  public:
   PairEAMFSB200(class LAMMPS *);
   virtual ~PairEAMFSB200() {}
+  const char *b200_style() const { return "eam/fs/b200"; }
+  const char *b200_class() const { return "PairEAMFSB200"; }
 };
 
 }

@@ -12,6 +12,7 @@
 #include "error.h"
 #include "force.h"
 #include "neighbor.h"
+#include "update.h"
 
 using namespace LAMMPS_NS;
 
@@ -39,7 +40,13 @@ void PairLJCutB200::settings(int narg, char **arg) {
    device-neighbor mode, src/GPU/pair_lj_cut_gpu.cpp:161-165) */
 void PairLJCutB200::init_style() {
   link->check_supported("pair_style lj/cut/b200");
+  // PairLJCut::init_style (src/pair_lj_cut.cpp:519-526) is where cut_respa
+  // is set, and PairLJCut::init_one reads it; the device has no rRESPA levels
+  if (strstr(update->integrate_style, "respa"))
+    error->all(FLERR, "pair_style lj/cut/b200 does not support run_style respa");
+  cut_respa = NULL;
   link->tables_dirty = 1;
+  link->banner("B200: pair_style lj/cut/b200 (PairLJCutB200), device neighbor list");
 }
 
 double PairLJCutB200::init_one(int i, int j) {
@@ -70,7 +77,5 @@ int PairLJCutB200::b200_upload_tables(b200_ctx *ctx) {
 void PairLJCutB200::compute(int eflag, int vflag) {
   if (eflag || vflag) ev_setup(eflag, vflag);
   else evflag = vflag_fdotr = 0;
-  link->sync_settings(this);
-  link->upload_atoms(0);
-  link->pair_compute(this, eflag, vflag);
+  link->pair_compute(this, this, eflag, vflag);
 }

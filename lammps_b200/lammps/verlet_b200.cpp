@@ -43,7 +43,14 @@ void VerletB200::init() {
   if (modify->n_post_integrate || modify->n_pre_exchange || modify->n_pre_neighbor ||
       modify->n_pre_force || modify->n_post_force || modify->n_end_of_step)
     resident = 0;
-  if (resident) link->check_supported("run_style verlet/b200");
+  if (resident) {
+    link->check_supported("run_style verlet/b200");
+    link->banner("B200: run_style verlet/b200 (VerletB200), resident mode: the run advances "
+                 "on the device");
+  } else {
+    link->banner("B200: run_style verlet/b200 (VerletB200), per-call mode: Verlet::run with "
+                 "the /b200 pair style");
+  }
 }
 
 /* Verlet::setup (forces at the current step through the per-call pair

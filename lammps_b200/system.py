@@ -155,6 +155,14 @@ class System:
                                              _abi.dptr(out["f"]), _abi.iptr(out["image"])))
         return out
 
+    def update_positions(self, x):
+        """New positions (caller order) keeping the cells and the neighbor
+        list of the last build (a Pair::compute between reneighborings)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        if x.shape != (self.n, 3):
+            raise ValueError(f"update_positions: need ({self.n}, 3) positions")
+        self._ck(self._L.b200_update_positions(self._h, _abi.dptr(x)))
+
     def cutforce(self):
         """Largest force cutoff of the pair style (Pair::cutforce)."""
         if isinstance(self.pair, PairEAM):
@@ -173,6 +181,8 @@ class System:
             g = ghost.contiguous()
             if g.dtype.itemsize != 4 or tuple(g.shape) != (self.n,):
                 raise ValueError(f"set_ghosts: need {self.n} int32 flags")
+            if g.is_cuda:
+                self._torch_ready()
             self._ck(self._L.b200_set_ghosts(self._h, _abi.tiptr(g)))
             return
         g = np.ascontiguousarray(ghost, dtype=np.int32)
@@ -182,6 +192,18 @@ class System:
 
     # device-tensor forms of set_atoms / download / compute (torch tensors on
     # this context's device; no host copy)
+    def _torch_ready(self):
+        """Wait for the work queued on torch's current stream of this device.
+
+        The engine runs on its own non-blocking stream, which does not wait
+        for torch's stream: a tensor that torch kernels are still producing
+        (an input), or a block that torch's caching allocator has just handed
+        out while kernels queued earlier on torch's stream may still use it
+        (an output), must be settled before the engine touches it.  Every
+        engine call returns after its own stream has finished, so outputs are
+        complete when the call returns."""
+        _torch().cuda.current_stream(self.device).synchronize()
+
     def set_atoms_dev(self, x, type_, v=None):
         """x (n, 3) float64, type_ (n,) int32, v (n, 3) float64 or None."""
         x = x.contiguous()
@@ -192,6 +214,7 @@ class System:
             raise ValueError("set_atoms_dev: x float64 (n, 3), type int32 (n,)")
         self.n = n
         self.type = None
+        self._torch_ready()
         self._ck(self._L.b200_upload_atoms(self._h, n, _abi.tdptr(x), _abi.tdptr(vv),
                                            _abi.tiptr(t), None))
 
@@ -203,6 +226,7 @@ class System:
                    image=torch.empty((n, 3), dtype=torch.int32, device=dev))
         if f:
             out["f"] = torch.empty((n, 3), dtype=torch.float64, device=dev)
+        self._torch_ready()
         self._ck(self._L.b200_download_atoms(self._h, _abi.tdptr(out["x"]), _abi.tdptr(out["v"]),
                                              _abi.tdptr(out.get("f")), _abi.tiptr(out["image"])))
         return out
@@ -212,6 +236,7 @@ class System:
         torch = _torch()
         ea = torch.empty(self.n, dtype=torch.float64, device=self.device)
         va = torch.empty((self.n, 6), dtype=torch.float64, device=self.device)
+        self._torch_ready()
         self._ck(self._L.b200_pair_compute(self._h, 2, 4, None, None, _abi.tdptr(ea),
                                            _abi.tdptr(va)))
         return dict(eatom=ea, vatom=va)
@@ -238,11 +263,13 @@ class System:
     def halo_pack(self, idx, buf):
         """buf[i] = x of atom idx[i] (device tensors)."""
         m, pi, pb = self._dev_args(idx, buf)
+        self._torch_ready()
         self._ck(self._L.b200_halo_pack(self._h, m, pi, pb))
 
     def halo_unpack(self, idx, buf):
         """x of atom idx[i] = buf[i] (device tensors)."""
         m, pi, pb = self._dev_args(idx, buf)
+        self._torch_ready()
         self._ck(self._L.b200_halo_unpack(self._h, m, pi, pb))
 
     # ---- actions ---------------------------------------------------------

@@ -128,9 +128,15 @@ class OracleSim:
         self._L.orc_set_threads(self._s, threads)
         self.ntypes = 1
 
+    def close(self):
+        """Free the simulation now (it is freed on garbage collection otherwise)."""
+        if self._s:
+            self._L.orc_destroy(self._s)
+            self._s = None
+
     def __del__(self):
         try:
-            self._L.orc_destroy(self._s)
+            self.close()
         except Exception:
             pass
 

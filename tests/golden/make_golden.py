@@ -6,9 +6,10 @@ parameters (transcribed from the matching ``in.*`` script) and the printed
 thermo rows, ghost count, neighbor total and build counts.  Also copies the
 ``Cu_u3.eam`` funcfl table the EAM benchmark reads.
 
-Run from the repository root, with the reference checked out at REFERENCE:
+Run from the repository root, naming the reference checkout (the directory
+that holds bench/, examples/ and src/) as the argument or in LAMMPS_ROOT:
 
-    python tests/golden/make_golden.py [REFERENCE]
+    python tests/golden/make_golden.py REFERENCE
 """
 import json
 import os
@@ -16,7 +17,9 @@ import re
 import shutil
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("LAMMPS_ROOT")
+if not REF:
+    sys.exit("usage: make_golden.py REFERENCE  (or set LAMMPS_ROOT)")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 # Run parameters of each input script.  lattice "fcc" with rho* (lj units) or

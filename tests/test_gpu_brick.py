@@ -125,6 +125,19 @@ def test_halo_index_errors_are_reported():
     # the context stays usable
     s.halo_pack(idx[:1], buf[:1])
     assert buf[0].cpu().numpy().tolist() == list(x[0])
+    # with ghosts marked, unpack writes ghosts only: an owned atom's index is
+    # refused and its position is left as it was
+    g = np.zeros(len(x), np.int32)
+    g[len(x) // 2:] = 1
+    s.set_ghosts(g)
+    idx = torch.tensor([len(x) - 1, 3], dtype=torch.int32, device="cuda")
+    buf = torch.full((2, 3), 0.5, dtype=torch.float64, device="cuda")
+    with pytest.raises(B200Error, match="owned"):
+        s.halo_unpack(idx, buf)
+    after = s.download()["x"]
+    assert after[3].tolist() == list(x[3])
+    s.halo_unpack(idx[:1], buf[:1])
+    assert s.download()["x"][len(x) - 1].tolist() == [0.5, 0.5, 0.5]
     # b200_run decides rebuilds alone: it refuses a context with ghosts
     s.set_ghosts(np.ones(len(x)))
     s.setup()

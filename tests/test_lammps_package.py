@@ -9,10 +9,13 @@ import subprocess
 
 import pytest
 
+from oracle import build_ref
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 PKG = os.path.join(ROOT, "lammps_b200", "lammps")
-# the reference tree, when present on this machine (read only)
-LAMMPS_SRC = os.environ.get("LAMMPS_SRC", "/root/reference/src")
+# the reference's src/ tree: LAMMPS_SRC, or the one oracle/build_ref.py
+# compiled (the tests skip when neither is present)
+LAMMPS_SRC = build_ref.built_src() or ""
 
 SOURCES = sorted(glob.glob(os.path.join(PKG, "*.cpp")))
 

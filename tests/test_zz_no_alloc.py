@@ -85,3 +85,26 @@ def test_rejects_sizes_beyond_limits():
     assert _noalloc(1 << 26, dv, dt, dm, 1, out) == -1  # B200_ERR_ARG
     assert _noalloc(0, dv, dt, dm, 1, out) == -1  # B200_ERR_ARG
     assert _noalloc(4, dv, dt, dm, 9, out) == -1  # B200_ERR_ARG
+
+
+def test_type_outside_range_gives_nan():
+    """A type outside 1..ntypes is never used as an index into mass[]: the
+    sum comes back NaN, and a following call with valid types is exact."""
+    n = 1000
+    rng = np.random.default_rng(3)
+    v = rng.normal(size=(n, 3))
+    t = np.ones(n, np.int32)
+    t[417] = 3  # ntypes = 2
+    m = np.array([0.0, 1.0, 2.0])
+    dv, dt, dm = _device(v, t, m)
+    out = torch.zeros(1, dtype=torch.float64, device="cuda:0")
+    assert _noalloc(n, dv, dt, dm, 2, out) == 0
+    torch.cuda.synchronize()
+    assert np.isnan(out.cpu().numpy()[0])
+    dt[417] = 2
+    assert _noalloc(n, dv, dt, dm, 2, out) == 0
+    torch.cuda.synchronize()
+    tt = t.copy()
+    tt[417] = 2
+    ref = float(np.sum(((v * v).sum(axis=1) * m[tt]).astype(np.longdouble)))
+    assert abs(out.cpu().numpy()[0] - ref) <= REL * abs(ref)
