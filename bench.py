@@ -1,16 +1,15 @@
 #!/usr/bin/env python
 """Throughput of the short-range MD step on B200, in Matom-steps/s.
 
-Workload (one bench step = the first 100 NVE timesteps from the seeded
-initial state; restore and Verlet setup are untimed): the EAM
-configuration -- 32,000 atoms, fcc 20^3, a = 3.615 A, synthetic
-5000-point setfl tables (lammps_b200/eam_synth.py), Gaussian
-velocities at 1600 K (seed 376847), dt = 5 fs, skin 1.0 A,
-`neigh_modify every 1 delay 5 check yes`, FP32-mixed precision.  The FP64
-form of the same workload and the 4,000,000-atom LJ configuration (fcc 100^3,
-rho* 0.8442, T* 1.44, rc 2.5, skin 0.3, rebuild every 20) in both precisions
-are reported beside it.  Inputs are seeded synthetic data of the reference's
-benchmark shapes.
+Headline workload (one bench step = the first 100 NVE timesteps from the
+seeded initial state; restore and Verlet setup are untimed): the
+4,000,000-atom LJ configuration -- fcc 100^3 at rho* 0.8442, Gaussian
+velocities at T* 1.44 (seed 87287, loop geom), lj/cut rc 2.5, skin 0.3,
+rebuild every 20 steps, dt 0.005 -- in FP32-mixed precision, with the FP64
+form, their ratio and both forms' errors against the oracle beside it.  The
+32,000-atom EAM configuration (synthetic 5000-point setfl tables) is a block
+of its own (eam_32k) with the same figures.  Inputs are seeded synthetic data
+of the reference's benchmark shapes.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
@@ -21,7 +20,9 @@ events.  `value` is the aggregate over ranks (max time over ranks).  `e2e` is
 the same metric through the public API with host buffers: upload of x, v,
 type, setup, 100 steps, download of x, v, f, image -- wall clock around
 synchronised calls.  Under torchrun each rank runs its own replica (weak
-scaling, no data-path collective).
+scaling, no data-path collective).  `--impl reference` times the reference's
+own CPU build (oracle/_ref/lmp_serial, -sf omp on all host cores) on the same
+workload.
 """
 from __future__ import annotations
 
@@ -270,17 +271,23 @@ EAM_HALF_PAIRS = 21.0             # half pairs inside 4.95 A per atom on the fcc
 EAM_FLOP_PER_ATOM_STEP = 80.0 * EAM_HALF_PAIRS + 15.0
 
 
-def step_roofline(n, step_ms, hbm_peak, clk):
+LJ_BYTES_PER_ATOM_STEP = 168.0   # x read for forces, f write, fused NVE x, v, f read, x, v write
+LJ_HALF_PAIRS = 27.6             # half pairs inside rc = 2.5 per atom in the fluid at rho* 0.8442
+LJ_FLOP_PER_ATOM_STEP = 27.0 * LJ_HALF_PAIRS
+
+
+def step_roofline(n, step_ms, hbm_peak, clk, bytes_per_atom=EAM_BYTES_PER_ATOM_STEP,
+                  flop_per_atom=EAM_FLOP_PER_ATOM_STEP):
     """Whole-step fractions: algorithmic bytes against the measured copy
     bandwidth and algorithmic FLOPs against the nominal FP32 FMA peak
     (148 SMs x 128 lanes x 2 FLOP x the sampled maximum SM clock)."""
     rate = n / (step_ms * 1e-3)  # atom-steps per second
     mhz = (clk or {}).get("sm_max_mhz") or 1965.0
     fp32_peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
-    gbs = EAM_BYTES_PER_ATOM_STEP * rate / 1e9
-    tflops = EAM_FLOP_PER_ATOM_STEP * rate / 1e12
-    return {"alg_bytes_per_atom_step": EAM_BYTES_PER_ATOM_STEP, "achieved_gbs": gbs,
-            "hbm_frac": gbs / hbm_peak, "alg_flop_per_atom_step": EAM_FLOP_PER_ATOM_STEP,
+    gbs = bytes_per_atom * rate / 1e9
+    tflops = flop_per_atom * rate / 1e12
+    return {"alg_bytes_per_atom_step": bytes_per_atom, "achieved_gbs": gbs,
+            "hbm_frac": gbs / hbm_peak, "alg_flop_per_atom_step": flop_per_atom,
             "achieved_tflops": tflops, "fp32_peak_tflops_nominal": fp32_peak,
             "fp32_frac": tflops / fp32_peak}
 
@@ -345,50 +352,212 @@ def e2e_run(sysm, x_pin, v_pin, t_pin, out_pin, K):
     return (t1 - t0) * 1e3, h2d, d2h
 
 
-def mixed_error(make):
-    """Norm-wise relative force error of the mixed form against the FP64
-    form on the same positions (taken after 100 FP64 steps, off-lattice)."""
-    s64 = make("fp64")
-    s64.setup()
-    s64.run(MD_STEPS)
-    st = s64.download()
-    s64.neigh_build()
-    f64 = s64.compute(1, 1)
-    F64 = s64.download()["f"]
-    s64.close()
-    smx = make("mixed")
-    smx.set_atoms(st["x"], None, st["v"])
-    smx.neigh_build()
-    fmx = smx.compute(1, 1)
-    Fmx = smx.download()["f"]
-    smx.close()
-    return {"force": float(np.linalg.norm(Fmx - F64) / np.linalg.norm(F64)),
-            "energy": abs(fmx["eng"] - f64["eng"]) / abs(f64["eng"]),
-            "virial_diag": float(np.max(np.abs(fmx["virial"][:3] - f64["virial"][:3]) /
-                                        np.abs(f64["virial"][:3])))}
+def host_cpu():
+    """The host's CPU model and the cores this process may use."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    try:
+        cores = len(os.sched_getaffinity(0))
+    except AttributeError:
+        cores = os.cpu_count() or 1
+    return {"model": model, "cores": cores}
 
 
-def cpu_reference(setfl, x, v, hi, seconds=10.0, threads=None):
-    """The oracle port (reference CPU algorithm) on the host cores."""
+# The reference's own CPU path: oracle/_ref/lmp_serial, the reference's
+# LAMMPS built from its sources (oracle/build_ref.py), on the workload of the
+# GPU arm -- the same lattice, velocities, potential, neighbor settings and
+# timestep, from the seeded initial state, one process per sample.  One core:
+# the plain styles; all cores: `-sf omp` (lj/cut/omp, eam/alloy/omp, nve/omp,
+# OpenMP neighbor builds) with OMP_NUM_THREADS threads.
+WORKLOADS = {
+    "eam32k": {"atoms": 32000, "script": [
+        "units metal", "atom_style atomic", "lattice fcc 3.615",
+        "region box block 0 20 0 20 0 20", "create_box 1 box", "create_atoms 1 box",
+        "pair_style eam/alloy", "pair_coeff * * Cu_synth.eam.alloy Cu",
+        "velocity all create 1600.0 376847 dist gaussian loop geom",
+        "neighbor 1.0 bin", "neigh_modify every 1 delay 5 check yes", "fix 1 all nve",
+        "timestep 0.005"]},
+    "lj32k": {"atoms": 32000, "script": [
+        "units lj", "atom_style atomic", "lattice fcc 0.8442",
+        "region box block 0 20 0 20 0 20", "create_box 1 box", "create_atoms 1 box",
+        "mass 1 1.0", "velocity all create 1.44 87287 dist gaussian loop geom",
+        "pair_style lj/cut 2.5", "pair_coeff 1 1 1.0 1.0 2.5", "neighbor 0.3 bin",
+        "neigh_modify delay 0 every 20 check no", "fix 1 all nve", "timestep 0.005"]},
+    "lj4m": {"atoms": 4000000, "script": [
+        "units lj", "atom_style atomic", "lattice fcc 0.8442",
+        "region box block 0 100 0 100 0 100", "create_box 1 box", "create_atoms 1 box",
+        "mass 1 1.0", "velocity all create 1.44 87287 dist gaussian loop geom",
+        "pair_style lj/cut 2.5", "pair_coeff 1 1 1.0 1.0 2.5", "neighbor 0.3 bin",
+        "neigh_modify delay 0 every 20 check no", "fix 1 all nve", "timestep 0.005"]},
+}
+
+
+def reference_binary():
+    p = os.path.join(ROOT, "oracle", "_ref", "lmp_serial")
+    return p if os.access(p, os.X_OK) else None
+
+
+def reference_cpu(workload, threads, samples, steps=MD_STEPS, setfl=None, timeout=900):
+    """Matom-steps/s of the reference's own binary: `samples` fresh runs of
+    the first `steps` steps from the seeded state; the median of the `Loop
+    time` rates (setup excluded, as the GPU arm's events exclude it)."""
+    import re
+    import shutil
+    exe = reference_binary()
+    w = WORKLOADS[workload]
+    tmp = tempfile.mkdtemp(prefix="b200ref_")
+    if setfl:
+        shutil.copy(setfl, os.path.join(tmp, "Cu_synth.eam.alloy"))
+    with open(os.path.join(tmp, "in.bench"), "w") as fh:
+        fh.write("\n".join(w["script"] + [f"thermo {steps}", f"run {steps}"]) + "\n")
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    args = [exe, "-in", "in.bench", "-log", "none", "-echo", "none"]
+    if threads > 1:
+        args += ["-sf", "omp"]
+    rates, secs = [], []
+    for _ in range(samples):
+        r = subprocess.run(args, cwd=tmp, env=env, capture_output=True, text=True, timeout=timeout)
+        m = re.search(r"Loop time of (\S+) on", r.stdout)
+        if r.returncode != 0 or not m:
+            raise RuntimeError(f"lmp_serial failed ({r.returncode}): {(r.stdout + r.stderr)[-500:]}")
+        secs.append(float(m.group(1)))
+        rates.append(w["atoms"] * steps / secs[-1] / 1e6)
+    style = "-sf omp, " if threads > 1 else "plain styles, "
+    return dict(value=statistics.median(rates), unit="Matom-steps/s", cores=threads,
+                kind="reference", samples=rates,
+                sample=f"{workload}: {samples} fresh runs of the first {steps} NVE steps from the "
+                       f"seeded state, reference lmp_serial ({style}{threads} thread(s)), median "
+                       f"of the Loop-time rates ({sum(secs):.1f} s of loop time)")
+
+
+def port_cpu(setfl, x, v, hi, threads, samples):
+    """Fallback when the reference binary is absent: the oracle port of the
+    reference's algorithm on the same first-100-steps workload."""
     import oracle
-    threads = threads or os.cpu_count() or 1
-    s = oracle.OracleSim("metal", threads=threads)
-    s.box([0.0, 0.0, 0.0], hi)
-    s.atoms(x, v)
-    s.eam_setfl(setfl, [0])
-    s.neighbor(1.0, 1, 5, True, 1000)
-    s.timestep(0.005)
-    s.setup()
-    t0 = time.perf_counter()
-    s.run(5)
-    dt5 = time.perf_counter() - t0
-    nsteps = max(5, min(5000, int(seconds / max(dt5 / 5, 1e-6))))
-    t0 = time.perf_counter()
-    s.run(nsteps)
-    dt = time.perf_counter() - t0
-    return dict(value=len(x) * nsteps / dt / 1e6, unit="Matom-steps/s", cores=threads, kind="port",
-                sample=f"EAM 32,000 atoms x {nsteps} NVE steps (oracle port, OpenMP {threads} threads), "
-                       f"{dt:.1f} s")
+    rates, secs = [], []
+    for _ in range(samples):
+        s = oracle.OracleSim("metal", threads=threads)
+        s.box([0.0, 0.0, 0.0], hi)
+        s.atoms(x, v)
+        s.eam_setfl(setfl, [0])
+        s.neighbor(1.0, 1, 5, True, 1000)
+        s.timestep(0.005)
+        s.setup()
+        t0 = time.perf_counter()
+        s.run(MD_STEPS)
+        secs.append(time.perf_counter() - t0)
+        rates.append(len(x) * MD_STEPS / secs[-1] / 1e6)
+        s.close()
+    return dict(value=statistics.median(rates), unit="Matom-steps/s", cores=threads, kind="port",
+                samples=rates,
+                sample=f"eam32k: {samples} runs of the first {MD_STEPS} NVE steps from the seeded "
+                       f"state, oracle port (OpenMP {threads} threads), median ({sum(secs):.1f} s)")
+
+
+def port_cpu_lj4m(threads, samples, steps):
+    """Fallback when the reference binary is absent: the oracle port on the
+    LJ-4M workload's first `steps` steps."""
+    import oracle
+    from lammps_b200 import inputs
+    a = inputs.lj_lattice_constant("fcc", 0.8442)
+    rates, secs = [], []
+    for _ in range(samples):
+        o = oracle.OracleSim("lj", threads=threads)
+        o.box([0.0, 0.0, 0.0], [100 * a] * 3)
+        o.atoms(oracle.lattice("fcc", 100, 100, 100, a))
+        o.mass(1, 1.0)
+        o.lj_cut(2.5)
+        o.lj_coeff(1, 1, 1.0, 1.0, 2.5)
+        o.velocity_create(1.44, 87287, gaussian=True, loop_geom=True)
+        o.neighbor(0.3, 20, 0, False, 1000)
+        o.timestep(0.005)
+        o.setup()
+        t0 = time.perf_counter()
+        o.run(steps)
+        secs.append(time.perf_counter() - t0)
+        rates.append(4000000 * steps / secs[-1] / 1e6)
+        o.close()
+    return dict(value=statistics.median(rates), unit="Matom-steps/s", cores=threads, kind="port",
+                samples=rates,
+                sample=f"lj4m: {samples} runs of the first {steps} NVE steps from the seeded "
+                       f"state, oracle port (OpenMP {threads} threads), median ({sum(secs):.1f} s)")
+
+
+def cpu_baseline_eam32k(setfl, x, v, hi, samples=3):
+    """All host cores (the baseline) plus a one-core row."""
+    host = host_cpu()
+    if reference_binary():
+        out = reference_cpu("eam32k", host["cores"], samples, setfl=setfl)
+        out["one_core"] = reference_cpu("eam32k", 1, 2, setfl=setfl)
+    else:
+        out = port_cpu(setfl, x, v, hi, host["cores"], samples)
+        out["one_core"] = port_cpu(setfl, x, v, hi, 1, 1)
+    out["cpu_model"] = host["model"]
+    out["nproc"] = host["cores"]
+    return out
+
+
+def errors_vs(f, eng, vir, ref):
+    """Force, energy and virial errors against a reference state: norm-wise
+    relative force error and the largest |dF_i| over the RMS force; relative
+    energy and virial diagonal; off-diagonal virial over |trace|."""
+    d = f - ref["f"]
+    rms = float(np.sqrt(np.mean(np.sum(ref["f"] ** 2, axis=1))))
+    tr = abs(float(np.sum(ref["virial"][:3])))
+    return {"force": float(np.linalg.norm(d) / np.linalg.norm(ref["f"])),
+            "force_max_over_rms": float(np.max(np.linalg.norm(d, axis=1)) / rms),
+            "energy": abs(eng - ref["eng"]) / abs(ref["eng"]),
+            "virial_diag": float(np.max(np.abs(vir[:3] - ref["virial"][:3]) / np.abs(ref["virial"][:3]))),
+            "virial_offdiag_over_trace": float(np.max(np.abs(vir[3:] - ref["virial"][3:])) / tr)}
+
+
+def lj4m_oracle_state(hi, steps=10):
+    """The oracle (all host threads) after `steps` steps of the LJ-4M
+    configuration, with forces, energy and pairwise virial of that state."""
+    import oracle
+    from lammps_b200 import inputs
+    a = inputs.lj_lattice_constant("fcc", 0.8442)
+    o = oracle.OracleSim("lj", threads=host_cpu()["cores"])
+    o.box([0.0, 0.0, 0.0], hi)
+    o.atoms(oracle.lattice("fcc", 100, 100, 100, a))
+    o.mass(1, 1.0)
+    o.lj_cut(2.5)
+    o.lj_coeff(1, 1, 1.0, 1.0, 2.5)
+    o.velocity_create(1.44, 87287, gaussian=True, loop_geom=True)
+    o.neighbor(0.3, 20, 0, False, 1000)
+    o.timestep(0.005)
+    o.setup()
+    o.run(steps)
+    o.compute(eflag=1, vflag=1)
+    out = dict(x=o.x, f=o.f, eng=o.eng_vdwl, virial=o.virial)
+    o.close()
+    return out
+
+
+def eam32k_oracle_state(setfl, x, hi, steps=10):
+    """The oracle after `steps` steps of the EAM-32k configuration, with the
+    forces, energy and pairwise virial of that state."""
+    import oracle
+    o = oracle.OracleSim("metal", threads=host_cpu()["cores"])
+    o.box([0.0, 0.0, 0.0], hi)
+    o.atoms(x)
+    o.eam_setfl(setfl, [0])
+    o.velocity_create(1600.0, 376847, gaussian=True, loop_geom=True)
+    o.neighbor(1.0, 1, 5, True, 1000)
+    o.timestep(0.005)
+    o.setup()
+    o.run(steps)
+    o.compute(eflag=1, vflag=1)
+    out = dict(x=o.x, f=o.f, eng=o.eng_vdwl, virial=o.virial)
+    o.close()
+    return out
 
 
 def replica_bench(prec, batch, torch, steps=1000, lat_steps=200):
@@ -546,46 +715,191 @@ def profile_case(args):
     s.close()
 
 
+def headline_timed(s, torch, flush, K, W, start, ws, dev):
+    """W untimed and K timed bench steps of one form, bracketed by a barrier
+    and a synchronize on both sides, with the SM clocks sampled during the
+    timed region: (value over all ranks, max-over-ranks total ms, launches,
+    clocks)."""
+    ext = torch.cuda.ExternalStream(s.stream)
+    s.setup()
+    for _ in range(W):
+        device_time_run(s, torch, ext, flush, MD_STEPS, start)
+    barrier(ws)
+    torch.cuda.synchronize()
+    clocks = clock_sampler(dev)
+    clocks.start()
+    l0 = s.kernel_launches
+    per = [device_time_run(s, torch, ext, flush, MD_STEPS, start) for _ in range(K)]
+    torch.cuda.synchronize()
+    launches = s.kernel_launches - l0
+    barrier(ws)
+    clk = clocks.stop()
+    total_ms = allmax(sum(per), ws, torch)
+    atoms_all = allsum(s.n, ws, torch)  # every rank advances its own box
+    return atoms_all * MD_STEPS * K / (total_ms * 1e3), total_ms, launches, clk
+
+
+def phase_times(s, torch, flush, start, runs=2):
+    """Per-MD-step device time of each phase, from the CUDA events recorded
+    inside the step graphs (a separate pass: the events cost time)."""
+    ext = torch.cuda.ExternalStream(s.stream)
+    s.set_timing(True)
+    device_time_run(s, torch, ext, flush, MD_STEPS, start)
+    s.timing(reset=True)
+    for _ in range(runs):
+        device_time_run(s, torch, ext, flush, MD_STEPS, start)
+    ph = s.timing(reset=True)
+    s.set_timing(False)
+    return {k: ph[k] / max(ph["steps"], 1) for k in s.PHASES}
+
+
+def e2e_block(torch, s, x, v, K, ws=1):
+    """The form's metric through the public API with page-locked host
+    buffers: upload x, v, type; setup; 100 steps; download x, v, f, image."""
+    n = len(x)
+    x_pin = pinned(torch, np.ascontiguousarray(x, dtype=np.float64))
+    v_pin = pinned(torch, np.ascontiguousarray(v, dtype=np.float64))
+    t_pin = pinned(torch, np.ones(n, np.int32))
+    o_pin = {k: pinned(torch, np.zeros((n, 3), dt)) for k, dt in
+             (("x", np.float64), ("v", np.float64), ("f", np.float64), ("image", np.int32))}
+    e2e_run(s, x_pin, v_pin, t_pin, o_pin, 1)
+    e_ms, h2d, d2h = e2e_run(s, x_pin, v_pin, t_pin, o_pin, K)
+    _PINNED.clear()
+    e_ms = allmax(e_ms, ws, torch)
+    atoms_all = allsum(n, ws, torch)
+    return {"value": atoms_all * MD_STEPS * K / (e_ms * 1e3), "unit": "Matom-steps/s",
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+
+
+def oracle_errors(make, ref):
+    """Both forms' force, energy and virial errors on the oracle's state."""
+    errs = {}
+    for prec in ("fp64", "mixed"):
+        s = make(prec)
+        s.set_atoms(ref["x"], None, None)
+        s.neigh_build()
+        r = s.compute(1, 1)
+        errs[prec] = errors_vs(s.download()["f"], r["eng"], r["virial"], ref)
+        s.close()
+    return errs
+
+
+def eam32k_block(torch, flush, K, W, setfl, clk, no_cpu):
+    """The 32,000-atom EAM configuration (synthetic 5000-point setfl) as a
+    line of its own: mixed and FP64, the dominant kernel's roofline, end to
+    end through the API, errors against the oracle, the reference's CPU
+    path on the same workload (all cores and one core)."""
+    x, v, hi = eam32k_inputs()
+    n = len(x)
+    out = {"workload": "eam-32k: fcc 20^3 a=3.615 A, synthetic 5000-point setfl (eam/alloy), "
+                       "1600 K Gaussian (seed 376847, loop geom), skin 1.0, every 1 delay 5 check "
+                       "yes, dt 5 fs; one bench step = the first 100 NVE steps from the seeded state",
+           "atoms": n, "unit": "Matom-steps/s",
+           "l2": "flushed (256 MB write) before every timed bench step"}
+    for prec in ("mixed", "fp64"):
+        s = make_eam32k(prec, setfl, x, v, hi)
+        t, _ = time_form(s, torch, flush, K, W, (x, v))
+        out[prec] = n * MD_STEPS * K / (t * 1e3)
+        out[prec + "_ms_per_md_step"] = t / (K * MD_STEPS)
+        ph = phase_times(s, torch, flush, (x, v))
+        out[prec + "_phases_ms_per_md_step"] = ph
+        if prec == "mixed":
+            out["e2e"] = e2e_block(torch, s, x, v, K)
+            peak, peak_kind = load_peaks()
+            dom = max(("pair1", "pair2"), key=lambda k: ph[k])
+            # force pass: x (24 B) and F' (8 B) read, f (24 B) written; density
+            # pass: x (24 B) read, rho and F' (16 B) written
+            bpa = 56.0 if dom == "pair2" else 40.0
+            ach = bpa * n / (ph[dom] * 1e-3) / 1e9
+            out["roofline"] = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                               "frac": ach / peak, "traffic": load_traffic().get(f"eam32k_mixed_{dom}"),
+                               "kernel": "k_eam_force (mixed)" if dom == "pair2" else "k_eam_rho (mixed)",
+                               "kernel_ms": ph[dom], "peak_source": f"{peak_kind} hbm_gbs",
+                               "step": step_roofline(n, out["mixed_ms_per_md_step"], peak, clk)}
+        s.close()
+    out["value"] = out["mixed"]
+    out["mixed_over_fp64"] = out["mixed"] / out["fp64"]
+    ref = eam32k_oracle_state(setfl, x, hi)
+    out["error_vs_oracle"] = oracle_errors(lambda p: make_eam32k(p, setfl, x, None, hi), ref)
+    out["error_vs_oracle"]["state"] = "oracle after 10 steps from the seeded state"
+    if not no_cpu:
+        out["cpu_baseline"] = cpu_baseline_eam32k(setfl, x, v, hi)
+    return out
+
+
+def cpu_rows(setfl):
+    """The reference's own CPU path on each configuration that runs on a
+    CPU in seconds: one core (plain styles) and all cores (-sf omp)."""
+    host = host_cpu()
+    rows = {"cpu_model": host["model"], "nproc": host["cores"]}
+    rows["lj_32k"] = {"one_core": reference_cpu("lj32k", 1, 1)["value"],
+                      "all_cores": reference_cpu("lj32k", host["cores"], 3)["value"]}
+    rows["eam_32k"] = {"one_core": reference_cpu("eam32k", 1, 1, setfl=setfl)["value"],
+                       "all_cores": reference_cpu("eam32k", host["cores"], 3, setfl=setfl)["value"]}
+    rows["note"] = ("Matom-steps/s of fresh runs of the first 100 steps from the seeded state "
+                    "(median of the all-core runs); lj_4M is in cpu_baseline")
+    return rows
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--no-extras", action="store_true", help="skip the FP64 and 4M-atom LJ lines")
-    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--no-extras", action="store_true", help="only the headline line")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline samples")
     ap.add_argument("--eager", action="store_true",
                     help="with --case: launch kernels one by one (for profilers)")
     ap.add_argument("--tpa", type=int, default=0,
                     help="with --case: threads per atom of the pair kernels (0 = autotuned)")
     ap.add_argument("--case", default=None,
                     help="profile one form only: eam32k-mixed, eam32k-fp64, lj4m-mixed, lj4m-fp64, "
-                         "c3-mixed, c3-fp64 (256 replicas)")
+                         "eam4m-mixed, eam4m-fp64, c3-mixed, c3-fp64 (256 replicas)")
     args = ap.parse_args()
     if args.case:
         return profile_case(args)
     K, W = args.steps, max(args.warmup, 3)
     ws, rank, local = dist_setup()
-    config = {"workload": "eam-32k: fcc 20^3 a=3.615, synthetic 5000-point setfl, 1600 K, "
-                          "the first 100 NVE steps from the seeded initial state per bench step; "
-                          "extras: eam Cu_u3 32k (bench/in.eam) and lj-4M fcc 100^3",
-              "atoms": 32000, "md_steps_per_step": MD_STEPS, "precision": "mixed",
-              "l2": "flushed (256 MB write) before every timed bench step",
+    config = {"workload": "lj-4M: fcc 100^3 (4,000,000 atoms), rho* 0.8442, T* 1.44 Gaussian "
+                          "(seed 87287, loop geom), lj/cut rc 2.5, skin 0.3, every 20 delay 0 "
+                          "check no, dt 0.005, mixed precision; one bench step = the first 100 "
+                          "NVE steps from the seeded initial state",
+              "atoms": 4000000, "md_steps_per_step": MD_STEPS, "precision": "mixed",
+              "l2": "inputs larger than L2 (4M atoms), and flushed (256 MB write) before every "
+                    "timed bench step",
               "parallelism": f"replicas x{ws}"}
     tmp = tempfile.mkdtemp(prefix="b200bench_")
     from lammps_b200.eam_synth import write_setfl
     setfl = write_setfl(os.path.join(tmp, "Cu_synth.eam.alloy"))
-    x, v, hi = eam32k_inputs()
+    x4, v4, hi4 = lj4m_inputs()
+    n4 = len(x4)
+    RS = 20  # MD steps of one reference sample of LJ-4M (one neighbor rebuild)
 
     if args.impl == "reference":
+        # the reference's own CPU path on all host cores; each bench step is a
+        # fresh run of the first RS steps of the workload (W discarded)
         if rank == 0:
-            cpu = cpu_reference(setfl, x, v, hi, seconds=max(5.0, 2.0 * (K + W) / 3))
-            line = {"metric": METRIC, "value": cpu["value"], "unit": "Matom-steps/s", "n_gpus": ws,
-                    "steps": K, "warmup": W, "ms_per_step": 32000 * MD_STEPS / (cpu["value"] * 1e3),
+            host = host_cpu()
+            if reference_binary():
+                cpu = reference_cpu("lj4m", host["cores"], W + K, steps=RS)
+                timed = cpu["samples"][W:]
+                secs = [n4 * RS / (r * 1e6) for r in timed]
+                value = n4 * RS * K / sum(secs) / 1e6
+                cpu["sample"] += f"; first {W} runs discarded as warm-up"
+            else:
+                cpu = port_cpu_lj4m(host["cores"], W + K, RS)
+                timed = cpu["samples"][W:]
+                secs = [n4 * RS / (r * 1e6) for r in timed]
+                value = n4 * RS * K / sum(secs) / 1e6
+                cpu["sample"] = "reference binary absent: " + cpu["sample"]
+            cpu.update(value=value, cpu_model=host["model"], nproc=host["cores"])
+            line = {"metric": METRIC, "value": value, "unit": "Matom-steps/s", "n_gpus": ws,
+                    "steps": K, "warmup": W, "ms_per_step": sum(secs) * 1e3 / K,
                     "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                    "dtype": "f64", "data": "synthetic (seeded lattice + velocities, synthetic setfl)",
+                    "dtype": "f64", "data": "synthetic (seeded fcc lattice + Gaussian velocities)",
                     "config": config, "impl": "reference", "cpu_baseline": cpu,
-                    "e2e": {"value": cpu["value"], "unit": "Matom-steps/s", "h2d_bytes_per_step": 0,
+                    "e2e": {"value": value, "unit": "Matom-steps/s", "h2d_bytes_per_step": 0,
                             "d2h_bytes_per_step": 0}}
             print(json.dumps(line))
         return
@@ -596,74 +910,60 @@ def main():
     DEVICE = dev
     torch.cuda.set_device(dev)
     flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
-    sysm = make_eam32k("mixed", setfl, x, v, hi)
-    n = sysm.n
-    ext = torch.cuda.ExternalStream(sysm.stream)
+    start = (x4, v4)
 
-    # ---- headline: mixed precision EAM, device-timed -----------------------
-    launches0 = None
-    sysm.setup()
-    start = (x, v)
-    for _ in range(W):
-        device_time_run(sysm, torch, ext, flush, MD_STEPS, start)
-    barrier(ws)
-    torch.cuda.synchronize()
-    clocks = clock_sampler(dev)
-    clocks.start()
-    launches0 = sysm.kernel_launches
-    per = [device_time_run(sysm, torch, ext, flush, MD_STEPS, start) for _ in range(K)]
-    torch.cuda.synchronize()
-    launches = sysm.kernel_launches - launches0
-    barrier(ws)
-    clk = clocks.stop()
-    total_ms = allmax(sum(per), ws, torch)
-    atoms_all = allsum(n, ws, torch)  # every rank advances its own box
-    value = atoms_all * MD_STEPS * K / (total_ms * 1e3)
-
-    # ---- per-phase device timers over the same number of bench steps ------
-    sysm.set_timing(True)
-    for _ in range(2):
-        device_time_run(sysm, torch, ext, flush, MD_STEPS, start)
-    sysm.timing(reset=True)
-    per_t = [device_time_run(sysm, torch, ext, flush, MD_STEPS, start) for _ in range(K)]
-    ph = sysm.timing(reset=True)
-    sysm.set_timing(False)
-    steps_t = max(ph["steps"], 1)
-    phases = {k: ph[k] / steps_t for k in sysm.PHASES}
-    dom = max(("pair1", "pair2"), key=lambda k: phases[k])
-    # algorithmic bytes per atom of the dominant EAM kernel: force pass reads
-    # x (24 B) and fp (8 B) and writes f (24 B); density pass reads x (24 B)
-    # and writes rho, fp (16 B)
-    bytes_per_atom = 56.0 if dom == "pair2" else 40.0
+    # ---- headline: LJ-4M, mixed precision, device-timed -------------------
+    sysm = make_lj("mixed", x4, v4, hi4)
+    value, total_ms, launches, clk = headline_timed(sysm, torch, flush, K, W, start, ws, dev)
+    phases = phase_times(sysm, torch, flush, start)
     peak, peak_kind = load_peaks()
-    achieved = bytes_per_atom * n / (phases[dom] * 1e-3) / 1e9
-    traffic = load_traffic().get(f"eam32k_mixed_{dom}")
-    step_ms = sum(per_t) / (K * MD_STEPS)
+    # algorithmic bytes of the dominant kernel (k_lj_mixed): x read (24 B)
+    # and f written (24 B) per atom, FP64 state
+    achieved = 48.0 * n4 / (phases["pair1"] * 1e-3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": traffic,
-                "kernel": "k_eam_force (mixed)" if dom == "pair2" else "k_eam_rho (mixed)",
-                "kernel_ms": phases[dom], "peak_source": f"{peak_kind} hbm_gbs",
-                "step": step_roofline(n, step_ms, peak, clk)}
+                "frac": achieved / peak, "traffic": load_traffic().get("lj4m_mixed_pair1"),
+                "kernel": "k_lj_mixed", "kernel_ms": phases["pair1"],
+                "peak_source": f"{peak_kind} hbm_gbs",
+                # whole-step figures from the headline runs (timing events off),
+                # so that they follow from `value`
+                "step": step_roofline(n4, total_ms / (K * MD_STEPS), peak, clk,
+                                      LJ_BYTES_PER_ATOM_STEP, LJ_FLOP_PER_ATOM_STEP)}
+    e2e = e2e_block(torch, sysm, x4, v4, K, ws)
+    sysm.close()
 
-    # ---- end to end through the public API --------------------------------
-    x_pin = pinned(torch, np.ascontiguousarray(x, dtype=np.float64))
-    v_pin = pinned(torch, np.ascontiguousarray(v, dtype=np.float64))
-    t_pin = pinned(torch, np.ones(n, np.int32))
-    out_pin = {k: pinned(torch, np.zeros((n, 3), dt)) for k, dt in
-               (("x", np.float64), ("v", np.float64), ("f", np.float64), ("image", np.int32))}
-    e2e_run(sysm, x_pin, v_pin, t_pin, out_pin, 1)
-    e_ms, h2d, d2h = e2e_run(sysm, x_pin, v_pin, t_pin, out_pin, K)
-    e_ms = allmax(e_ms, ws, torch)
-    e2e = {"value": atoms_all * MD_STEPS * K / (e_ms * 1e3), "unit": "Matom-steps/s",
-           "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+    # ---- the FP64 form of the same workload -------------------------------
+    s64 = make_lj("fp64", x4, v4, hi4)
+    v64, t64, _, _ = headline_timed(s64, torch, flush, K, W, start, ws, dev)
+    ph64 = phase_times(s64, torch, flush, start)
+    s64.close()
 
-    extras = {}
+    extras = {"fp64": v64, "mixed_over_fp64": value / v64,
+              "ms_per_md_step": {"mixed": total_ms / (K * MD_STEPS), "fp64": t64 / (K * MD_STEPS)},
+              "phases_ms_per_md_step": {"mixed": phases, "fp64": ph64}}
     if not args.no_extras:
-        s64 = make_eam32k("fp64", setfl, x, v, hi)
-        t64, _ = time_form(s64, torch, flush, K, W, start)
-        extras["eam_32k"] = {"mixed": value / ws, "fp64": n * MD_STEPS * K / (t64 * 1e3)}
-        extras["eam_32k"]["mixed_over_fp64"] = extras["eam_32k"]["mixed"] / extras["eam_32k"]["fp64"]
-        s64.close()
+        ref = lj4m_oracle_state(hi4)
+        extras["error_vs_oracle"] = oracle_errors(lambda p: make_lj(p, x4, v4, hi4, atoms=False),
+                                                  ref)
+        extras["error_vs_oracle"]["state"] = ("oracle after 10 steps from the seeded state "
+                                              "(all host threads)")
+        # NVE energy conservation over 1000 steps (thermo every 100), both
+        # forms from the same state
+        nve, etot = {}, {}
+        for prec in ("mixed", "fp64"):
+            s = make_lj(prec, x4, v4, hi4)
+            s.set_thermo(100)
+            rows = [s.setup()] + s.run(1000)
+            st = np.array([r["Step"] for r in rows], dtype=float)
+            e = np.array([r["TotEng"] for r in rows])
+            etot[prec] = e
+            nve[prec] = {"etot_first": float(e[0]), "etot_last": float(e[-1]),
+                         "slope_per_step": float(np.polyfit(st, e, 1)[0])}
+            s.close()
+        nve["max_abs_etot_diff"] = float(np.max(np.abs(etot["mixed"] - etot["fp64"])))
+        extras["nve_1000"] = nve
+
+        extras["eam_32k"] = eam32k_block(torch, flush, K, W, setfl, clk,
+                                         args.no_cpu or rank != 0 or ws != 1)
         cu = {}
         for prec in ("mixed", "fp64"):
             scu, st = make_eam_cu(prec)
@@ -672,41 +972,6 @@ def main():
             scu.close()
         cu["mixed_over_fp64"] = cu["mixed"] / cu["fp64"]
         extras["eam_cu_u3_32k"] = cu
-        x4, v4, hi4 = lj4m_inputs()
-        lj = {}
-        for prec in ("mixed", "fp64"):
-            s = make_lj(prec, x4, v4, hi4)
-            k4 = max(2, K // 3)
-            t, _ = time_form(s, torch, flush, k4, 2, (x4, v4))
-            s.set_timing(True)
-            ext4 = torch.cuda.ExternalStream(s.stream)
-            device_time_run(s, torch, ext4, flush, MD_STEPS, (x4, v4))
-            s.timing(reset=True)
-            device_time_run(s, torch, ext4, flush, MD_STEPS, (x4, v4))
-            ph4 = s.timing(reset=True)
-            lj[prec] = len(x4) * MD_STEPS * k4 / (t * 1e3)
-            lj[prec + "_phases_ms_per_step"] = {k: ph4[k] / max(ph4["steps"], 1) for k in s.PHASES}
-            s.close()
-        lj["mixed_over_fp64"] = lj["mixed"] / lj["fp64"]
-        f_ms = lj["mixed_phases_ms_per_step"]["pair1"]
-        lj["force_kernel_gbs"] = 48.0 * len(x4) / (f_ms * 1e-3) / 1e9
-        # NVE energy conservation over 1000 steps (thermo every 100), both
-        # forms from the same state: TotEng per atom, its least-squares slope
-        # per step, and the largest mixed - FP64 difference along the run
-        etot = {}
-        for prec in ("mixed", "fp64"):
-            s = make_lj(prec, x4, v4, hi4)
-            s.set_thermo(100)
-            r0 = s.setup()
-            rows = [r0] + s.run(1000)
-            st = np.array([r["Step"] for r in rows], dtype=float)
-            e = np.array([r["TotEng"] for r in rows])
-            etot[prec] = e
-            lj[prec + "_nve_1000"] = {"etot_first": float(e[0]), "etot_last": float(e[-1]),
-                                      "slope_per_step": float(np.polyfit(st, e, 1)[0])}
-            s.close()
-        lj["nve_1000_max_abs_etot_diff"] = float(np.max(np.abs(etot["mixed"] - etot["fp64"])))
-        extras["lj_4M"] = lj
         # the EAM workload at 4M atoms: the density and force kernels at a
         # size where they are not launch- and latency-bound
         xe, ve, hie = eam4m_inputs()
@@ -716,14 +981,8 @@ def main():
             s = make_eam32k(prec, setfl, xe, ve, hie)
             k4 = max(2, K // 3)
             t, _ = time_form(s, torch, flush, k4, 2, (xe, ve))
-            s.set_timing(True)
-            exte = torch.cuda.ExternalStream(s.stream)
-            device_time_run(s, torch, exte, flush, MD_STEPS, (xe, ve))
-            s.timing(reset=True)
-            device_time_run(s, torch, exte, flush, MD_STEPS, (xe, ve))
-            phe = s.timing(reset=True)
+            ph = phase_times(s, torch, flush, (xe, ve), runs=1)
             em[prec] = len(xe) * MD_STEPS * k4 / (t * 1e3)
-            ph = {k: phe[k] / max(phe["steps"], 1) for k in s.PHASES}
             em[prec + "_phases_ms_per_step"] = ph
             # algorithmic bytes: density pass 40 B/atom, force pass 56 B/atom
             em[prec + "_rho_kernel_gbs"] = 40.0 * len(xe) / (ph["pair1"] * 1e-3) / 1e9
@@ -733,7 +992,6 @@ def main():
         extras["eam_4M"] = em
         extras["bricks_lj_4M"] = brick_bench(torch, x4, v4, hi4)
 
-    if not args.no_extras:
         from lammps_b200.replicas import replica_batch, shard_batch
         full = replica_batch(nrep=256)
         # under torchrun the 256 replicas are sharded across the ranks (no
@@ -768,25 +1026,30 @@ def main():
             "2-type lj/cut, 8000 atoms, 10x10x20 fcc rho*=0.85 + 0.05 jitter; errors of "
             "dL/d(eps,sigma) vs FP64 central differences (h=1e-5, cutoffs held) relative to "
             "the largest component, and of dL/dx along 8 unit directions relative to |dL/dx|")
-        extras["mixed_force_error"] = {
-            "eam_32k": mixed_error(lambda prec: make_eam32k(prec, setfl, x, v, hi)),
-            "lj_4M": mixed_error(lambda prec: make_lj(prec, x4, v4, hi4)),
-            "metric": "||F_mixed - F_fp64|| / ||F_fp64|| over all atoms, after 100 steps"}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        cpu = cpu_reference(setfl, x, v, hi, seconds=10.0)
+        host = host_cpu()
+        if reference_binary():
+            cpu = reference_cpu("lj4m", host["cores"], 3, steps=RS)
+            cpu["one_core"] = reference_cpu("lj4m", 1, 1, steps=5)
+            cpu["one_core"]["sample"] += (" (no rebuild inside the 5 steps: the set-up build is "
+                                          "untimed)")
+            if not args.no_extras:
+                cpu["rows"] = cpu_rows(setfl)
+        else:
+            cpu = port_cpu_lj4m(host["cores"], 1, RS)
+        cpu.update(cpu_model=host["model"], nproc=host["cores"])
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "Matom-steps/s", "n_gpus": ws, "steps": K,
                 "warmup": W, "ms_per_step": total_ms / K, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32-mixed (f64 positions/sums)",
-                "data": "synthetic (seeded fcc lattice + Gaussian velocities, synthetic setfl EAM)",
+                "data": "synthetic (seeded fcc lattice + Gaussian velocities; synthetic setfl EAM)",
                 "config": config, "clocks": clk, "e2e": e2e, "gpu_launches": int(launches),
-                "roofline": roofline, "phases_ms_per_md_step": phases, "cpu_baseline": cpu}
+                "roofline": roofline, "cpu_baseline": cpu}
         line.update(extras)
         print(json.dumps(line))
-    sysm.close()
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

@@ -127,6 +127,22 @@ int b200_natoms(const b200_ctx *ctx);
    b200_neigh_build) on its reneighbor steps. */
 int b200_update_positions(b200_ctx *ctx, const double *x);
 
+/* Column groups of b200_gather. */
+enum b200_field {
+  B200_FIELD_X = 1,     /* x y z */
+  B200_FIELD_V = 2,     /* vx vy vz */
+  B200_FIELD_F = 4,     /* fx fy fz */
+  B200_FIELD_IMAGE = 8  /* box crossings since the upload, ix iy iz (as doubles) */
+};
+/* The per-atom columns a dump writes, straight from the device: the
+   per-atom part of DumpCustom::pack (src/dump_custom.cpp:913-961) without a
+   download of the whole state.  Row r of out (host or device memory) holds
+   the requested groups, in the order x, v, f, image, of atom idx[r] (caller
+   index; host or device memory), or of atom r when idx is NULL; out has
+   m * 3 * (number of groups) doubles.  An index outside [0, n) returns
+   B200_ERR_ARG. */
+int b200_gather(b200_ctx *ctx, int fields, int m, const int *idx, double *out);
+
 /* ---- per-step entry points ------------------------------------------------- */
 
 /* Domain::pbc + periodic images + cell counting sort + full neighbor list

@@ -18,6 +18,8 @@ STATUS_NAMES = {
     -7: "B200_ERR_LOST_ATOMS", -8: "B200_ERR_TIMEOUT",
 }
 PREC = {"fp64": 0, "mixed": 1}
+# column groups of b200_gather (enum b200_field)
+FIELDS = {"x": 1, "v": 2, "f": 4, "image": 8}
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
@@ -40,6 +42,7 @@ SIGNATURES = {
     "b200_download_atoms": (C.c_int, [_vp, _dp, _dp, _dp, _ip]),
     "b200_natoms": (C.c_int, [_vp]),
     "b200_update_positions": (C.c_int, [_vp, _dp]),
+    "b200_gather": (C.c_int, [_vp, C.c_int, C.c_int, _ip, _dp]),
     "b200_neigh_build": (C.c_int, [_vp]),
     "b200_pair_compute": (C.c_int, [_vp, C.c_int, C.c_int, _dp, _dp, _dp, _dp]),
     "b200_nve_initial": (C.c_int, [_vp, C.c_double, C.c_double]),

@@ -148,6 +148,47 @@ __global__ void k_unsort(int n, int stride, const int *__restrict__ orig,
   }
 }
 
+// per-atom columns of m atoms (caller indices idx, or 0..m-1) in row-major
+// order: x y z | vx vy vz | fx fy fz | ix iy iz, the requested groups only
+__global__ void k_gather_cols(int m, int n, int stride, int fields, int ncols,
+                              const int *__restrict__ idx, const int *__restrict__ where,
+                              const double4 *__restrict__ x4, const double *__restrict__ v,
+                              const double *__restrict__ f, const int *__restrict__ image,
+                              double *__restrict__ out, int *__restrict__ status) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= m) return;
+  const int o = idx ? idx[r] : r;
+  if (o < 0 || o >= n) {  // recorded for the host; the row is left as it is
+    atomicExch(&status[ST_HALO_BAD], 1);
+    return;
+  }
+  const int k = where[o];
+  double *row = out + (size_t)r * ncols;
+  int c = 0;
+  if (fields & B200_FIELD_X) {
+    const double4 p = x4[k];
+    row[c++] = p.x;
+    row[c++] = p.y;
+    row[c++] = p.z;
+  }
+  if (fields & B200_FIELD_V) {
+    row[c++] = v[k];
+    row[c++] = v[stride + k];
+    row[c++] = v[2 * stride + k];
+  }
+  if (fields & B200_FIELD_F) {
+    row[c++] = f[k];
+    row[c++] = f[stride + k];
+    row[c++] = f[2 * stride + k];
+  }
+  if (fields & B200_FIELD_IMAGE) {
+    const int img = image[k];
+    row[c++] = (double)((img & MD_IMGMASK) - MD_IMGMAX);
+    row[c++] = (double)(((img >> 10) & MD_IMGMASK) - MD_IMGMAX);
+    row[c++] = (double)(((img >> 20) & MD_IMGMASK) - MD_IMGMAX);
+  }
+}
+
 __global__ void k_unsort_scalar(int n, const int *__restrict__ orig, const double *__restrict__ a,
                                 double *__restrict__ out) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1028,6 +1069,43 @@ int b200_upload_atoms(b200_ctx *c, int n, const double *x, const double *v, cons
 }
 
 int b200_natoms(const b200_ctx *c) { return c ? c->n : 0; }
+
+int b200_gather(b200_ctx *c, int fields, int m, const int *idx, double *out) {
+  if (!c || !out || m < 0 || fields <= 0 ||
+      (fields & ~(B200_FIELD_X | B200_FIELD_V | B200_FIELD_F | B200_FIELD_IMAGE)))
+    return set_err(c, B200_ERR_ARG, "gather: bad fields or arguments");
+  if (!c->have_atoms) return set_err(c, B200_ERR_STATE, "no atoms uploaded");
+  if (!idx && m > c->n) return set_err(c, B200_ERR_ARG, "gather: %d rows of %d atoms", m, c->n);
+  if (m == 0) return B200_OK;
+  CK(cudaSetDevice(c->device));
+  const int ncols = 3 * (((fields & B200_FIELD_X) != 0) + ((fields & B200_FIELD_V) != 0) +
+                         ((fields & B200_FIELD_F) != 0) + ((fields & B200_FIELD_IMAGE) != 0));
+  const size_t obytes = (size_t)m * ncols * sizeof(double);
+  const bool dev_out = is_device_ptr(out);
+  const bool dev_idx = idx && is_device_ptr(idx);
+  char *st[2];
+  const size_t sb[2] = {dev_out ? 0 : obytes, (idx && !dev_idx) ? (size_t)m * sizeof(int) : 0};
+  int rc = xfer_parts(c, 2, sb, st);
+  if (rc) return rc;
+  double *dout = dev_out ? out : reinterpret_cast<double *>(st[0]);
+  const int *didx = idx;
+  if (idx && !dev_idx) {
+    CK(cudaMemcpyAsync(st[1], idx, (size_t)m * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    didx = reinterpret_cast<const int *>(st[1]);
+  }
+  CK(cudaMemsetAsync(c->status + ST_HALO_BAD, 0, sizeof(int), c->stream));
+  k_gather_cols<<<md_blocks(m, 256), 256, 0, c->stream>>>(m, c->n, c->stride, fields, ncols, didx,
+                                                          c->where, c->x4, c->v, c->f, c->image,
+                                                          dout, c->status);
+  c->launches++;
+  CK(cudaGetLastError());
+  if (!dev_out) CK(cudaMemcpyAsync(out, dout, obytes, cudaMemcpyDeviceToHost, c->stream));
+  rc = read_status(c);
+  if (rc) return rc;
+  if (c->status_host[ST_HALO_BAD])
+    return set_err(c, B200_ERR_ARG, "gather: an atom index is outside [0, %d)", c->n);
+  return B200_OK;
+}
 
 int b200_update_positions(b200_ctx *c, const double *x) {
   if (!c || !x) return B200_ERR_ARG;

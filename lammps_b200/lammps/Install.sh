@@ -9,7 +9,7 @@
 mode=$1
 files="b200_link.h b200_link.cpp pair_lj_cut_b200.h pair_lj_cut_b200.cpp
        pair_eam_b200.h pair_eam_b200.cpp fix_nve_b200.h fix_nve_b200.cpp
-       verlet_b200.h verlet_b200.cpp"
+       verlet_b200.h verlet_b200.cpp dump_custom_b200.h dump_custom_b200.cpp"
 
 if (test $mode = 1 || test $mode = 2) then
   if (test ! -e ../pair_eam.h) then

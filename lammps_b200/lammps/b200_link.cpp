@@ -52,22 +52,38 @@ B200Link::B200Link(LAMMPS *lmp) : Pointers(lmp) {
   nbuilt = -1;
   fbuf = NULL;
   ibuf = NULL;
+  img_applied = NULL;
+  gbuf = NULL;
   nbuf = 0;
+  stale = 0;
 }
 
 B200Link::~B200Link() {
   if (ctx) b200_destroy(ctx);
   memory->destroy(fbuf);
   memory->destroy(ibuf);
+  memory->destroy(img_applied);
+  memory->destroy(gbuf);
 }
 
 void B200Link::grow(int n) {
   if (n <= nbuf) return;
+  const int old = nbuf;
   nbuf = n + n / 4 + 16;
   memory->destroy(fbuf);
   memory->destroy(ibuf);
+  memory->destroy(gbuf);
   memory->create(fbuf, 3 * nbuf, "b200:fbuf");
   memory->create(ibuf, 3 * nbuf, "b200:ibuf");
+  memory->create(gbuf, 12 * nbuf, "b200:gbuf");
+  memory->grow(img_applied, 3 * nbuf, "b200:img_applied");
+  for (int k = 3 * old; k < 3 * nbuf; k++) img_applied[k] = 0;
+}
+
+void B200Link::reset_images() {
+  grow(atom->nlocal);
+  for (int k = 0; k < 3 * nbuf; k++) img_applied[k] = 0;
+  stale = 0;
 }
 
 void B200Link::check_supported(const char *style) {
@@ -209,17 +225,62 @@ void B200Link::download_state() {
     f[i][0] = fbuf[3 * i];
     f[i][1] = fbuf[3 * i + 1];
     f[i][2] = fbuf[3 * i + 2];
-    // the device counts box crossings since the upload; add them to the
-    // packed image flags (src/domain.cpp:478-560 convention)
-    imageint img = atom->image[i];
-    imageint ix = (img & IMGMASK) - IMGMAX + ibuf[3 * i];
-    imageint iy = (img >> IMGBITS & IMGMASK) - IMGMAX + ibuf[3 * i + 1];
-    imageint iz = (img >> IMG2BITS) - IMGMAX + ibuf[3 * i + 2];
-    atom->image[i] = ((imageint)(iz + IMGMAX) << IMG2BITS) |
-                     ((imageint)(iy + IMGMAX) << IMGBITS) | (imageint)(ix + IMGMAX);
   }
+  apply_images(ibuf);
+  stale = 0;
   long long total = 0;
   int ncalls = 0, ndanger = 0, maxneigh = 0, cap = 0;
   check(b200_neigh_stats(ctx, &total, &ncalls, &ndanger, &maxneigh, &cap), "neigh_stats");
   if (maxneigh > neighbor->oneatom) check(B200_ERR_NEIGH_OVERFLOW, "run");
+}
+
+/* The device counts each atom's box crossings since the upload; add to the
+   packed image flags (src/domain.cpp:478-560 convention) the crossings not
+   yet added by an earlier download of the same run.  img[3i..3i+2] are the
+   device's counts of atom i. */
+void B200Link::apply_images(const int *img) {
+  const int n = atom->nlocal;
+  for (int i = 0; i < n; i++) {
+    int d[3];
+    for (int k = 0; k < 3; k++) {
+      d[k] = img[3 * i + k] - img_applied[3 * i + k];
+      img_applied[3 * i + k] = img[3 * i + k];
+    }
+    imageint im = atom->image[i];
+    imageint ix = (im & IMGMASK) - IMGMAX + d[0];
+    imageint iy = (im >> IMGBITS & IMGMASK) - IMGMAX + d[1];
+    imageint iz = (im >> IMG2BITS) - IMGMAX + d[2];
+    atom->image[i] = ((imageint)(iz + IMGMAX) << IMG2BITS) |
+                     ((imageint)(iy + IMGMAX) << IMGBITS) | (imageint)(ix + IMGMAX);
+  }
+}
+
+void B200Link::refresh(int fields) {
+  const int need = fields & stale;
+  if (!need || !ctx) return;
+  const int n = atom->nlocal;
+  grow(n);
+  int ncol = 0;
+  for (int b = 1; b <= B200_FIELD_IMAGE; b <<= 1)
+    if (need & b) ncol += 3;
+  if (n > 0) check(b200_gather(ctx, need, n, NULL, gbuf), "gather");
+  int c = 0;
+  double **arr[3] = {atom->x, atom->v, atom->f};
+  const int bit[3] = {B200_FIELD_X, B200_FIELD_V, B200_FIELD_F};
+  for (int g = 0; g < 3; g++) {
+    if (!(need & bit[g])) continue;
+    double **a = arr[g];
+    for (int i = 0; i < n; i++) {
+      a[i][0] = gbuf[(size_t)ncol * i + c];
+      a[i][1] = gbuf[(size_t)ncol * i + c + 1];
+      a[i][2] = gbuf[(size_t)ncol * i + c + 2];
+    }
+    c += 3;
+  }
+  if (need & B200_FIELD_IMAGE) {
+    for (int i = 0; i < n; i++)
+      for (int k = 0; k < 3; k++) ibuf[3 * i + k] = (int)gbuf[(size_t)ncol * i + c + k];
+    apply_images(ibuf);
+  }
+  stale &= ~need;
 }

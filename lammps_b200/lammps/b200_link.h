@@ -72,6 +72,14 @@ class B200Link : protected Pointers {
 
   /* resident mode: host x, v, f and image flags from the device */
   void download_state();
+  /* resident mode: bring the host arrays of the B200_FIELD_* groups in
+     `fields` that are behind the device (stale) up to date -- only those
+     columns cross PCIe, gathered on the device (b200_gather) */
+  void refresh(int fields);
+  /* groups of host arrays behind the device after a partial download */
+  int stale;
+  /* atoms uploaded for a resident run: restart the image-flag bookkeeping */
+  void reset_images();
 
   b200_ctx *ctx;
   int ctx_precision;
@@ -83,8 +91,11 @@ class B200Link : protected Pointers {
  private:
   double *fbuf;       // nlocal*3 forces in caller order
   int *ibuf;          // tags as int, image triplets
+  int *img_applied;   // per atom, the device's box crossings already added to atom->image
+  double *gbuf;       // gathered columns, nlocal x up to 12
   int nbuf;
   void grow(int n);
+  void apply_images(const int *img);
 };
 
 }

@@ -7,6 +7,8 @@
 
 #include "b200_link.h"
 #include "b200md.h"
+#include "dump_custom_b200.h"
+#include "fix_nve_b200.h"
 #include "verlet_b200.h"
 
 #include "atom.h"
@@ -18,6 +20,7 @@
 #include "neighbor.h"
 #include "output.h"
 #include "pair.h"
+#include "thermo.h"
 #include "timer.h"
 #include "update.h"
 
@@ -37,7 +40,9 @@ void VerletB200::init() {
   tables = force->pair ? dynamic_cast<B200PairTables *>(force->pair) : NULL;
   resident = tables != NULL;
   if (atom->molecular || force->kspace || atom->rmass_flag) resident = 0;
-  if (modify->nfix != 1 || strcmp(modify->fix[0]->style, "nve/b200") != 0 ||
+  // by class: a fix created through the -sf b200 suffix keeps the style
+  // name it was given ("nve"), src/modify.cpp:715-727 and src/fix.cpp:46-47
+  if (modify->nfix != 1 || !dynamic_cast<FixNVEB200 *>(modify->fix[0]) ||
       modify->fix[0]->igroup != 0)
     resident = 0;
   if (modify->n_post_integrate || modify->n_pre_exchange || modify->n_pre_neighbor ||
@@ -61,6 +66,7 @@ void VerletB200::setup() {
   if (!resident) return;
   link->sync_settings(tables);
   link->upload_atoms(1);
+  link->reset_images();
   double row[9];
   link->check(b200_setup(link->ctx, row), "setup");
   ncalls0 = neighbor->ncalls;
@@ -86,8 +92,20 @@ void VerletB200::run(int n) {
     timer->stamp(TIME_PAIR);
     update->ntimestep = stop;
 
-    // host arrays and the pair's tallies for this step's output
-    link->download_state();
+    // host arrays and the pair's tallies for this step's output: at the end
+    // of the run all of them; on an output step, the velocities that the
+    // default thermo reads (Temp, Press), and the rest only when an output
+    // other than `dump custom/b200` is due (which gathers its own columns)
+    if (stop == end || !output_needs_velocities_only(stop)) {
+      link->download_state();
+    } else {
+      link->stale = B200_FIELD_X | B200_FIELD_V | B200_FIELD_F | B200_FIELD_IMAGE;
+      link->refresh(B200_FIELD_V);
+      long long total = 0;
+      int nc = 0, nd = 0, maxneigh = 0, cap = 0;
+      link->check(b200_neigh_stats(ctx, &total, &nc, &nd, &maxneigh, &cap), "stats");
+      if (maxneigh > neighbor->oneatom) link->check(B200_ERR_NEIGH_OVERFLOW, "run");
+    }
     ev_set(stop);
     Pair *pair = force->pair;
     if (nrows > 0) {
@@ -106,4 +124,17 @@ void VerletB200::run(int n) {
       timer->stamp(TIME_OUTPUT);
     }
   }
+}
+
+/* true when the output due at `step` is the default thermo line (which reads
+   velocities, plus the pair's energy and virial taken from the device's
+   thermo row) and dumps of style custom/b200 only */
+int VerletB200::output_needs_velocities_only(bigint step) {
+  if (step != output->next) return 1;  // no output: the host is not read
+  if (output->restart_flag && output->next_restart == step) return 0;
+  if (output->next_thermo == step && strcmp(output->thermo->style, "one") != 0) return 0;
+  for (int i = 0; i < output->ndump; i++)
+    if (output->next_dump[i] == step && !dynamic_cast<DumpCustomB200 *>(output->dump[i]))
+      return 0;
+  return 1;
 }

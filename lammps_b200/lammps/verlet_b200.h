@@ -37,6 +37,7 @@ class VerletB200 : public Verlet {
   class B200PairTables *tables;
   int resident;
   bigint ncalls0, ndanger0;  // host neighbor counters at setup
+  int output_needs_velocities_only(bigint step);
 };
 
 }

@@ -155,6 +155,27 @@ class System:
                                              _abi.dptr(out["f"]), _abi.iptr(out["image"])))
         return out
 
+    def gather(self, fields=("x", "v", "f", "image"), idx=None):
+        """Per-atom columns straight from the device, as a dump writes them:
+        {group: (m, 3) array} for the requested groups of atoms idx (caller
+        indices; all atoms when None).  Image flags count box crossings since
+        the upload."""
+        order = [k for k in ("x", "v", "f", "image") if k in fields]
+        if not order or len(order) != len(set(fields)):
+            raise ValueError(f"gather: fields from x, v, f, image, not {fields}")
+        bits = sum(_abi.FIELDS[k] for k in order)
+        if idx is None:
+            m, ip = self.n, None
+        else:
+            ii = np.ascontiguousarray(idx, dtype=np.int32)
+            m, ip = len(ii), _abi.iptr(ii)
+        out = np.zeros((m, 3 * len(order)))
+        self._ck(self._L.b200_gather(self._h, bits, m, ip, _abi.dptr(out)))
+        res = {k: out[:, 3 * c:3 * c + 3] for c, k in enumerate(order)}
+        if "image" in res:
+            res["image"] = res["image"].astype(np.int32)
+        return res
+
     def update_positions(self, x):
         """New positions (caller order) keeping the cells and the neighbor
         list of the last build (a Pair::compute between reneighborings)."""

@@ -16,6 +16,7 @@ reference's Verlet::run, following its reneighbor schedule) and resident
 import json
 import os
 
+import numpy as np
 import pytest
 
 from lammps_runs import GOLDEN, input_script, parse_log, run_lammps
@@ -107,3 +108,48 @@ def test_mixed_precision_keyword(name, tmp_path):
     text, out = _run(case, tmp_path, "resident", "mixed")
     assert "mixed precision" in text
     _golden(case, out, exact=False, rel=1e-5)
+
+
+@needs_binary
+@pytest.mark.parametrize("name", ["bench_lj", "bench_eam"])
+def test_dump_custom_b200_matches_reference_dump(name, tmp_path):
+    """`dump custom/b200` in a resident run (its columns gathered on the
+    device at the output steps between the run's ends) against `dump custom`
+    of the reference's own binary on the same input: positions, velocities
+    and forces at steps 0, 50 and 100, and the image flags, which count the
+    box crossings of the whole run."""
+    from lammps_runs import read_dump
+    ref_exe = build_ref.lmp_serial()
+    if ref_exe is None:
+        pytest.skip("reference binary not built")
+    case = LOGS[name]
+    cols = "id x y z vx vy vz fx fy fz ix iy iz"
+    fmt = "\"%d" + " %.17g" * 9 + " %d %d %d\""
+
+    def script(style):
+        st = _styles(case, "resident")
+        extra = [f"dump d all {style} 50 dump.txt {cols}", f"dump_modify d sort id format {fmt}"]
+        if style == "custom":
+            return input_script(case, extra=extra)
+        if case["pair"]["style"] == "lj/cut":
+            sc = input_script(case, fix=st["fix"], run_style=st["run_style"], extra=extra)
+            return sc.replace("pair_style lj/cut ", "pair_style lj/cut/b200 ")
+        return input_script(case, pair_style=st["pair_style"], fix=st["fix"],
+                            run_style=st["run_style"], extra=extra)
+
+    run_lammps(ref_exe, script("custom"), str(tmp_path / "ref"))
+    text = run_lammps(LMP, script("custom/b200"), str(tmp_path / "b200"), env=ENV)
+    assert "resident mode" in text
+    ref = read_dump(str(tmp_path / "ref" / "dump.txt"))
+    got = read_dump(str(tmp_path / "b200" / "dump.txt"))
+    assert sorted(ref) == sorted(got) == [0, 50, 100]
+    for step in (0, 50, 100):
+        r, g = ref[step], got[step]
+        assert np.array_equal(r[:, 0], g[:, 0])
+        assert np.array_equal(r[:, 10:13], g[:, 10:13]), step  # image flags
+        for c0, what in ((1, "x"), (4, "v"), (7, "f")):
+            a, b = g[:, c0:c0 + 3], r[:, c0:c0 + 3]
+            err = np.linalg.norm(a - b) / np.linalg.norm(b)
+            assert err <= 1e-9, (step, what, err)
+    # some atoms crossed the box during the run
+    assert np.abs(ref[100][:, 10:13]).sum() > 0

@@ -41,11 +41,11 @@ def test_every_style_header_registers_a_style():
     for h in glob.glob(os.path.join(PKG, "*.h")):
         with open(h) as fh:
             for line in fh:
-                for kind in ("PairStyle(", "FixStyle(", "IntegrateStyle("):
+                for kind in ("PairStyle(", "FixStyle(", "IntegrateStyle(", "DumpStyle("):
                     if line.startswith(kind):
                         styles[line[len(kind):].split(",")[0]] = os.path.basename(h)
     assert set(styles) == {"lj/cut/b200", "eam/b200", "eam/alloy/b200", "eam/fs/b200",
-                           "nve/b200", "verlet/b200"}
+                           "nve/b200", "verlet/b200", "custom/b200"}
 
 
 def test_install_script_round_trip(tmp_path):
