@@ -259,6 +259,24 @@ int b200_neigh_check(b200_ctx *ctx, int *moved);
 int b200_halo_pack(b200_ctx *ctx, int m, const int *idx, double *buf);
 int b200_halo_unpack(b200_ctx *ctx, int m, const int *idx, const double *buf);
 
+/* PairEAM::compute in two calls around the forward communication of F'(rho)
+   (src/MANYBODY/pair_eam.cpp:160-232, then :237-303), for a context whose
+   ghosts get F' from their owners -- the split of the GPU package's
+   eam_gpu_compute / eam_gpu_compute_force with its fp_ptr
+   (lib/gpu/lal_eam_ext.cpp:122,133).  b200_eam_density: rho, F'(rho) and the
+   embedding energy of every atom (a ghost's F' is then overwritten by
+   b200_eam_fp_unpack).  b200_eam_fp_pack / unpack: F' of the caller atoms
+   idx[0..m) to / from buf[m] (DEVICE pointers; PairEAM::pack_forward_comm /
+   unpack_forward_comm, src/MANYBODY/pair_eam.cpp:809-831); unpack writes
+   ghosts only when ghosts are marked.  b200_eam_force: forces, with energy
+   and virial as b200_pair_compute, completing the tallies of the density
+   call; it must follow a b200_eam_density with the same eflag and vflag. */
+int b200_eam_density(b200_ctx *ctx, int eflag, int vflag);
+int b200_eam_fp_pack(b200_ctx *ctx, int m, const int *idx, double *buf);
+int b200_eam_fp_unpack(b200_ctx *ctx, int m, const int *idx, const double *buf);
+int b200_eam_force(b200_ctx *ctx, int eflag, int vflag, double *eng, double virial[6],
+                   double *eatom, double *vatom);
+
 /* ---- batched replicas ---------------------------------------------------- */
 
 /* No counterpart in the reference (which runs one box per process): make the

@@ -43,6 +43,10 @@ SIGNATURES = {
     "b200_natoms": (C.c_int, [_vp]),
     "b200_update_positions": (C.c_int, [_vp, _dp]),
     "b200_gather": (C.c_int, [_vp, C.c_int, C.c_int, _ip, _dp]),
+    "b200_eam_density": (C.c_int, [_vp, C.c_int, C.c_int]),
+    "b200_eam_fp_pack": (C.c_int, [_vp, C.c_int, _vp, _vp]),
+    "b200_eam_fp_unpack": (C.c_int, [_vp, C.c_int, _vp, _vp]),
+    "b200_eam_force": (C.c_int, [_vp, C.c_int, C.c_int, _dp, _dp, _dp, _dp]),
     "b200_neigh_build": (C.c_int, [_vp]),
     "b200_pair_compute": (C.c_int, [_vp, C.c_int, C.c_int, _dp, _dp, _dp, _dp]),
     "b200_nve_initial": (C.c_int, [_vp, C.c_double, C.c_double]),

@@ -15,10 +15,12 @@ How it differs from the reference, and why:
 
 - Full neighbor lists with owner-only force writes, so no reverse
   communication of forces (CommBrick::reverse_comm, src/comm_brick.cpp:513).
-- For EAM the ghost depth is twice the list cutoff: every ghost within the
-  list cutoff of the brick then has its whole neighborhood on the rank and
-  gets its own density, so the forward communication of F'(rho) in
-  PairEAM::compute (src/MANYBODY/pair_eam.cpp:232) is not needed.
+- The ghost depth is the list cutoff for every pair style.  For EAM a step
+  computes rho and F'(rho) of all atoms, then forwards each owner's F' to its
+  ghosts, then computes forces -- the forward communication of
+  PairEAM::compute (src/MANYBODY/pair_eam.cpp:232, pack/unpack_forward_comm
+  :809-831).  The reverse communication of rho (:206) is not needed: an owned
+  atom's full list holds all its neighbors.
 - A rank orders its atoms (owned and ghost) by global id.  The builder orders
   each cell by caller index, so every owned atom's neighbor list holds the
   same entries in the same order as in the single box: forces, and with them
@@ -250,7 +252,9 @@ class BrickRun:
         e0 = engines[comm.ranks[0]]
         self.every, self.delay, self.check = e0.every, e0.delay, e0.check
         self.cutneigh = e0.cutforce() + e0.skin
-        self.depth = self.cutneigh * (2.0 if isinstance(e0.pair, PairEAM) else 1.0)
+        self.depth = self.cutneigh
+        # EAM over several bricks: F' of the ghosts comes from their owners
+        self.fp_halo = isinstance(getattr(e0, "pair", None), PairEAM) and comm.world > 1
         self.mass = np.asarray(e0.mass, dtype=np.float64)
         self.e0 = e0
         self.natoms = 0
@@ -395,6 +399,18 @@ class BrickRun:
                 torch.cuda.current_stream(s.dev).synchronize()
             s.engine.halo_unpack(s.recv_idx, buf.contiguous())
 
+    # ---- CommBrick::forward_comm_pair (F' of EAM) -------------------------------
+    def _forward_fp(self):
+        send, cnt, rcnt = {}, {}, {}
+        for r, s in self.st.items():
+            buf = torch.empty(len(s.send_idx), dtype=torch.float64, device=s.dev)
+            s.engine.eam_fp_pack(s.send_idx, buf)
+            send[r], cnt[r], rcnt[r] = buf.reshape(-1, 1), s.send_counts, s.recv_counts
+        got = self.comm.alltoall_rows(send, cnt, rcnt)
+        for r, (buf, _) in got.items():
+            s = self.st[r]
+            s.engine.eam_fp_unpack(s.recv_idx, buf.reshape(-1).contiguous())
+
     # ---- Neighbor::decide ------------------------------------------------------
     def _decide(self, moved):
         self.ago += 1
@@ -410,9 +426,15 @@ class BrickRun:
     # ---- thermo ----------------------------------------------------------------
     def _force(self, thermo):
         rows = {}
+        if self.fp_halo:
+            for s in self.st.values():
+                s.engine.eam_density(2 if thermo else 0, 4 if thermo else 0)
+            self._forward_fp()
         for r, s in self.st.items():
-            if thermo:
-                o = s.engine.compute_dev()
+            if self.fp_halo and not thermo:
+                s.engine.eam_force(0, 0)
+            elif thermo:
+                o = s.engine.eam_force_dev() if self.fp_halo else s.engine.compute_dev()
                 own = ~s.ghost
                 rows[r] = torch.cat([torch.zeros(1, dtype=torch.float64, device=s.dev),
                                      o["eatom"][own].sum().reshape(1),

@@ -797,6 +797,7 @@ int b200_destroy(b200_ctx *c) {
   dfree(c->orig); dfree(c->origb); dfree(c->image); dfree(c->imageb); dfree(c->cell);
   dfree(c->where); dfree(c->ghost);
   dfree(c->xr); dfree(c->xhold); dfree(c->xfer); dfree(c->rho); dfree(c->fp); dfree(c->fpf); dfree(c->mass_dev);
+  dfree(c->eam_eatom);
   dfree(c->cell_count); dfree(c->cell_start); dfree(c->scan_tmp);
   dfree(c->slot); dfree(c->perm); dfree(c->cell_tmp);
   dfree(c->nlist); dfree(c->numneigh); dfree(c->partial); dfree(c->counter); dfree(c->ev);
@@ -1201,6 +1202,92 @@ int b200_pair_compute(b200_ctx *c, int eflag, int vflag, double *eng, double vir
   double h[8];
   if (ev) CK(cudaMemcpyAsync(h, c->ev, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   if (de) CK(cudaMemcpyAsync(eatom, de, (size_t)n * sizeof(double), cudaMemcpyDefault, c->stream));
+  if (dv) CK(cudaMemcpyAsync(vatom, dv, 6 * (size_t)n * sizeof(double), cudaMemcpyDefault, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (ev) {
+    if (eg && eng) *eng = h[0];
+    if (vg && virial)
+      for (int k = 0; k < 6; k++) virial[k] = h[1 + k];
+  }
+  return B200_OK;
+}
+
+// ---- EAM in two calls with the F'(rho) forward communication between them --
+
+static int eam_split_check(b200_ctx *c) {
+  if (!c) return B200_ERR_ARG;
+  if (!c->sorted_once) return set_err(c, B200_ERR_STATE, "neighbor list not built");
+  if (c->pstyle != B200_PAIR_EAM) return set_err(c, B200_ERR_STATE, "pair style is not eam");
+  CK(cudaSetDevice(c->device));
+  return B200_OK;
+}
+
+int b200_eam_density(b200_ctx *c, int eflag, int vflag) {
+  int rc = eam_split_check(c);
+  if (rc) return rc;
+  const bool eg = (eflag & 1) != 0, ea = (eflag & 2) != 0;
+  const bool vg = (vflag % 4) != 0, va = (vflag & 4) != 0;
+  if (ea && c->eam_eatom_n < c->n) {
+    dfree(c->eam_eatom);
+    CK(dalloc(&c->eam_eatom, (size_t)c->nalloc));
+    c->eam_eatom_n = c->nalloc;
+  }
+  CK(md_eam_compute(c, eg || ea || vg || va, ea || va, ea ? c->eam_eatom : nullptr, nullptr,
+                    nullptr, EAM_DENSITY));
+  CK(cudaStreamSynchronize(c->stream));
+  c->eam_split_eflag = eflag;
+  c->eam_split_vflag = vflag;
+  return B200_OK;
+}
+
+static int eam_fp_call(b200_ctx *c, int m, const int *idx, double *buf, bool pack) {
+  int rc = eam_split_check(c);
+  if (rc) return rc;
+  if (m < 0 || (m > 0 && (!idx || !buf))) return set_err(c, B200_ERR_ARG, "Illegal F' halo");
+  if (m == 0) return B200_OK;
+  CK(cudaMemsetAsync(c->status + ST_HALO_BAD, 0, sizeof(int), c->stream));
+  CK(md_eam_fp_halo(c, m, idx, buf, pack));
+  rc = read_status(c);
+  if (rc) return rc;
+  if (c->status_host[ST_HALO_BAD] == 2)
+    return set_err(c, B200_ERR_ARG, "F' unpack: an index names an owned atom, not a ghost");
+  if (c->status_host[ST_HALO_BAD])
+    return set_err(c, B200_ERR_ARG, "F' %s: an atom index is outside [0, %d)",
+                   pack ? "pack" : "unpack", c->n);
+  return B200_OK;
+}
+
+int b200_eam_fp_pack(b200_ctx *c, int m, const int *idx, double *buf) {
+  return eam_fp_call(c, m, idx, buf, true);
+}
+
+int b200_eam_fp_unpack(b200_ctx *c, int m, const int *idx, const double *buf) {
+  return eam_fp_call(c, m, idx, const_cast<double *>(buf), false);
+}
+
+int b200_eam_force(b200_ctx *c, int eflag, int vflag, double *eng, double virial[6],
+                   double *eatom, double *vatom) {
+  int rc = eam_split_check(c);
+  if (rc) return rc;
+  if (c->eam_split_eflag != eflag || c->eam_split_vflag != vflag)
+    return set_err(c, B200_ERR_STATE,
+                   "b200_eam_force needs a b200_eam_density call with the same flags before it");
+  c->eam_split_eflag = c->eam_split_vflag = -1;
+  const bool eg = (eflag & 1) != 0, ea = (eflag & 2) != 0;
+  const bool vg = (vflag % 4) != 0, va = (vflag & 4) != 0;
+  const bool ev = eg || ea || vg || va;
+  const int n = c->n;
+  char *st[1];
+  const size_t sb[1] = {(va && vatom) ? 6 * (size_t)n * sizeof(double) : 0};
+  rc = xfer_parts(c, 1, sb, st);
+  if (rc) return rc;
+  double *dv = reinterpret_cast<double *>(st[0]);
+  CK(md_eam_compute(c, ev, ea || va, ea ? c->eam_eatom : nullptr, dv, nullptr, EAM_FORCE));
+  double h[8];
+  if (ev) CK(cudaMemcpyAsync(h, c->ev, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (ea && eatom)
+    CK(cudaMemcpyAsync(eatom, c->eam_eatom, (size_t)n * sizeof(double), cudaMemcpyDefault,
+                       c->stream));
   if (dv) CK(cudaMemcpyAsync(vatom, dv, 6 * (size_t)n * sizeof(double), cudaMemcpyDefault, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   if (ev) {

@@ -108,6 +108,11 @@ struct b200_ctx {
   size_t xfer_bytes = 0;
   double *rho = nullptr, *fp = nullptr;
   float *fpf = nullptr;
+  // split EAM compute (b200_eam_density, then b200_eam_force): the eflag /
+  // vflag of the density call and its per-atom embedding energies
+  int eam_split_eflag = -1, eam_split_vflag = -1;
+  double *eam_eatom = nullptr;  // caller order, n doubles
+  int eam_eatom_n = 0;
   double *mass_dev = nullptr; // per-type masses (device)
   bool have_atoms = false, sorted_once = false;
 
@@ -200,9 +205,16 @@ cudaError_t md_halo_unpack(b200_ctx *c, int m, const int *idx, const double *buf
 cudaError_t md_set_positions(b200_ctx *c, const double *x);
 // ---- pair kernels (pair_lj.cu, pair_eam.cu) --------------------------------
 cudaError_t md_lj_compute(b200_ctx *c, bool ev, bool atom_ev, double *eatom, double *vatom);
-// `mid`, when given, is recorded between the density and the force kernel
+// `mid`, when given, is recorded between the density and the force kernel;
+// `stage` runs both passes or one of them (the density pass sets the global
+// energy/virial sums and the per-atom embedding energies, the force pass
+// adds its pair terms to them)
+enum { EAM_BOTH = 0, EAM_DENSITY = 1, EAM_FORCE = 2 };
 cudaError_t md_eam_compute(b200_ctx *c, bool ev, bool atom_ev, double *eatom, double *vatom,
-                           cudaEvent_t mid = nullptr);
+                           cudaEvent_t mid = nullptr, int stage = EAM_BOTH);
+// F'(rho) of the caller atoms idx[0..m) to buf (pack) or from it (unpack,
+// ghosts only when ghosts are marked); idx and buf on the device
+cudaError_t md_eam_fp_halo(b200_ctx *c, int m, const int *idx, double *buf, bool pack);
 // ---- integration (integrate.cu) --------------------------------------------
 cudaError_t md_nve_initial(b200_ctx *c, double dtv, double dtf);
 cudaError_t md_decide(b200_ctx *c);

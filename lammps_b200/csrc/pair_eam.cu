@@ -450,40 +450,95 @@ void record_mid(b200_ctx *c, cudaEvent_t mid) {
     cudaEventRecord(mid, c->stream);
 }
 
+// stage: EAM_BOTH, or EAM_DENSITY (passes 1-2) / EAM_FORCE (pass 3) alone
 template <int TPA, bool EV, bool ATOM, bool SINGLE>
-void launch_t(b200_ctx *c, const EamArgs &a, cudaEvent_t mid) {
+void launch_t(b200_ctx *c, const EamArgs &a, cudaEvent_t mid, int stage) {
   const int B = 128;
   const int grid = md_blocks((long long)a.n * TPA, B);
-  if (c->prec == B200_PREC_MIXED) {
-    k_eam_rho<TPA, EV, ATOM, true, SINGLE><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
-    record_mid(c, mid);
-    k_eam_force<TPA, EV, ATOM, true, SINGLE><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
-  } else {
-    k_eam_rho<TPA, EV, ATOM, false, SINGLE><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
-    record_mid(c, mid);
-    k_eam_force<TPA, EV, ATOM, false, SINGLE><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
+  if (stage != EAM_FORCE) {
+    if (c->prec == B200_PREC_MIXED)
+      k_eam_rho<TPA, EV, ATOM, true, SINGLE><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
+    else
+      k_eam_rho<TPA, EV, ATOM, false, SINGLE><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
+    c->launches++;
   }
-  c->launches += 2;
+  record_mid(c, mid);
+  if (stage != EAM_DENSITY) {
+    if (c->prec == B200_PREC_MIXED)
+      k_eam_force<TPA, EV, ATOM, true, SINGLE><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
+    else
+      k_eam_force<TPA, EV, ATOM, false, SINGLE><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
+    c->launches++;
+  }
 }
 
 template <int TPA, bool SINGLE>
-void launch_ts(b200_ctx *c, const EamArgs &a, bool ev, bool atom, cudaEvent_t mid) {
-  if (!ev) launch_t<TPA, false, false, SINGLE>(c, a, mid);
-  else if (!atom) launch_t<TPA, true, false, SINGLE>(c, a, mid);
-  else launch_t<TPA, true, true, SINGLE>(c, a, mid);
+void launch_ts(b200_ctx *c, const EamArgs &a, bool ev, bool atom, cudaEvent_t mid, int stage) {
+  if (!ev) launch_t<TPA, false, false, SINGLE>(c, a, mid, stage);
+  else if (!atom) launch_t<TPA, true, false, SINGLE>(c, a, mid, stage);
+  else launch_t<TPA, true, true, SINGLE>(c, a, mid, stage);
 }
 
 template <int TPA>
-void launch_tpa(b200_ctx *c, const EamArgs &a, bool ev, bool atom, cudaEvent_t mid) {
+void launch_tpa(b200_ctx *c, const EamArgs &a, bool ev, bool atom, cudaEvent_t mid, int stage) {
   // one element type: spline rows hoisted out of the pair loop (mixed form)
-  if (c->ntypes == 1) launch_ts<TPA, true>(c, a, ev, atom, mid);
-  else launch_ts<TPA, false>(c, a, ev, atom, mid);
+  if (c->ntypes == 1) launch_ts<TPA, true>(c, a, ev, atom, mid, stage);
+  else launch_ts<TPA, false>(c, a, ev, atom, mid, stage);
+}
+
+// F'(rho) of caller atoms idx[i] into / from buf[i] (PairEAM::pack_forward_comm
+// / unpack_forward_comm, src/MANYBODY/pair_eam.cpp:809-831); unpack also
+// sets the FP32 copy the mixed force pass reads
+__global__ void k_fp_pack(int m, int n, const int *__restrict__ idx, const int *__restrict__ where,
+                          const double *__restrict__ fp, double *__restrict__ buf,
+                          int *__restrict__ status) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const int j = idx[i];
+  if (j < 0 || j >= n) {
+    atomicExch(&status[ST_HALO_BAD], 1);
+    return;
+  }
+  buf[i] = fp[where[j]];
+}
+
+__global__ void k_fp_unpack(int m, int n, const int *__restrict__ idx,
+                            const int *__restrict__ where, const int *__restrict__ ghost,
+                            const double *__restrict__ buf, double *__restrict__ fp,
+                            float *__restrict__ fpf, int *__restrict__ status) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const int j = idx[i];
+  if (j < 0 || j >= n) {
+    atomicExch(&status[ST_HALO_BAD], 1);
+    return;
+  }
+  if (ghost && ghost[j] == 0) {  // owned atoms keep their own F'
+    atomicExch(&status[ST_HALO_BAD], 2);
+    return;
+  }
+  const int k = where[j];
+  fp[k] = buf[i];
+  if (fpf) fpf[k] = (float)buf[i];
 }
 
 }  // namespace
 
+cudaError_t md_eam_fp_halo(b200_ctx *c, int m, const int *idx, double *buf, bool pack) {
+  if (m < 1) return cudaSuccess;
+  if (pack)
+    k_fp_pack<<<md_blocks(m, 256), 256, 0, c->stream>>>(m, c->n, idx, c->where, c->fp, buf,
+                                                        c->status);
+  else
+    k_fp_unpack<<<md_blocks(m, 256), 256, 0, c->stream>>>(
+        m, c->n, idx, c->where, c->ghosts_on ? c->ghost : nullptr, buf, c->fp,
+        c->prec == B200_PREC_MIXED ? c->fpf : nullptr, c->status);
+  c->launches++;
+  return cudaGetLastError();
+}
+
 cudaError_t md_eam_compute(b200_ctx *c, bool ev, bool atom_ev, double *eatom, double *vatom,
-                           cudaEvent_t mid) {
+                           cudaEvent_t mid, int stage) {
   EamArgs a;
   a.n = c->n;
   a.stride = c->stride;
@@ -521,12 +576,12 @@ cudaError_t md_eam_compute(b200_ctx *c, bool ev, bool atom_ev, double *eatom, do
   a.eatom = eatom;
   a.vatom = vatom;
   switch (c->tpa) {
-    case 1: launch_tpa<1>(c, a, ev, atom_ev, mid); break;
-    case 2: launch_tpa<2>(c, a, ev, atom_ev, mid); break;
-    case 4: launch_tpa<4>(c, a, ev, atom_ev, mid); break;
-    case 8: launch_tpa<8>(c, a, ev, atom_ev, mid); break;
-    case 16: launch_tpa<16>(c, a, ev, atom_ev, mid); break;
-    default: launch_tpa<32>(c, a, ev, atom_ev, mid); break;
+    case 1: launch_tpa<1>(c, a, ev, atom_ev, mid, stage); break;
+    case 2: launch_tpa<2>(c, a, ev, atom_ev, mid, stage); break;
+    case 4: launch_tpa<4>(c, a, ev, atom_ev, mid, stage); break;
+    case 8: launch_tpa<8>(c, a, ev, atom_ev, mid, stage); break;
+    case 16: launch_tpa<16>(c, a, ev, atom_ev, mid, stage); break;
+    default: launch_tpa<32>(c, a, ev, atom_ev, mid, stage); break;
   }
   return cudaGetLastError();
 }

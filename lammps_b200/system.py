@@ -262,6 +262,48 @@ class System:
                                            _abi.tdptr(va)))
         return dict(eatom=ea, vatom=va)
 
+    # split EAM compute around the forward communication of F'(rho)
+    def eam_density(self, eflag=0, vflag=0):
+        """Passes 1-2 of PairEAM::compute: rho, F'(rho), embedding energy."""
+        self._ck(self._L.b200_eam_density(self._h, eflag, vflag))
+
+    @staticmethod
+    def _fp_args(idx, buf):
+        if not (idx.is_cuda and buf.is_cuda and idx.dtype.itemsize == 4 and buf.is_contiguous()
+                and idx.is_contiguous() and buf.numel() == idx.numel()):
+            raise ValueError("F' halo: idx (m int32) and buf (m float64) must be contiguous CUDA tensors")
+        return idx.numel(), C.c_void_p(idx.data_ptr()), C.c_void_p(buf.data_ptr())
+
+    def eam_fp_pack(self, idx, buf):
+        """buf[i] = F' of atom idx[i] (device tensors)."""
+        m, pi, pb = self._fp_args(idx, buf)
+        self._torch_ready()
+        self._ck(self._L.b200_eam_fp_pack(self._h, m, pi, pb))
+
+    def eam_fp_unpack(self, idx, buf):
+        """F' of ghost atom idx[i] = buf[i] (device tensors)."""
+        m, pi, pb = self._fp_args(idx, buf)
+        self._torch_ready()
+        self._ck(self._L.b200_eam_fp_unpack(self._h, m, pi, pb))
+
+    def eam_force(self, eflag=0, vflag=0):
+        """Pass 3 of PairEAM::compute after eam_density with the same flags."""
+        eng = C.c_double(0.0)
+        vir = np.zeros(6)
+        self._ck(self._L.b200_eam_force(self._h, eflag, vflag, C.byref(eng), _abi.dptr(vir), None,
+                                        None))
+        return dict(eng=eng.value, virial=vir)
+
+    def eam_force_dev(self):
+        """Pass 3 with per-atom energy (n,) and virial (n, 6) as device
+        tensors; the density call must have had eflag 2, vflag 4."""
+        torch = _torch()
+        ea = torch.empty(self.n, dtype=torch.float64, device=self.device)
+        va = torch.empty((self.n, 6), dtype=torch.float64, device=self.device)
+        self._torch_ready()
+        self._ck(self._L.b200_eam_force(self._h, 2, 4, None, None, _abi.tdptr(ea), _abi.tdptr(va)))
+        return dict(eatom=ea, vatom=va)
+
     def neigh_check(self):
         """The local half of Neighbor::check_distance since the last call."""
         m = C.c_int(0)

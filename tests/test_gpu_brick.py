@@ -3,8 +3,10 @@ engine contexts on one GPU, stepped together in one process (`LocalComm`;
 the halo exchange is a device copy and no kernel waits on another).  Each
 owned atom sees the same neighbors in the same order as in the single box,
 so a decomposed run must reproduce the single-box trajectory bit for bit --
-for lj/cut and EAM, FP64 and mixed, through rebuilds (check yes) with
-exchange and borders, and the per-step halo pack / unpack in between."""
+for lj/cut and EAM (whose ghosts get F'(rho) from their owners between the
+density and force passes), FP64 and mixed, through rebuilds (check yes) with
+exchange and borders, and the per-step halo pack / unpack in between; and
+the decomposed run must match the oracle's serial run."""
 import os
 import socket
 
@@ -87,6 +89,46 @@ def test_bricks_reproduce_single_box(style, precision):
         for r1, r2 in zip(rows1, rows):
             for k in ("Temp", "E_pair", "Press"):
                 assert r2[k] == pytest.approx(r1[k], rel=1e-11, abs=1e-11), (grid, k)
+
+
+@pytest.mark.parametrize("style", ["lj", "eam"])
+def test_bricks_match_oracle(style):
+    """Two bricks (EAM with the forward communication of F'(rho) between the
+    density and force passes) against the oracle's serial run of the same
+    steps: positions, velocities and image flags after the run, the thermo
+    rows and the number of neighbor builds."""
+    import oracle
+    make, x, v, steps = (_lj if style == "lj" else _eam)("fp64")
+    b, rows, got = _brick((make, x, v, steps), (2, 1, 1))
+    e = make()
+    o = oracle.OracleSim("lj" if style == "lj" else "metal", threads=os.cpu_count() or 4)
+    o.box([0.0] * 3, e.box_hi)
+    o.atoms(x, v)
+    if style == "lj":
+        o.mass(1, 1.0)
+        o.lj_cut(2.5)
+        o.lj_coeff(1, 1, 1.0, 1.0, 2.5)
+        o.neighbor(0.3, 1, 0, True, 1000)
+    else:
+        o.eam_funcfl([os.path.join(ROOT, "tests", "golden", "Cu_u3.eam")], [0])
+        o.neighbor(1.0, 1, 5, True, 1000)
+    o.timestep(e.dt)
+    o.thermo(steps // 2)
+    o.setup()
+    o.run(steps)
+    order = np.argsort(o.tag)
+    for k in ("x", "v"):
+        ref = getattr(o, k)[order]
+        err = float(np.max(np.abs(got[k] - ref)))
+        assert err <= 1e-9, (k, err)
+    assert np.array_equal(got["image"], o.image[order])
+    assert b.ncalls == o.ncalls
+    orows = o.thermo_rows()
+    for r, orow in zip(rows, orows[1:]):
+        assert r["Step"] == int(orow[0])
+        for key, col in (("Temp", 1), ("E_pair", 2), ("Press", 4)):
+            assert r[key] == pytest.approx(orow[col], rel=1e-9, abs=1e-9), (r["Step"], key)
+    e.close()
 
 
 @pytest.mark.parametrize("style", ["lj", "eam"])

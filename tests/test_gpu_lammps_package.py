@@ -143,13 +143,19 @@ def test_dump_custom_b200_matches_reference_dump(name, tmp_path):
     ref = read_dump(str(tmp_path / "ref" / "dump.txt"))
     got = read_dump(str(tmp_path / "b200" / "dump.txt"))
     assert sorted(ref) == sorted(got) == [0, 50, 100]
+    # on the step-0 lattice the forces cancel to ~1e-13: their differences
+    # are measured against the RMS force of step 50
+    frms = float(np.sqrt(np.mean(np.sum(ref[50][:, 7:10] ** 2, axis=1))))
     for step in (0, 50, 100):
         r, g = ref[step], got[step]
         assert np.array_equal(r[:, 0], g[:, 0])
         assert np.array_equal(r[:, 10:13], g[:, 10:13]), step  # image flags
         for c0, what in ((1, "x"), (4, "v"), (7, "f")):
             a, b = g[:, c0:c0 + 3], r[:, c0:c0 + 3]
-            err = np.linalg.norm(a - b) / np.linalg.norm(b)
+            if step == 0 and what == "f":
+                err = float(np.abs(a - b).max()) / frms
+            else:
+                err = np.linalg.norm(a - b) / np.linalg.norm(b)
             assert err <= 1e-9, (step, what, err)
     # some atoms crossed the box during the run
     assert np.abs(ref[100][:, 10:13]).sum() > 0
