@@ -584,7 +584,12 @@ def replica_bench(prec, batch, torch, steps=1000, lat_steps=200):
     st = s.step_times(reset=True)
     s.set_timing(False)
     nrep = len(batch["natoms"])
+    form = s.replica_step()
     out = {"replica_steps_per_s": nrep * steps / (ms * 1e-3),
+           "step_form": ("one launch per step: clusters of %d CTAs x %d threads, %d thread(s) "
+                         "per atom" % (form["cluster"], form["block"], form["tpa"])
+                         if form["onelaunch"] else "graph of kernels per step"),
+           "tuned_ms_per_step": {"graph": form["graph_ms"], "one_launch": form["onelaunch_ms"]},
            "matom_steps_per_s": float(batch["natoms"].sum()) * steps / (ms * 1e3),
            "ms_per_step": ms / steps, "launch": s.launch(),
            "step_ms_p50": float(np.percentile(st, 50)), "step_ms_p99": float(np.percentile(st, 99))}

@@ -292,6 +292,23 @@ int b200_eam_force(b200_ctx *ctx, int eflag, int vflag, double *eng, double viri
 int b200_set_replicas(b200_ctx *ctx, int nrep, const int *natoms, const double *lo,
                       const double *hi);
 int b200_replica_count(const b200_ctx *ctx);
+/* Step form of a replica batch.  mode 1: a graph of kernels per MD step
+   (the pair kernel over every replica, then the fused half-steps).  mode 2:
+   one launch per MD step (between rebuilds and outputs): thread-block
+   clusters of `cluster` CTAs of `block` threads, each cluster owning a fixed
+   set of whole replicas balanced by atom count, compute their forces, meet at
+   a cluster barrier, and apply the final half-step and the next initial
+   half-step; the last CTA makes the rebuild decision.  `tpa` threads per
+   atom.  mode 0 (default): the next b200_setup times the graph path and every
+   one-launch shape (cluster 1/2/4, block 256/512, tpa 1/2/4; a nonzero
+   argument fixes that value) and keeps the fastest.  Both forms give the same
+   results bit for bit.  Applies from the next b200_setup. */
+int b200_set_replica_step(b200_ctx *ctx, int mode, int cluster, int block, int tpa);
+/* The form in use (*onelaunch 1 for the one-launch step) with its shape, and
+   ms[0], ms[1]: the per-step device time of the graph path and of the best
+   one-launch shape measured by the last tuning (0 when not measured). */
+int b200_get_replica_step(const b200_ctx *ctx, int *onelaunch, int *cluster, int *block, int *tpa,
+                          double *ms);
 /* Per-replica thermo of the current positions and velocities (forces are
    recomputed with per-atom energy and virial): rows[9r..9r+8] =
    {natoms, sum m v^2, eng_vdwl, virial[0..5]}, from which Temp, E_pair and

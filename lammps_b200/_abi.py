@@ -43,6 +43,8 @@ SIGNATURES = {
     "b200_natoms": (C.c_int, [_vp]),
     "b200_update_positions": (C.c_int, [_vp, _dp]),
     "b200_gather": (C.c_int, [_vp, C.c_int, C.c_int, _ip, _dp]),
+    "b200_set_replica_step": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int]),
+    "b200_get_replica_step": (C.c_int, [_vp, _ip, _ip, _ip, _ip, _dp]),
     "b200_eam_density": (C.c_int, [_vp, C.c_int, C.c_int]),
     "b200_eam_fp_pack": (C.c_int, [_vp, C.c_int, _vp, _vp]),
     "b200_eam_fp_unpack": (C.c_int, [_vp, C.c_int, _vp, _vp]),

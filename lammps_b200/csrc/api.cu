@@ -562,6 +562,11 @@ cudaError_t launch_piece(b200_ctx *c, int kind, double dtv, double dtf, cudaEven
     const bool out = kind == PIECE_POST_OUT || kind == PIECE_FUSED_OUT;
     const bool fused = kind == PIECE_FUSED_OUT || kind == PIECE_FUSED;
     if (ev) e = record(c, ev[0]);
+    if (kind == PIECE_FUSED && c->rep_onelaunch && c->nrep && c->pstyle == B200_PAIR_LJ_CUT) {
+      // replicas: this step's forces, final half-step and the next step's
+      // initial half-step and decision in one cluster launch
+      return md_rep_step(c, dtv, dtf);
+    }
     if (e == cudaSuccess) {
       if (c->pstyle == B200_PAIR_LJ_CUT) {
         e = md_lj_compute(c, out, false, nullptr, nullptr);
@@ -578,6 +583,79 @@ cudaError_t launch_piece(b200_ctx *c, int kind, double dtv, double dtf, cudaEven
     if (e == cudaSuccess && ev) e = record(c, ev[3]);
   }
   return e;
+}
+
+// Step form of a replica batch: device time per step of the graph path's
+// fused piece (pair kernel + fused half-steps) and of the one-launch step for
+// each cluster size, block size and threads per atom, keeping the fastest.
+// The steps are timed with a zero timestep, so positions and velocities do
+// not change; the step counters, rebuild schedule and decision mailbox that
+// the steps advance are put back afterwards.
+int tune_replica_step(b200_ctx *c) {
+  const bool lj = c->pstyle == B200_PAIR_LJ_CUT;
+  c->rep_onelaunch = false;
+  c->rep_tune_ms[0] = c->rep_tune_ms[1] = 0.0;
+  if (!c->nrep || !lj || c->rep_mode == 1) return B200_OK;
+  int status_save[ST_COUNT], dcount_save = 0;
+  CK(cudaMemcpyAsync(status_save, c->status, sizeof(status_save), cudaMemcpyDeviceToHost,
+                     c->stream));
+  CK(cudaMemcpyAsync(&dcount_save, c->dec_count, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  const int mail_save[2] = {c->mail_host[0], c->mail_host[1]};
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  const int steps = 16;
+  auto time_steps = [&](bool one, float *ms) -> int {
+    for (int r = 0; r < steps + 2; r++) {
+      if (r == 2) CK(cudaEventRecord(e0, c->stream));
+      CK(one ? md_rep_step(c, 0.0, 0.0) : launch_piece(c, PIECE_FUSED, 0.0, 0.0, nullptr));
+    }
+    CK(cudaEventRecord(e1, c->stream));
+    CK(cudaEventSynchronize(e1));
+    CK(cudaEventElapsedTime(ms, e0, e1));
+    *ms /= steps;
+    return B200_OK;
+  };
+  float graph_ms = 1e30f;
+  int rc = B200_OK;
+  if (c->rep_mode == 0) rc = time_steps(false, &graph_ms);
+  float best = 1e30f;
+  int bcs = 0, bblock = 0, btpa = 0;
+  const int cs_c[3] = {1, 2, 4}, bl_c[2] = {256, 512}, tp_c[3] = {1, 2, 4};
+  for (int a = 0; a < 3 && !rc; a++)
+    for (int b = 0; b < 2 && !rc; b++)
+      for (int t = 0; t < 3 && !rc; t++) {
+        if ((c->rep_fix_cs > 0 && cs_c[a] != c->rep_fix_cs) ||
+            (c->rep_fix_block > 0 && bl_c[b] != c->rep_fix_block) ||
+            (c->rep_fix_tpa > 0 && tp_c[t] != c->rep_fix_tpa))
+          continue;
+        rc = md_rep_plan(c, cs_c[a], bl_c[b], tp_c[t]);
+        float ms = 0.f;
+        if (!rc) rc = time_steps(true, &ms);
+        if (!rc && ms < best) {
+          best = ms;
+          bcs = cs_c[a];
+          bblock = bl_c[b];
+          btpa = tp_c[t];
+        }
+      }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (!rc && bcs) rc = md_rep_plan(c, bcs, bblock, btpa);
+  CK(cudaMemcpyAsync(c->status, status_save, sizeof(status_save), cudaMemcpyHostToDevice,
+                     c->stream));
+  CK(cudaMemcpyAsync(c->dec_count, &dcount_save, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->mail_host[0] = mail_save[0];
+  c->mail_host[1] = mail_save[1];
+  if (rc) return rc;
+  c->rep_tune_ms[0] = graph_ms < 1e29f ? graph_ms : 0.0;
+  c->rep_tune_ms[1] = best < 1e29f ? best : 0.0;
+  c->rep_onelaunch = bcs > 0 && (c->rep_mode == 2 || best < graph_ms);
+  c->rep_tuned = true;
+  invalidate_graphs(c);
+  return B200_OK;
 }
 
 int capture_piece(b200_ctx *c, int kind, double dtv, double dtf) {
@@ -797,7 +875,7 @@ int b200_destroy(b200_ctx *c) {
   dfree(c->orig); dfree(c->origb); dfree(c->image); dfree(c->imageb); dfree(c->cell);
   dfree(c->where); dfree(c->ghost);
   dfree(c->xr); dfree(c->xhold); dfree(c->xfer); dfree(c->rho); dfree(c->fp); dfree(c->fpf); dfree(c->mass_dev);
-  dfree(c->eam_eatom);
+  dfree(c->eam_eatom); dfree(c->d_rep_grp_first); dfree(c->d_rep_ranges);
   dfree(c->cell_count); dfree(c->cell_start); dfree(c->scan_tmp);
   dfree(c->slot); dfree(c->perm); dfree(c->cell_tmp);
   dfree(c->nlist); dfree(c->numneigh); dfree(c->partial); dfree(c->counter); dfree(c->ev);
@@ -1334,6 +1412,12 @@ int b200_setup(b200_ctx *c, double *row) {
     }
     c->tuned = true;
   }
+  if (c->nrep && !c->rep_tuned) {
+    // forces first: the tuning steps run the half-steps on them
+    rc = pair_compute_dev(c, false, false, nullptr, nullptr);
+    if (!rc) rc = tune_replica_step(c);
+    if (rc) return rc;
+  }
   rc = pair_compute_dev(c, true, false, nullptr, nullptr);
   if (rc) return rc;
   CK(md_ke(c));
@@ -1804,11 +1888,40 @@ int b200_set_replicas(b200_ctx *c, int nrep, const int *natoms, const double *lo
   c->box = c->rep_box[0];
   c->box_set = true;
   c->sorted_once = false;
+  c->rep_tuned = false;  // a new batch: its step form is chosen again
   invalidate_graphs(c);
   return B200_OK;
 }
 
 int b200_replica_count(const b200_ctx *c) { return c ? c->nrep : 0; }
+
+int b200_set_replica_step(b200_ctx *c, int mode, int cluster, int block, int tpa) {
+  if (!c || mode < 0 || mode > 2 || !(cluster == 0 || cluster == 1 || cluster == 2 || cluster == 4) ||
+      !(block == 0 || block == 256 || block == 512) || !(tpa == 0 || tpa == 1 || tpa == 2 || tpa == 4))
+    return set_err(c, B200_ERR_ARG, "Illegal replica step form");
+  c->rep_mode = mode;
+  c->rep_fix_cs = cluster;
+  c->rep_fix_block = block;
+  c->rep_fix_tpa = tpa;
+  c->rep_onelaunch = false;  // decided again by the next b200_setup
+  c->rep_tuned = false;
+  invalidate_graphs(c);
+  return B200_OK;
+}
+
+int b200_get_replica_step(const b200_ctx *c, int *onelaunch, int *cluster, int *block, int *tpa,
+                          double *ms) {
+  if (!c) return B200_ERR_ARG;
+  if (onelaunch) *onelaunch = c->rep_onelaunch ? 1 : 0;
+  if (cluster) *cluster = c->rep_cs;
+  if (block) *block = c->rep_block;
+  if (tpa) *tpa = c->rep_tpa;
+  if (ms) {
+    ms[0] = c->rep_tune_ms[0];
+    ms[1] = c->rep_tune_ms[1];
+  }
+  return B200_OK;
+}
 
 int b200_replica_thermo(b200_ctx *c, double *rows) {
   if (!c || !rows) return B200_ERR_ARG;

@@ -11,65 +11,12 @@
 
 namespace {
 
-// Neighbor::decide (src/neighbor.cpp:1294-1309) on the device: the host
-// mirrors the same schedule and reads ST_REBUILD only when the distance
-// criterion decides.
-__device__ __forceinline__ void decide_dev(int *status, int every, int delay, int check,
-                                           int *dcount, volatile int *mail) {
-  const int ago = status[ST_AGO] + 1;
-  status[ST_AGO] = ago;
-  int rebuild = 0;
-  const bool candidate = ago >= delay && ago % every == 0;
-  if (candidate) {
-    if (!check) rebuild = 1;
-    else {
-      rebuild = status[ST_MOVED] != 0;
-      if (rebuild && ago == (every > delay ? every : delay)) status[ST_NDANGER] += 1;
-    }
-  }
-  bool forced = false;
-  if (status[ST_FORCE_BUILD]) {  // replay after a list overflow: lists are stale
-    rebuild = 1;
-    forced = true;
-    status[ST_FORCE_BUILD] = 0;
-  }
-  status[ST_MOVED] = 0;
-  status[ST_REBUILD] = rebuild;
-  unsigned int lo = (unsigned int)status[ST_STEP_LO] + 1u;
-  if (lo == 0u) status[ST_STEP_HI] += 1;
-  status[ST_STEP_LO] = (int)lo;
-  if (check && candidate && !forced) {
-    // a decision the host waits for (the distance criterion): the flag
-    // first, then, after a system-wide fence, the new decision count
-    const int k = *dcount + 1;
-    *dcount = k;
-    mail[0] = rebuild;
-    __threadfence_system();
-    mail[1] = k;
-  }
-}
-
-__device__ __forceinline__ void record_row_dev(int *status, const double *ev, double *rows,
-                                               int cap) {
-  const int r = status[ST_ROW];
-  if (r < cap) {
-    double *row = rows + 9 * (size_t)r;
-    const long long step = ((long long)(unsigned int)status[ST_STEP_HI] << 32) |
-                           (long long)(unsigned int)status[ST_STEP_LO];
-    row[0] = (double)step;
-    row[1] = ev[7];
-    row[2] = ev[0];
-    for (int k = 0; k < 6; k++) row[3 + k] = ev[1 + k];
-  }
-  status[ST_ROW] = r + 1;
-}
-
 __global__ void k_decide(int *status, int every, int delay, int check, int *dcount, int *mail) {
-  decide_dev(status, every, delay, check, dcount, mail);
+  md_decide_dev(status, every, delay, check, dcount, mail);
 }
 
 __global__ void k_record_row(int *status, const double *ev, double *rows, int cap) {
-  record_row_dev(status, ev, rows, cap);
+  md_record_row_dev(status, ev, rows, cap);
 }
 
 template <bool BATCH>
@@ -176,40 +123,9 @@ __global__ void __launch_bounds__(256) k_nve_fused(int n, int stride, double dtv
   double acc[1] = {0.0};
   bool moved = false;
   if (i < n) {
-    double4 p = x4[i];
-    const double m = mass[(int)p.w];
-    const double dtfm = dtf / m;
-    const double fx = f[i], fy = f[stride + i], fz = f[2 * stride + i];
-    double vx = __dadd_rn(v[i], __dmul_rn(dtfm, fx));
-    double vy = __dadd_rn(v[stride + i], __dmul_rn(dtfm, fy));
-    double vz = __dadd_rn(v[2 * stride + i], __dmul_rn(dtfm, fz));
-    // ComputeTemp::compute_scalar term of this step (src/compute_temp.cpp:84-86)
-    if (KE) acc[0] = (vx * vx + vy * vy + vz * vz) * m;
-    vx = __dadd_rn(vx, __dmul_rn(dtfm, fx));
-    vy = __dadd_rn(vy, __dmul_rn(dtfm, fy));
-    vz = __dadd_rn(vz, __dmul_rn(dtfm, fz));
-    p.x = __dadd_rn(p.x, __dmul_rn(dtv, vx));
-    p.y = __dadd_rn(p.y, __dmul_rn(dtv, vy));
-    p.z = __dadd_rn(p.z, __dmul_rn(dtv, vz));
-    v[i] = vx;
-    v[stride + i] = vy;
-    v[2 * stride + i] = vz;
-    x4[i] = p;
-    if (xr) {
-      const BoxGeom &box = BATCH ? reps.box[reps.rep_of_atom[i]] : box1;
-      int cx, cy, cz;
-      md_cell_unpack(cell[i], cx, cy, cz);
-      const double ox = box.lo[0] + (cx + 0.5) * box.cs[0];
-      const double oy = box.lo[1] + (cy + 0.5) * box.cs[1];
-      const double oz = box.lo[2] + (cz + 0.5) * box.cs[2];
-      xr[i] = make_float4((float)(p.x - ox), (float)(p.y - oy), (float)(p.z - oz),
-                          __int_as_float((int)p.w));
-    }
-    if (xhold) {
-      const double4 h = xhold[i];
-      const double rsq = dsq3(__dsub_rn(p.x, h.x), __dsub_rn(p.y, h.y), __dsub_rn(p.z, h.z));
-      moved = rsq > triggersq;
-    }
+    const BoxGeom &box = BATCH ? reps.box[reps.rep_of_atom[i]] : box1;
+    moved = md_nve_fused_atom<KE>(i, stride, dtv, dtf, mass, x4, v, f, xr, cell, box, xhold,
+                                  triggersq, acc[0]);
   }
   if (xhold && __any_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0) {
     atomicExch(&status[ST_MOVED], 1);
@@ -233,8 +149,8 @@ __global__ void __launch_bounds__(256) k_nve_fused(int n, int stride, double dtv
     if (threadIdx.x == 0) ev[7] = s[0];
   }
   if (threadIdx.x == 0) {
-    if (KE) record_row_dev(status, ev, rows, rows_cap);
-    decide_dev(status, every, delay, check, dcount, mail);
+    if (KE) md_record_row_dev(status, ev, rows, rows_cap);
+    md_decide_dev(status, every, delay, check, dcount, mail);
     *counter = 0u;
   }
 }

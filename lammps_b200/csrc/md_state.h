@@ -163,6 +163,19 @@ struct b200_ctx {
   int tpa = 0, block = 128;
   bool tuned = false;
 
+  // one-launch replica step (b200_set_replica_step): each thread-block
+  // cluster of rep_cs CTAs of rep_block threads owns a fixed set of whole
+  // replicas (group g: atom ranges d_rep_ranges[d_rep_grp_first[g] ..
+  // d_rep_grp_first[g+1]) as (start, count)), balanced by atom count
+  int rep_mode = 0;       // 0 chosen on the next b200_setup, 1 graph of kernels, 2 one launch
+  int rep_fix_cs = 0, rep_fix_block = 0, rep_fix_tpa = 0;  // shapes fixed by the caller (0 = tuned)
+  bool rep_tuned = false;  // the form has been chosen for the current batch
+  bool rep_onelaunch = false;
+  int rep_cs = 0, rep_block = 0, rep_tpa = 0, rep_groups = 0;
+  int *d_rep_grp_first = nullptr;
+  int2 *d_rep_ranges = nullptr;
+  double rep_tune_ms[2] = {0, 0};  // per-step device time of the two forms when tuned
+
   // CUDA graph of one MD step (captured lazily by b200_run)
   // graphs of the step pieces: [0] initial half-step + decision, [1] rebuild,
   // [2] forces + final half-step with thermo output, [3] the same without
@@ -215,6 +228,12 @@ cudaError_t md_eam_compute(b200_ctx *c, bool ev, bool atom_ev, double *eatom, do
 // F'(rho) of the caller atoms idx[0..m) to buf (pack) or from it (unpack,
 // ghosts only when ghosts are marked); idx and buf on the device
 cudaError_t md_eam_fp_halo(b200_ctx *c, int m, const int *idx, double *buf, bool pack);
+// one-launch replica step (pair_lj.cu): this step's lj/cut forces, final
+// half-step and the next step's initial half-step and rebuild decision, for
+// every replica, in one cluster launch (non-output steps)
+cudaError_t md_rep_step(b200_ctx *c, double dtv, double dtf);
+// group plan of the one-launch step: cluster size cs, block size, groups
+int md_rep_plan(b200_ctx *c, int cs, int block, int tpa);
 // ---- integration (integrate.cu) --------------------------------------------
 cudaError_t md_nve_initial(b200_ctx *c, double dtv, double dtf);
 cudaError_t md_decide(b200_ctx *c);

@@ -20,6 +20,8 @@
 // (src/neigh_half_bin.cpp:355-360, src/atom_vec_atomic.cpp:297-299).
 #include <cstdio>
 
+#include <type_traits>
+
 #include "md_state.h"
 
 namespace {
@@ -300,10 +302,19 @@ __device__ __forceinline__ bool exact_pair(const double4 &xi, const double4 &xj,
   return dsq3(delx, dely, delz) <= cutsq;
 }
 
-// Shared memory of k_neigh_tiles: stage_cap + 32 float4 positions (32 spare
-// slots: a chunk may read past a row) and stage_cap int entries.
-static size_t neigh_smem(int stage_cap) {
-  return (size_t)(stage_cap + 32) * sizeof(float4) + (size_t)stage_cap * sizeof(int);
+// Shared memory of k_neigh_tiles: stage_cap + 32 float4 staged atoms (32
+// spare slots: a chunk may read past a row).  The .w word of a staged atom
+// packs its list entry and type: bits 6..31 the atom index, bits 3..5 the
+// type minus one, bits 0..2 the staged column sx (0 .. kTileCells+1).
+static size_t neigh_smem(int stage_cap) { return (size_t)(stage_cap + 32) * sizeof(float4); }
+
+__device__ __forceinline__ int stage_word(int j, int type, int sx) {
+  return (int)(((unsigned)j << 6) | ((unsigned)(type - 1) << 3) | (unsigned)sx);
+}
+__device__ __forceinline__ int stage_type(float w) { return ((__float_as_int(w) >> 3) & 7) + 1; }
+// the list entry (j << 6 | sx) of a staged atom
+__device__ __forceinline__ unsigned stage_entry(float w) {
+  return (unsigned)__float_as_int(w) & ~0x38u;
 }
 
 template <bool SINGLE, bool BATCH>
@@ -320,13 +331,13 @@ __global__ void __launch_bounds__(kNeighThreads, 8) k_neigh_tiles(
   const int *__restrict__ cell_start = BATCH ? cell_start_g + reps.cell_base[rep] : cell_start_g;
   extern __shared__ float4 s_stage[];
   float4 *sp = s_stage;
-  int *sj = reinterpret_cast<int *>(s_stage + stage_cap + 32);
   __shared__ int s_start[kStageCells + 1];
   __shared__ int s_src[kStageCells];
   __shared__ double s_sh[kStageCells][3];
   __shared__ double cns[(MD_MAXTYPES + 1) * (MD_MAXTYPES + 1)];
   __shared__ float cns_lo[(MD_MAXTYPES + 1) * (MD_MAXTYPES + 1)];
   __shared__ float cns_hi[(MD_MAXTYPES + 1) * (MD_MAXTYPES + 1)];
+  __shared__ float s_reach;  // largest list cutoff squared, with a safety margin
   const int ncx = box.ncell[0], ncy = box.ncell[1], ncz = box.ncell[2];
   const int tiles_x = (ncx + kTileCells - 1) / kTileCells;
   const int bx = tile % tiles_x;
@@ -339,6 +350,11 @@ __global__ void __launch_bounds__(kNeighThreads, 8) k_neigh_tiles(
     cns[k] = c;
     cns_lo[k] = (float)(c * (1.0 - 1.0e-5));
     cns_hi[k] = (float)(c * (1.0 + 1.0e-5));
+  }
+  if (threadIdx.x == 0) {
+    double c = 0.0;
+    for (int k = 0; k < ntp1 * ntp1; k++) c = fmax(c, cutneighsq_g[k]);
+    s_reach = (float)(c * (1.0 + 1.0e-4));
   }
   // staged cells: id = sx + (kTileCells+2)*(sy + 3*sz) is global cell
   // (cx0-1+sx, cy-1+sy, cz-1+sz), wrapped, with the shift of its image
@@ -383,14 +399,15 @@ __global__ void __launch_bounds__(kNeighThreads, 8) k_neigh_tiles(
         const double4 p = x4[g0 + t];
         const int o = s_start[id] + t;
         sp[o] = make_float4((float)(__dadd_rn(p.x, shx) - rx), (float)(__dadd_rn(p.y, shy) - ry),
-                            (float)(__dadd_rn(p.z, shz) - rz), __int_as_float((int)p.w));
-        sj[o] = md_make_entry(g0 + t, id % (kTileCells + 2));
+                            (float)(__dadd_rn(p.z, shz) - rz),
+                            __int_as_float(stage_word(g0 + t, (int)p.w, id % (kTileCells + 2))));
       }
     }
   }
   // the spare slots after the last staged row: far away, type 1
   if (staged && threadIdx.x < 32)
-    sp[s_start[kStageCells] + threadIdx.x] = make_float4(1.0e30f, 1.0e30f, 1.0e30f, __int_as_float(1));
+    sp[s_start[kStageCells] + threadIdx.x] =
+        make_float4(1.0e30f, 1.0e30f, 1.0e30f, __int_as_float(stage_word(0, 1, 0)));
   __syncthreads();
   // Warp w owns cell (cx0 + w, cy, cz); each lane takes one of its atoms.
   // The 27 neighbour cells are 9 contiguous staged ranges (3 cells along x
@@ -413,9 +430,28 @@ __global__ void __launch_bounds__(kNeighThreads, 8) k_neigh_tiles(
       // the FP64 position is read again only for a pair in the FP32 band
       const int ti = SINGLE ? 1 : (int)x4[act ? i : a0].w;
       const int my_m = act ? o0 + (i - a0) : -1;
+      // distances of this atom to the faces of its cell in y and z (staged
+      // offsets are from the centre of the owned row of cells): a stencil row
+      // whose y-z slab lies farther than the list cutoff holds no neighbour.
+      // Replica boxes only: their cells are up to a third wider than the
+      // list cutoff, so about a third of the tests fall away; a large box's
+      // cells are barely wider than the cutoff and the check costs more than
+      // it saves.
+      constexpr bool CULL = BATCH;
+      float fyl = 0.f, fyh = 0.f, fzl = 0.f, fzh = 0.f;
+      if constexpr (CULL) if (act) {
+        const float4 me = sp[my_m];
+        const float hy = 0.5f * (float)box.cs[1], hz = 0.5f * (float)box.cs[2];
+        fyl = fmaxf(0.f, me.y + hy);
+        fyh = fmaxf(0.f, hy - me.y);
+        fzl = fmaxf(0.f, me.z + hz);
+        fzh = fmaxf(0.f, hz - me.z);
+      }
+      const float reach2 = s_reach;
       // the owned atoms of this batch, staged as sp[ob .. ob + na) with the
       // same FP32 offsets from the tile centre as every candidate
       const int ob = o0 + (base - a0), na = min(32, a1 - base);
+      const unsigned batch_mask = na == 32 ? 0xffffffffu : ((1u << na) - 1u);
       int count = 0;
       int4 buf = make_int4(0, 0, 0, 0);
       for (int dz = -1; dz <= 1; dz++)
@@ -424,30 +460,51 @@ __global__ void __launch_bounds__(kNeighThreads, 8) k_neigh_tiles(
           const int r0 = s_start[idL], r1 = s_start[idL + 3];
           // entry code of a candidate in staged column sx: dx + 1 = sx - warp
           const unsigned rowadd = (unsigned)(((dy + 1) << 2) + ((dz + 1) << 4) - warp);
+          // owned atoms of the batch that this row can reach (warp-uniform mask)
+          unsigned reach = batch_mask;
+          if constexpr (CULL) {
+            const float gy = dy < 0 ? fyl : (dy > 0 ? fyh : 0.f);
+            const float gz = dz < 0 ? fzl : (dz > 0 ? fzh : 0.f);
+            reach = __ballot_sync(0xffffffffu, act && gy * gy + gz * gz <= reach2);
+            if (reach == 0u) continue;
+          }
           for (int cb = r0; cb < r1; cb += 32) {
             const int nc = min(32, r1 - cb);
             // this lane's candidate (the spare slots past the last row are
             // far away, and candidates past the row end are masked below)
             const float4 pc = sp[cb + lane];
-            const int tc = __float_as_int(pc.w) & 15;
+            const int tc = stage_type(pc.w);
             unsigned acc = 0u, band = 0u;
-            for (int a = 0; a < na; a++) {
-              const float4 q = sp[ob + a];
-              const float ddx = q.x - pc.x, ddy = q.y - pc.y, ddz = q.z - pc.z;
-              const float r2 = ddx * ddx + ddy * ddy + ddz * ddz;
-              float lo = lo1, hi = hi1;
-              if (!SINGLE) {
-                const int tt = (__float_as_int(q.w) & 15) * ntp1 + tc;
-                lo = cns_lo[tt];
-                hi = cns_hi[tt];
+            // the test of every owned atom of the batch against the lane's
+            // candidate; CHK skips the atoms this row cannot reach (a
+            // warp-uniform test), the other form is for rows that reach all
+            auto test_chunk = [&](auto chk_tag) {
+              constexpr bool CHK = decltype(chk_tag)::value;
+              for (int a = 0; a < na; a++) {
+                if (CHK && !((reach >> a) & 1u)) continue;
+                const float4 q = sp[ob + a];
+                const float ddx = q.x - pc.x, ddy = q.y - pc.y, ddz = q.z - pc.z;
+                const float r2 = ddx * ddx + ddy * ddy + ddz * ddz;
+                float lo = lo1, hi = hi1;
+                if (!SINGLE) {
+                  const int tt = stage_type(q.w) * ntp1 + tc;
+                  lo = cns_lo[tt];
+                  hi = cns_hi[tt];
+                }
+                const bool in = r2 <= hi;
+                const unsigned m = __ballot_sync(0xffffffffu, in);
+                const unsigned b = __ballot_sync(0xffffffffu, in && r2 >= lo);
+                if (lane == a) {
+                  acc = m;
+                  band = b;
+                }
               }
-              const bool in = r2 <= hi;
-              const unsigned m = __ballot_sync(0xffffffffu, in);
-              const unsigned b = __ballot_sync(0xffffffffu, in && r2 >= lo);
-              if (lane == a) {
-                acc = m;
-                band = b;
-              }
+            };
+            if constexpr (CULL) {
+              if ((reach & batch_mask) == batch_mask) test_chunk(std::false_type{});
+              else test_chunk(std::true_type{});
+            } else {
+              test_chunk(std::false_type{});
             }
             // candidates past the row end are not neighbours
             acc &= nc == 32 ? 0xffffffffu : ((1u << nc) - 1u);
@@ -458,19 +515,19 @@ __global__ void __launch_bounds__(kNeighThreads, 8) k_neigh_tiles(
                 const int t = __ffs(acc) - 1;
                 acc &= acc - 1u;
                 append_entry(nlist, stride, i, count, capacity,
-                             (int)((unsigned)sj[cb + t] + rowadd), buf);
+                             (int)(stage_entry(sp[cb + t].w) + rowadd), buf);
               }
             } else {
               while (acc) {
                 const int t = __ffs(acc) - 1;
                 acc &= acc - 1u;
                 const int m = cb + t;
-                const unsigned bits = (unsigned)sj[m];
+                const unsigned bits = stage_entry(sp[m].w);
                 // inside the FP32 uncertainty band: the reference's FP64 test
                 if ((band >> t) & 1u) {
                   const int id = idL - warp + (int)(bits & 7u);
                   if (!exact_pair(x4[i], x4[md_entry_j(bits)], s_sh[id][0], s_sh[id][1], s_sh[id][2],
-                                  SINGLE ? cut1 : cns[ti * ntp1 + (__float_as_int(sp[m].w) & 15)]))
+                                  SINGLE ? cut1 : cns[ti * ntp1 + stage_type(sp[m].w)]))
                     continue;
                 }
                 append_entry(nlist, stride, i, count, capacity, (int)(bits + rowadd), buf);

@@ -21,7 +21,11 @@
 // four slabs at a time with the next four already loading, evaluates every
 // entry branch-free with the one-instruction FP32 reciprocal, and adds the
 // FP32 force sum of each eight entries to the FP64 accumulator.
+#include <cooperative_groups.h>
+
+#include <algorithm>
 #include <type_traits>
+#include <vector>
 
 #include "md_state.h"
 
@@ -44,21 +48,41 @@ __device__ __forceinline__ void decode(unsigned int e, int &j, int &dx, int &dy,
   md_entry(e, j, dx, dy, dz);
 }
 
-template <int TPA, bool EV, bool ATOM, bool SINGLE, bool BATCH>
-__global__ void __launch_bounds__(128) k_lj_fp64(PairArgs a, const double4 *__restrict__ x4) {
-  __shared__ double tab[6 * TABSZ];
-  __shared__ double red[7 * 4];
-  const int nt2 = a.ntp1 * a.ntp1;
-  if (!SINGLE) {
-    for (int k = threadIdx.x; k < 6 * nt2; k += blockDim.x)
-      tab[k] = a.tables[(TAB_CUTSQ + k / nt2) * TABSZ + k % nt2];
-    __syncthreads();
+// lane sums of one atom's force (and per-atom energy/virial), stored by lane 0
+template <int TPA, bool EV, bool ATOM>
+__device__ __forceinline__ void lj_atom_store(const PairArgs &a, int i, int lane, bool active,
+                                              double fx, double fy, double fz,
+                                              const double (&acc)[7]) {
+  fx = lane_sum<TPA>(fx);
+  fy = lane_sum<TPA>(fy);
+  fz = lane_sum<TPA>(fz);
+  if (active && lane == 0) {
+    a.f[i] = fx;
+    a.f[a.stride + i] = fy;
+    a.f[2 * a.stride + i] = fz;
   }
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = t / TPA, lane = t % TPA;
-  const bool active = i < a.n;
-  double fx = 0.0, fy = 0.0, fz = 0.0;
-  double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+  if (EV && ATOM) {
+    double e[7];
+#pragma unroll
+    for (int k = 0; k < 7; k++) e[k] = lane_sum<TPA>(acc[k]);
+    if (active && lane == 0) {
+      const int o = a.orig[i];
+      if (a.eatom) a.eatom[o] = e[0];
+      if (a.vatom)
+#pragma unroll
+        for (int k = 0; k < 6; k++) a.vatom[6 * (size_t)o + k] = e[1 + k];
+    }
+  }
+}
+
+// One atom's pair forces in FP64 (this thread's lane of the TPA threads of
+// atom i): adds to fx, fy, fz (and to acc with EV).  `tab` is the per-type
+// table in shared memory (unused with SINGLE).
+template <int TPA, bool EV, bool SINGLE, bool BATCH>
+__device__ __forceinline__ void lj_atom_fp64(const PairArgs &a, const double4 *__restrict__ x4,
+                                             const double *tab, int nt2, int i, int lane,
+                                             bool active, double &fx, double &fy, double &fz,
+                                             double (&acc)[7]) {
   if (active) {
     double cutsq1 = 0, lj1 = 0, lj2 = 0, lj3 = 0, lj4 = 0, off = 0;
     if (SINGLE) {
@@ -149,46 +173,15 @@ __global__ void __launch_bounds__(128) k_lj_fp64(PairArgs a, const double4 *__re
     if (interior) slabs(std::false_type{});
     else slabs(std::true_type{});
   }
-  fx = lane_sum<TPA>(fx);
-  fy = lane_sum<TPA>(fy);
-  fz = lane_sum<TPA>(fz);
-  if (active && lane == 0) {
-    a.f[i] = fx;
-    a.f[a.stride + i] = fy;
-    a.f[2 * a.stride + i] = fz;
-  }
-  if (EV) {
-    if (ATOM) {
-      double e[7];
-#pragma unroll
-      for (int k = 0; k < 7; k++) e[k] = lane_sum<TPA>(acc[k]);
-      if (active && lane == 0) {
-        const int o = a.orig[i];
-        if (a.eatom) a.eatom[o] = e[0];
-        if (a.vatom)
-#pragma unroll
-          for (int k = 0; k < 6; k++) a.vatom[6 * (size_t)o + k] = e[1 + k];
-      }
-    }
-    block_partials_finish<7>(acc, red, a.partial, a.counter, a.ev, false);
-  }
 }
 
-template <int TPA, bool EV, bool ATOM, bool SINGLE, bool BATCH>
-__global__ void __launch_bounds__(128) k_lj_mixed(PairArgs a, const float4 *__restrict__ xr) {
-  __shared__ float tabf[6 * TABSZ];
-  __shared__ double red[7 * 4];
-  const int nt2 = a.ntp1 * a.ntp1;
-  if (!SINGLE) {
-    for (int k = threadIdx.x; k < 6 * nt2; k += blockDim.x)
-      tabf[k] = (float)a.tables[(TAB_CUTSQ + k / nt2) * TABSZ + k % nt2];
-    __syncthreads();
-  }
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = t / TPA, lane = t % TPA;
-  const bool active = i < a.n;
-  double fx = 0.0, fy = 0.0, fz = 0.0;
-  double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+// One atom's pair forces in the mixed form (FP32 pair math, FP64 sums), as
+// lj_atom_fp64.  `tabf` is the per-type table in shared memory.
+template <int TPA, bool EV, bool SINGLE, bool BATCH>
+__device__ __forceinline__ void lj_atom_mixed(const PairArgs &a, const float4 *__restrict__ xr,
+                                              const float *tabf, int nt2, int i, int lane,
+                                              bool active, double &fx, double &fy, double &fz,
+                                              double (&acc)[7]) {
   if (active) {
     float cutsq1 = 0, lj1 = 0, lj2 = 0, lj3 = 0, lj4 = 0, off = 0;
     if (SINGLE) {
@@ -284,29 +277,172 @@ __global__ void __launch_bounds__(128) k_lj_mixed(PairArgs a, const float4 *__re
       c4 = cn;
     }
   }
-  fx = lane_sum<TPA>(fx);
-  fy = lane_sum<TPA>(fy);
-  fz = lane_sum<TPA>(fz);
-  if (active && lane == 0) {
-    a.f[i] = fx;
-    a.f[a.stride + i] = fy;
-    a.f[2 * a.stride + i] = fz;
+}
+
+template <int TPA, bool EV, bool ATOM, bool SINGLE, bool BATCH>
+__global__ void __launch_bounds__(128) k_lj_fp64(PairArgs a, const double4 *__restrict__ x4) {
+  __shared__ double tab[6 * TABSZ];
+  __shared__ double red[7 * 4];
+  const int nt2 = a.ntp1 * a.ntp1;
+  if (!SINGLE) {
+    for (int k = threadIdx.x; k < 6 * nt2; k += blockDim.x)
+      tab[k] = a.tables[(TAB_CUTSQ + k / nt2) * TABSZ + k % nt2];
+    __syncthreads();
   }
-  if (EV) {
-    if (ATOM) {
-      double e[7];
-#pragma unroll
-      for (int k = 0; k < 7; k++) e[k] = lane_sum<TPA>(acc[k]);
-      if (active && lane == 0) {
-        const int o = a.orig[i];
-        if (a.eatom) a.eatom[o] = e[0];
-        if (a.vatom)
-#pragma unroll
-          for (int k = 0; k < 6; k++) a.vatom[6 * (size_t)o + k] = e[1 + k];
-      }
-    }
-    block_partials_finish<7>(acc, red, a.partial, a.counter, a.ev, false);
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = t / TPA, lane = t % TPA;
+  const bool active = i < a.n;
+  double fx = 0.0, fy = 0.0, fz = 0.0;
+  double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+  lj_atom_fp64<TPA, EV, SINGLE, BATCH>(a, x4, tab, nt2, i, lane, active, fx, fy, fz, acc);
+  lj_atom_store<TPA, EV, ATOM>(a, i, lane, active, fx, fy, fz, acc);
+  if (EV) block_partials_finish<7>(acc, red, a.partial, a.counter, a.ev, false);
+}
+
+template <int TPA, bool EV, bool ATOM, bool SINGLE, bool BATCH>
+__global__ void __launch_bounds__(128) k_lj_mixed(PairArgs a, const float4 *__restrict__ xr) {
+  __shared__ float tabf[6 * TABSZ];
+  __shared__ double red[7 * 4];
+  const int nt2 = a.ntp1 * a.ntp1;
+  if (!SINGLE) {
+    for (int k = threadIdx.x; k < 6 * nt2; k += blockDim.x)
+      tabf[k] = (float)a.tables[(TAB_CUTSQ + k / nt2) * TABSZ + k % nt2];
+    __syncthreads();
   }
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = t / TPA, lane = t % TPA;
+  const bool active = i < a.n;
+  double fx = 0.0, fy = 0.0, fz = 0.0;
+  double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+  lj_atom_mixed<TPA, EV, SINGLE, BATCH>(a, xr, tabf, nt2, i, lane, active, fx, fy, fz, acc);
+  lj_atom_store<TPA, EV, ATOM>(a, i, lane, active, fx, fy, fz, acc);
+  if (EV) block_partials_finish<7>(acc, red, a.partial, a.counter, a.ev, false);
+}
+
+// One MD step of every replica of a batched context in one launch.  Cluster g
+// (rep_cs CTAs) owns a fixed set of whole replicas: the concatenation of the
+// atom ranges ranges[first[g] .. first[g+1]).  Each CTA takes an equal share
+// of that concatenation.  A replica's atoms interact only with each other, so
+// the step needs no grid-wide ordering:
+//   1. pair forces of the share's atoms (lj_atom_*, the same code and order as
+//      k_lj_fp64 / k_lj_mixed);
+//   2. a cluster barrier: every position of the group has been read;
+//   3. FixNVE final half-step of this step and initial half-step of the next
+//      for the share's atoms (md_nve_fused_atom, as k_nve_fused);
+//   4. the last CTA of the grid to finish makes the next step's rebuild
+//      decision, with every CTA's displacement flag (as k_nve_fused).
+// The per-atom arithmetic is the graph path's, so both give the same bits.
+struct RepStepArgs {
+  const int *first;   // per group: first range, ngroups + 1 entries
+  const int2 *ranges; // (start, count) of sorted atoms
+  double dtv, dtf, triggersq;
+  const double *mass;
+  double4 *x4;
+  double *v;
+  const int *cell;
+  const double4 *xhold;
+  int *status, *dcount, *mail;
+  unsigned int *counter;
+  int every, delay, check;
+};
+
+// sorted atom index of position k in the concatenation of ranges [r0, r1)
+__device__ __forceinline__ int rep_atom(const int2 *__restrict__ ranges, int r0, int r1, int k) {
+  for (int r = r0; r < r1; r++) {
+    const int2 rg = ranges[r];
+    if (k < rg.y) return rg.x + k;
+    k -= rg.y;
+  }
+  return -1;
+}
+
+template <int TPA, bool MIXED, bool SINGLE>
+__global__ void __launch_bounds__(512) k_rep_step(PairArgs a, const double4 *__restrict__ x4,
+                                                   const float4 *__restrict__ xr, RepStepArgs s) {
+  namespace cg = cooperative_groups;
+  __shared__ double tab[6 * TABSZ];
+  __shared__ bool last;
+  const int nt2 = a.ntp1 * a.ntp1;
+  if (!SINGLE) {
+    for (int k = threadIdx.x; k < 6 * nt2; k += blockDim.x)
+      tab[k] = a.tables[(TAB_CUTSQ + k / nt2) * TABSZ + k % nt2];
+  }
+  float *tabf = reinterpret_cast<float *>(tab);
+  if (!SINGLE && MIXED) {
+    __syncthreads();
+    for (int k = threadIdx.x; k < 6 * nt2; k += blockDim.x) tabf[k] = (float)tab[k];
+  }
+  __syncthreads();
+  cg::cluster_group cl = cg::this_cluster();
+  const int cs = (int)cl.num_blocks(), cr = (int)cl.block_rank();
+  const int g = blockIdx.x / cs;
+  const int r0 = s.first[g], r1 = s.first[g + 1];
+  int total = 0;
+  for (int r = r0; r < r1; r++) total += s.ranges[r].y;
+  const int k0 = (int)((long long)total * cr / cs), k1 = (int)((long long)total * (cr + 1) / cs);
+  // 1. forces: TPA threads per atom, every thread takes the same trip count
+  const int work = (k1 - k0) * TPA;
+  for (int base = 0; base < work; base += blockDim.x) {
+    const int t = base + threadIdx.x;
+    const int lane = t % TPA;
+    const bool active = t < work;
+    const int i = active ? rep_atom(s.ranges, r0, r1, k0 + t / TPA) : 0;
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    if (MIXED)
+      lj_atom_mixed<TPA, false, SINGLE, true>(a, xr, tabf, nt2, i, lane, active, fx, fy, fz, acc);
+    else
+      lj_atom_fp64<TPA, false, SINGLE, true>(a, x4, tab, nt2, i, lane, active, fx, fy, fz, acc);
+    lj_atom_store<TPA, false, false>(a, i, lane, active, fx, fy, fz, acc);
+  }
+  // 2. every CTA of the cluster has read the group's positions
+  cl.sync();
+  // 3. half-steps of the share's atoms
+  bool moved = false;
+  for (int k = k0 + (int)threadIdx.x; k < k1; k += blockDim.x) {
+    const int i = rep_atom(s.ranges, r0, r1, k);
+    double ke = 0.0;
+    moved |= md_nve_fused_atom<false>(i, a.stride, s.dtv, s.dtf, s.mass, const_cast<double4 *>(x4),
+                                      s.v, a.f, MIXED ? const_cast<float4 *>(xr) : nullptr, s.cell,
+                                      a.reps.box[a.reps.rep_of_atom[i]], s.xhold, s.triggersq, ke);
+  }
+  if (s.xhold && __any_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0) {
+    atomicExch(&s.status[ST_MOVED], 1);
+    __threadfence();  // the flag is visible before this block counts itself done
+  }
+  // 4. the last CTA to finish makes the next step's rebuild decision
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(s.counter, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    md_decide_dev(s.status, s.every, s.delay, s.check, s.dcount, s.mail);
+    *s.counter = 0u;
+  }
+}
+
+template <int TPA, bool MIXED>
+cudaError_t launch_rep_t(b200_ctx *c, const PairArgs &a, const RepStepArgs &s) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(c->rep_groups * c->rep_cs), 1, 1);
+  cfg.blockDim = dim3((unsigned)c->rep_block, 1, 1);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = c->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)c->rep_cs;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (c->ntypes == 1)
+    return cudaLaunchKernelEx(&cfg, k_rep_step<TPA, MIXED, true>, a, (const double4 *)c->x4,
+                              (const float4 *)c->xr, s);
+  return cudaLaunchKernelEx(&cfg, k_rep_step<TPA, MIXED, false>, a, (const double4 *)c->x4,
+                            (const float4 *)c->xr, s);
 }
 
 template <int TPA, bool EV, bool ATOM, bool SINGLE, bool BATCH>
@@ -341,6 +477,110 @@ void launch_tpa(b200_ctx *c, const PairArgs &a, bool ev, bool atom, bool single)
 }
 
 }  // namespace
+
+static PairArgs pair_args(b200_ctx *c, double *eatom, double *vatom) {
+  PairArgs a;
+  a.n = c->n;
+  a.stride = c->stride;
+  a.ntp1 = c->ntypes + 1;
+  a.box = c->box;
+  a.reps = c->reps();
+  a.tables = c->tables_dev;
+  a.cell = c->cell;
+  a.nlist = c->nlist;
+  a.numneigh = c->numneigh;
+  a.orig = c->orig;
+  a.f = c->f;
+  a.partial = c->partial;
+  a.counter = c->counter;
+  a.ev = c->ev;
+  a.eatom = eatom;
+  a.vatom = vatom;
+  return a;
+}
+
+cudaError_t md_rep_step(b200_ctx *c, double dtv, double dtf) {
+  const PairArgs a = pair_args(c, nullptr, nullptr);
+  RepStepArgs s;
+  s.first = c->d_rep_grp_first;
+  s.ranges = c->d_rep_ranges;
+  s.dtv = dtv;
+  s.dtf = dtf;
+  s.triggersq = 0.25 * c->skin * c->skin;  // src/neighbor.cpp:239
+  s.mass = c->mass_dev;
+  s.x4 = c->x4;
+  s.v = c->v;
+  s.cell = c->cell;
+  s.xhold = c->check ? c->xhold : nullptr;
+  s.status = c->status;
+  s.dcount = c->dec_count;
+  s.mail = c->mail_dev;
+  s.counter = c->counter;
+  s.every = c->every;
+  s.delay = c->delay;
+  s.check = c->check;
+  const bool mixed = c->prec == B200_PREC_MIXED;
+  cudaError_t e;
+  switch (c->rep_tpa) {
+    case 1: e = mixed ? launch_rep_t<1, true>(c, a, s) : launch_rep_t<1, false>(c, a, s); break;
+    case 2: e = mixed ? launch_rep_t<2, true>(c, a, s) : launch_rep_t<2, false>(c, a, s); break;
+    default: e = mixed ? launch_rep_t<4, true>(c, a, s) : launch_rep_t<4, false>(c, a, s); break;
+  }
+  c->launches++;
+  if (e != cudaSuccess) return e;
+  return cudaGetLastError();
+}
+
+// Group plan: G = (SMs x CTAs per SM) / cs clusters, at most one per replica;
+// replicas go, largest first, to the group with the fewest atoms (longest
+// processing time first), so the cluster that finishes last carries about
+// the mean load whenever no replica is larger than it.
+int md_rep_plan(b200_ctx *c, int cs, int block, int tpa) {
+  int dev_sms = 148;
+  cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->device);
+  const int per_sm = block <= 256 ? 4 : 2;
+  int groups = dev_sms * per_sm / cs;
+  if (groups > c->nrep) groups = c->nrep;
+  if (groups < 1) groups = 1;
+  std::vector<int> order(c->nrep);
+  for (int r = 0; r < c->nrep; r++) order[r] = r;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int x, int y) { return c->rep_natoms[x] > c->rep_natoms[y]; });
+  std::vector<long long> load(groups, 0);
+  std::vector<std::vector<int>> members(groups);
+  for (int r : order) {
+    int best = 0;
+    for (int k = 1; k < groups; k++)
+      if (load[k] < load[best]) best = k;
+    load[best] += c->rep_natoms[r];
+    members[best].push_back(r);
+  }
+  std::vector<int> first(groups + 1, 0);
+  std::vector<int2> ranges;
+  for (int k = 0; k < groups; k++) {
+    std::sort(members[k].begin(), members[k].end());
+    for (int r : members[k]) ranges.push_back(make_int2(c->rep_atom_start[r], c->rep_natoms[r]));
+    first[k + 1] = (int)ranges.size();
+  }
+  if (c->d_rep_grp_first) cudaFree(c->d_rep_grp_first);
+  if (c->d_rep_ranges) cudaFree(c->d_rep_ranges);
+  c->d_rep_grp_first = nullptr;
+  c->d_rep_ranges = nullptr;
+  cudaError_t e = cudaMalloc((void **)&c->d_rep_grp_first, first.size() * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_rep_ranges, ranges.size() * sizeof(int2));
+  if (e == cudaSuccess)
+    e = cudaMemcpy(c->d_rep_grp_first, first.data(), first.size() * sizeof(int),
+                   cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(c->d_rep_ranges, ranges.data(), ranges.size() * sizeof(int2),
+                   cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return B200_ERR_CUDA;
+  c->rep_cs = cs;
+  c->rep_block = block;
+  c->rep_tpa = tpa;
+  c->rep_groups = groups;
+  return B200_OK;
+}
 
 cudaError_t md_lj_compute(b200_ctx *c, bool ev, bool atom_ev, double *eatom, double *vatom) {
   PairArgs a;

@@ -456,6 +456,21 @@ class System:
         self.rep_lo, self.rep_hi = lo, hi
         self.box_lo, self.box_hi = lo[0], hi[0]
 
+    def set_replica_step(self, mode=0, cluster=0, block=0, tpa=0):
+        """Step form of the replica batch: 0 chosen by timing on the next
+        setup, 1 a graph of kernels per step, 2 one cluster launch per step
+        (cluster 1/2/4, block 256/512, tpa 1/2/4; 0 = tuned)."""
+        self._ck(self._L.b200_set_replica_step(self._h, mode, cluster, block, tpa))
+
+    def replica_step(self):
+        """The step form in use and the per-step times the tuning measured."""
+        one, cs, bl, tp = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        ms = np.zeros(2)
+        self._ck(self._L.b200_get_replica_step(self._h, C.byref(one), C.byref(cs), C.byref(bl),
+                                               C.byref(tp), _abi.dptr(ms)))
+        return dict(onelaunch=bool(one.value), cluster=cs.value, block=bl.value, tpa=tp.value,
+                    graph_ms=float(ms[0]), onelaunch_ms=float(ms[1]))
+
     def replica_thermo(self):
         """Per-replica thermo (Temp, E_pair, TotEng, Press as thermo_style
         one, normalised per atom in lj units) of the current state."""

@@ -72,3 +72,40 @@ def test_step_times_recorded(batch):
     ms = s.step_times()
     s.close()
     assert len(ms) == 30 and np.all(ms > 0)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_one_launch_step_equals_graph_path(batch, precision):
+    """The one-launch replica step (clusters owning whole replicas) and the
+    graph of kernels take the same rounded steps: identical trajectories
+    through two rebuilds, for every cluster size."""
+    ref = make_batch(batch, precision, tpa=1)
+    ref.set_replica_step(1)
+    ref.setup()
+    assert not ref.replica_step()["onelaunch"]
+    ref.run(STEPS)
+    want = ref.download()
+    ref.close()
+    for cs, block in ((1, 256), (2, 512), (4, 256)):
+        s = make_batch(batch, precision, tpa=1)
+        s.set_replica_step(2, cs, block, 1)
+        s.setup()
+        st = s.replica_step()
+        assert st["onelaunch"] and st["cluster"] == cs and st["block"] == block
+        s.run(STEPS)
+        got = s.download()
+        for k in ("x", "v", "image"):
+            assert np.array_equal(got[k], want[k]), (cs, block, k)
+        s.close()
+
+
+def test_step_form_is_tuned():
+    """mode 0 times both forms on setup and reports them."""
+    b = replica_batch(nrep=24, seed=99)
+    s = make_batch(b, "mixed")
+    s.setup()
+    st = s.replica_step()
+    assert st["graph_ms"] > 0 and st["onelaunch_ms"] > 0
+    assert st["onelaunch"] == (st["onelaunch_ms"] < st["graph_ms"])
+    s.run(25)
+    s.close()
