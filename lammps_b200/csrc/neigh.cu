@@ -20,8 +20,6 @@
 // (src/neigh_half_bin.cpp:355-360, src/atom_vec_atomic.cpp:297-299).
 #include <cstdio>
 
-#include <type_traits>
-
 #include "md_state.h"
 
 namespace {
@@ -262,7 +260,9 @@ __global__ void k_copyback(int n, int stride, const double4 *__restrict__ x4b,
 // are decided by the reference's FP64 arithmetic on the global FP64
 // positions, so the list is bit-identical to the FP64 criterion.
 constexpr int kTileCells = MD_TILE_CELLS;
-constexpr int kStageCapMax = 2048;  // keeps the builder within 48 KB of shared memory
+// staged atoms per tile at most: 8192 x 16 B = 128 KB of shared memory, with
+// the opt-in above the default 48 KB (set on the first build)
+constexpr int kStageCapMax = 8192;
 constexpr int kStageCells = 3 * 3 * (kTileCells + 2);
 constexpr int kNeighThreads = 32 * kTileCells;  // one warp per owned cell
 
@@ -322,7 +322,7 @@ __global__ void __launch_bounds__(kNeighThreads, 8) k_neigh_tiles(
     int n, int stride, int capacity, int stage_cap, BoxGeom box1, Reps reps, int ntp1,
     const double *__restrict__ cutneighsq_g, const double4 *__restrict__ x4,
     const int *__restrict__ cell_start_g, int *__restrict__ nlist, int *__restrict__ numneigh,
-    int *__restrict__ status, const int *flag) {
+    int *__restrict__ status, const int *flag, int pass, int cap1) {
   if (!rebuild_on(flag)) return;
   // batched: this tile's replica, its box and its cells' slice of cell_start
   const int rep = BATCH ? reps.tile_rep[blockIdx.x] : 0;
@@ -337,7 +337,6 @@ __global__ void __launch_bounds__(kNeighThreads, 8) k_neigh_tiles(
   __shared__ double cns[(MD_MAXTYPES + 1) * (MD_MAXTYPES + 1)];
   __shared__ float cns_lo[(MD_MAXTYPES + 1) * (MD_MAXTYPES + 1)];
   __shared__ float cns_hi[(MD_MAXTYPES + 1) * (MD_MAXTYPES + 1)];
-  __shared__ float s_reach;  // largest list cutoff squared, with a safety margin
   const int ncx = box.ncell[0], ncy = box.ncell[1], ncz = box.ncell[2];
   const int tiles_x = (ncx + kTileCells - 1) / kTileCells;
   const int bx = tile % tiles_x;
@@ -350,11 +349,6 @@ __global__ void __launch_bounds__(kNeighThreads, 8) k_neigh_tiles(
     cns[k] = c;
     cns_lo[k] = (float)(c * (1.0 - 1.0e-5));
     cns_hi[k] = (float)(c * (1.0 + 1.0e-5));
-  }
-  if (threadIdx.x == 0) {
-    double c = 0.0;
-    for (int k = 0; k < ntp1 * ntp1; k++) c = fmax(c, cutneighsq_g[k]);
-    s_reach = (float)(c * (1.0 + 1.0e-4));
   }
   // staged cells: id = sx + (kTileCells+2)*(sy + 3*sz) is global cell
   // (cx0-1+sx, cy-1+sy, cz-1+sz), wrapped, with the shift of its image
@@ -383,8 +377,13 @@ __global__ void __launch_bounds__(kNeighThreads, 8) k_neigh_tiles(
     for (int id = 0; id < kStageCells; id++) s_start[id + 1] += s_start[id];
   }
   __syncthreads();
-  const bool staged = s_start[kStageCells] <= stage_cap;
-  if (threadIdx.x == 0) atomicMax(&status[ST_MAXSTAGE], s_start[kStageCells]);
+  // pass 0: every tile (staged, or the global-memory path when it does not
+  // fit); pass 1: the tiles that fit stage_cap; pass 2: only the tiles that
+  // pass 1 left (more than cap1 atoms), with a larger stage_cap
+  const int nstage = s_start[kStageCells];
+  if ((pass == 1 && nstage > stage_cap) || (pass == 2 && nstage <= cap1)) return;
+  const bool staged = nstage <= stage_cap;
+  if (threadIdx.x == 0) atomicMax(&status[ST_MAXSTAGE], nstage);
   // FP32 reference point: centre of cell (cx0, cy, cz)
   const double rx = box.lo[0] + (cx0 + 0.5) * box.cs[0];
   const double ry = box.lo[1] + (cy + 0.5) * box.cs[1];
@@ -430,28 +429,9 @@ __global__ void __launch_bounds__(kNeighThreads, 8) k_neigh_tiles(
       // the FP64 position is read again only for a pair in the FP32 band
       const int ti = SINGLE ? 1 : (int)x4[act ? i : a0].w;
       const int my_m = act ? o0 + (i - a0) : -1;
-      // distances of this atom to the faces of its cell in y and z (staged
-      // offsets are from the centre of the owned row of cells): a stencil row
-      // whose y-z slab lies farther than the list cutoff holds no neighbour.
-      // Replica boxes only: their cells are up to a third wider than the
-      // list cutoff, so about a third of the tests fall away; a large box's
-      // cells are barely wider than the cutoff and the check costs more than
-      // it saves.
-      constexpr bool CULL = BATCH;
-      float fyl = 0.f, fyh = 0.f, fzl = 0.f, fzh = 0.f;
-      if constexpr (CULL) if (act) {
-        const float4 me = sp[my_m];
-        const float hy = 0.5f * (float)box.cs[1], hz = 0.5f * (float)box.cs[2];
-        fyl = fmaxf(0.f, me.y + hy);
-        fyh = fmaxf(0.f, hy - me.y);
-        fzl = fmaxf(0.f, me.z + hz);
-        fzh = fmaxf(0.f, hz - me.z);
-      }
-      const float reach2 = s_reach;
       // the owned atoms of this batch, staged as sp[ob .. ob + na) with the
       // same FP32 offsets from the tile centre as every candidate
       const int ob = o0 + (base - a0), na = min(32, a1 - base);
-      const unsigned batch_mask = na == 32 ? 0xffffffffu : ((1u << na) - 1u);
       int count = 0;
       int4 buf = make_int4(0, 0, 0, 0);
       for (int dz = -1; dz <= 1; dz++)
@@ -460,14 +440,6 @@ __global__ void __launch_bounds__(kNeighThreads, 8) k_neigh_tiles(
           const int r0 = s_start[idL], r1 = s_start[idL + 3];
           // entry code of a candidate in staged column sx: dx + 1 = sx - warp
           const unsigned rowadd = (unsigned)(((dy + 1) << 2) + ((dz + 1) << 4) - warp);
-          // owned atoms of the batch that this row can reach (warp-uniform mask)
-          unsigned reach = batch_mask;
-          if constexpr (CULL) {
-            const float gy = dy < 0 ? fyl : (dy > 0 ? fyh : 0.f);
-            const float gz = dz < 0 ? fzl : (dz > 0 ? fzh : 0.f);
-            reach = __ballot_sync(0xffffffffu, act && gy * gy + gz * gz <= reach2);
-            if (reach == 0u) continue;
-          }
           for (int cb = r0; cb < r1; cb += 32) {
             const int nc = min(32, r1 - cb);
             // this lane's candidate (the spare slots past the last row are
@@ -475,36 +447,23 @@ __global__ void __launch_bounds__(kNeighThreads, 8) k_neigh_tiles(
             const float4 pc = sp[cb + lane];
             const int tc = stage_type(pc.w);
             unsigned acc = 0u, band = 0u;
-            // the test of every owned atom of the batch against the lane's
-            // candidate; CHK skips the atoms this row cannot reach (a
-            // warp-uniform test), the other form is for rows that reach all
-            auto test_chunk = [&](auto chk_tag) {
-              constexpr bool CHK = decltype(chk_tag)::value;
-              for (int a = 0; a < na; a++) {
-                if (CHK && !((reach >> a) & 1u)) continue;
-                const float4 q = sp[ob + a];
-                const float ddx = q.x - pc.x, ddy = q.y - pc.y, ddz = q.z - pc.z;
-                const float r2 = ddx * ddx + ddy * ddy + ddz * ddz;
-                float lo = lo1, hi = hi1;
-                if (!SINGLE) {
-                  const int tt = stage_type(q.w) * ntp1 + tc;
-                  lo = cns_lo[tt];
-                  hi = cns_hi[tt];
-                }
-                const bool in = r2 <= hi;
-                const unsigned m = __ballot_sync(0xffffffffu, in);
-                const unsigned b = __ballot_sync(0xffffffffu, in && r2 >= lo);
-                if (lane == a) {
-                  acc = m;
-                  band = b;
-                }
+            for (int a = 0; a < na; a++) {
+              const float4 q = sp[ob + a];
+              const float ddx = q.x - pc.x, ddy = q.y - pc.y, ddz = q.z - pc.z;
+              const float r2 = ddx * ddx + ddy * ddy + ddz * ddz;
+              float lo = lo1, hi = hi1;
+              if (!SINGLE) {
+                const int tt = stage_type(q.w) * ntp1 + tc;
+                lo = cns_lo[tt];
+                hi = cns_hi[tt];
               }
-            };
-            if constexpr (CULL) {
-              if ((reach & batch_mask) == batch_mask) test_chunk(std::false_type{});
-              else test_chunk(std::true_type{});
-            } else {
-              test_chunk(std::false_type{});
+              const bool in = r2 <= hi;
+              const unsigned m = __ballot_sync(0xffffffffu, in);
+              const unsigned b = __ballot_sync(0xffffffffu, in && r2 >= lo);
+              if (lane == a) {
+                acc = m;
+                band = b;
+              }
             }
             // candidates past the row end are not neighbours
             acc &= nc == 32 ? 0xffffffffu : ((1u << nc) - 1u);
@@ -683,8 +642,28 @@ __global__ void k_prefix_ll(int n, const int *__restrict__ cnt, long long *__res
 // kStageCapMax.  A tile that stages more atoms takes the global-memory path
 // (same list, slower); a smaller capacity leaves room for more resident
 // CTAs per SM.
+static int round_cap(int cap) {
+  cap = (cap + 127) & ~127;
+  if (cap < 256) cap = 256;
+  return cap < kStageCapMax ? cap : kStageCapMax;
+}
+
+// Staging capacity of the builder tiles: 1.25 x the mean atom count of the 54
+// staged cells, raised when a build reports a more crowded tile.  For a batch
+// the mean is the batch's (the common case, at full occupancy); the densest
+// replicas' tiles are rebuilt in a second pass with md_stage_cap2.
 int md_stage_cap(const b200_ctx *c) {
-  double per_cell = c->ncells > 0 ? (double)c->n / c->ncells : 0.0;
+  const double per_cell = c->ncells > 0 ? (double)c->n / c->ncells : 0.0;
+  int cap = (int)(1.25 * kStageCells * per_cell) + 64;
+  if (!c->nrep && c->stage_need > cap) cap = c->stage_need;
+  return round_cap(cap);
+}
+
+// second-pass capacity of a batch: the densest replica's tiles (0 when the
+// first pass holds every tile)
+int md_stage_cap2(const b200_ctx *c) {
+  if (!c->nrep) return 0;
+  double per_cell = 0.0;
   for (int r = 0; r < c->nrep; r++) {
     const BoxGeom &b = c->rep_box[r];
     const double d = (double)c->rep_natoms[r] / ((double)b.ncell[0] * b.ncell[1] * b.ncell[2]);
@@ -692,19 +671,21 @@ int md_stage_cap(const b200_ctx *c) {
   }
   int cap = (int)(1.25 * kStageCells * per_cell) + 64;
   if (c->stage_need > cap) cap = c->stage_need;
-  cap = (cap + 127) & ~127;
-  if (cap < 256) cap = 256;
-  return cap < kStageCapMax ? cap : kStageCapMax;
+  cap = round_cap(cap);
+  return cap > md_stage_cap(c) ? cap : 0;
 }
 
 // After a build: raise the staging capacity when some tile staged more atoms
 // than the current one holds.  Returns true when the capacity changed (the
 // caller re-captures its graphs).
 bool md_stage_feedback(b200_ctx *c, int staged_max) {
-  const int cap = md_stage_cap(c);
+  const int cap = c->nrep ? (md_stage_cap2(c) > 0 ? md_stage_cap2(c) : md_stage_cap(c))
+                          : md_stage_cap(c);
   if (staged_max <= cap || cap >= kStageCapMax) return false;
   c->stage_need = staged_max + staged_max / 10;
-  return md_stage_cap(c) != cap;
+  const int now = c->nrep ? (md_stage_cap2(c) > 0 ? md_stage_cap2(c) : md_stage_cap(c))
+                          : md_stage_cap(c);
+  return now != cap;
 }
 
 static cudaError_t launch_scan(b200_ctx *c, int m, const int *in, int *out, const int *flag) {
@@ -757,22 +738,47 @@ cudaError_t md_rebuild(b200_ctx *c, const int *d_flag) {
     const int tiles = c->nrep ? c->ntiles
                               : ((c->box.ncell[0] + kTileCells - 1) / kTileCells) *
                                     c->box.ncell[1] * c->box.ncell[2];
+    // the shared-memory opt-in, once per device this process uses
+    static unsigned long long smem_opt_in = 0ull;
+    const unsigned long long dev_bit = 1ull << (c->device & 63);
+    if (!(smem_opt_in & dev_bit)) {
+      const int most = (int)neigh_smem(kStageCapMax);
+      cudaFuncSetAttribute(k_neigh_tiles<true, false>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, most);
+      cudaFuncSetAttribute(k_neigh_tiles<true, true>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, most);
+      cudaFuncSetAttribute(k_neigh_tiles<false, false>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, most);
+      cudaFuncSetAttribute(k_neigh_tiles<false, true>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, most);
+      smem_opt_in |= dev_bit;
+    }
     const int cap = md_stage_cap(c);
-    const size_t smem = neigh_smem(cap);
+    const int cap2 = md_stage_cap2(c);  // a batch's densest tiles, or 0
+    auto launch = [&](int stage_cap, int pass) {
+      const size_t smem = neigh_smem(stage_cap);
 #define MD_NEIGH_ARGS                                                                         \
-  n, c->stride, c->capacity, cap, c->box, R, c->ntypes + 1, c->cutneighsq_dev, c->x4,        \
-      c->cell_start, c->nlist, c->numneigh, c->status, d_flag
-    if (c->ntypes == 1 && !c->nrep)
-      k_neigh_tiles<true, false><<<tiles, kNeighThreads, smem, c->stream>>>(MD_NEIGH_ARGS);
-    else if (c->ntypes == 1)
-      k_neigh_tiles<true, true><<<tiles, kNeighThreads, smem, c->stream>>>(MD_NEIGH_ARGS);
-    else if (!c->nrep)
-      k_neigh_tiles<false, false><<<tiles, kNeighThreads, smem, c->stream>>>(MD_NEIGH_ARGS);
-    else
-      k_neigh_tiles<false, true><<<tiles, kNeighThreads, smem, c->stream>>>(MD_NEIGH_ARGS);
+  n, c->stride, c->capacity, stage_cap, c->box, R, c->ntypes + 1, c->cutneighsq_dev, c->x4,  \
+      c->cell_start, c->nlist, c->numneigh, c->status, d_flag, pass, cap
+      if (c->ntypes == 1 && !c->nrep)
+        k_neigh_tiles<true, false><<<tiles, kNeighThreads, smem, c->stream>>>(MD_NEIGH_ARGS);
+      else if (c->ntypes == 1)
+        k_neigh_tiles<true, true><<<tiles, kNeighThreads, smem, c->stream>>>(MD_NEIGH_ARGS);
+      else if (!c->nrep)
+        k_neigh_tiles<false, false><<<tiles, kNeighThreads, smem, c->stream>>>(MD_NEIGH_ARGS);
+      else
+        k_neigh_tiles<false, true><<<tiles, kNeighThreads, smem, c->stream>>>(MD_NEIGH_ARGS);
 #undef MD_NEIGH_ARGS
+      c->launches++;
+    };
+    if (cap2 > 0) {
+      launch(cap, 1);
+      launch(cap2, 2);
+    } else {
+      launch(cap, 0);
+    }
   }
-  c->launches += 4;
+  c->launches += 3;
   return cudaGetLastError();
 }
 
