@@ -4,8 +4,8 @@ ctypes binding of ``oracle/md_oracle.c``, a plain-C restatement of the
 reference's serial CPU path (LAMMPS 8 Aug 2014: CommBrick::borders,
 Neighbor::half_bin_newton, PairLJCut::compute, PairEAM::compute, FixNVE,
 Pair::virial_fdotr_compute, Thermo).  Only the tests, ``__graft_entry__.smoke``
-and the CPU-baseline leg of ``bench.py`` may use it, and only as the checker
-or the timed CPU baseline.  The product (``lammps_b200``) never imports it.
+and the CPU-baseline leg of ``bench.py`` may use it, and only to check the
+engine's results or as the timed CPU baseline.  The product (``lammps_b200``) never imports it.
 
 Parity pin: the oracle is checked against the reference's own golden thermo
 logs and neighbor statistics (``tests/golden/``); see

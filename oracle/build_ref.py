@@ -30,7 +30,7 @@ touching a source file; the arithmetic is unchanged.
 
 Usage: python oracle/build_ref.py [--src DIR] [--no-b200] [-j N]
 The reference's src/ tree comes from --src, the LAMMPS_SRC environment
-variable, or the checkout this build reads (DEFAULT_SRC).
+variable, or the default checkout location (DEFAULT_SRC).
 """
 from __future__ import annotations
 
@@ -64,7 +64,7 @@ STYLE_CLASSES = [("ANGLE_CLASS", "angle_", "angle"), ("ATOM_CLASS", "atom_vec_",
                  ("READER_CLASS", "reader_", "reader"), ("REGION_CLASS", "region_", "region")]
 
 
-DEFAULT_SRC = "/root/reference/src"  # where this build's reference checkout lies
+DEFAULT_SRC = "/root/reference/src"  # the reference checkout of the machine that builds
 SOURCE_NOTE = os.path.join(OUT, "SOURCE")  # the tree the last build compiled
 
 

@@ -2,7 +2,7 @@
 type), for testing the decomposition driver (`lammps_b200.brick`) without a
 GPU.  Test infrastructure only.
 
-It keeps the properties the driver relies on: atoms addressed in upload
+It keeps the properties the brick driver (lammps_b200.brick) relies on: atoms addressed in upload
 order, lists built at rebuilds with the periodic image of each pair fixed
 until the next build, each atom's forces summed over its neighbors in
 ascending caller index, ghosts neither integrated nor distance-checked, and
@@ -134,3 +134,84 @@ class NumpyLJ:
 
     def halo_unpack(self, idx, buf):
         self.x[idx.numpy()] = buf.numpy()
+
+
+class NumpyEAM(NumpyLJ):
+    """EAM stand-in with the split compute of the engine (density pass, F'
+    pack/unpack by caller index, force pass): one element with analytic
+    rho(r) = exp(-2 (r - r0)) s(r), F(rho) = -sqrt(rho), phi(r) = exp(-3 (r - r0)) s(r),
+    s(r) = (1 - (r/rc)^2)^2 inside rc.  A ghost's own density is incomplete;
+    its F' must come from its owner through eam_fp_unpack."""
+
+    def __init__(self, lo, hi, rc=3.0, r0=1.2, mass=1.0, skin=0.3, every=1, delay=0, check=True,
+                 dt=0.002, units="lj"):
+        super().__init__(lo, hi, rc=rc, mass=mass, skin=skin, every=every, delay=delay,
+                         check=check, dt=dt, units=units)
+        from lammps_b200.pair import PairEAM
+        self.pair = PairEAM(1)  # marks the engine as EAM for the brick driver
+        self.r0 = r0
+        self.fp = None
+        self.emb = None
+
+    def _terms(self, rsq):
+        r = np.sqrt(rsq)
+        q = 1.0 - rsq / (self.rc * self.rc)
+        s, ds = q * q, -4.0 * q * r / (self.rc * self.rc)
+        a, b = np.exp(-2.0 * (r - self.r0)), np.exp(-3.0 * (r - self.r0))
+        return r, a * s, (-2.0 * a * s + a * ds), b * s, (-3.0 * b * s + b * ds)
+
+    def _pairs(self):
+        cutsq = self.rc * self.rc
+        for k in range(self.J.shape[1]):
+            j = self.J[:, k]
+            dl = self.x - (self.x[j] + self.S[:, k] * self.prd)
+            rsq = np.sum(dl * dl, axis=1)
+            m = self.ok[:, k] & (rsq < cutsq)
+            yield j, dl, np.where(m, rsq, 1.0), m
+
+    def eam_density(self, eflag=0, vflag=0):
+        rho = np.zeros(len(self.x))
+        for j, dl, rsq, m in self._pairs():
+            _, rh, _, _, _ = self._terms(rsq)
+            rho += np.where(m, rh, 0.0)
+        self.fp = -0.5 / np.sqrt(np.maximum(rho, 1e-300))
+        self.emb = -np.sqrt(rho)
+
+    def eam_fp_pack(self, idx, buf):
+        buf.copy_(torch.from_numpy(self.fp[idx.numpy()]))
+
+    def eam_fp_unpack(self, idx, buf):
+        ii = idx.numpy()
+        assert np.all(self.ghost[ii]), "F' unpack into an owned atom"
+        self.fp[ii] = buf.numpy()
+
+    def _force(self):
+        n = len(self.x)
+        f = np.zeros((n, 3))
+        e = self.emb.copy()
+        w = np.zeros((n, 6))
+        for j, dl, rsq, m in self._pairs():
+            r, _, drh, ph, dph = self._terms(rsq)
+            fpair = np.where(m, -((self.fp + self.fp[j]) * drh + dph) / r, 0.0)
+            f += fpair[:, None] * dl
+            e += np.where(m, 0.5 * ph, 0.0)
+            for c, (a, b) in enumerate(((0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2))):
+                w[:, c] += 0.5 * dl[:, a] * dl[:, b] * fpair
+        self.f = f
+        return dict(eng=float(e.sum()), virial=w.sum(axis=0), eatom=e, vatom=w)
+
+    def eam_force(self, eflag=0, vflag=0):
+        o = self._force()
+        return dict(eng=o["eng"], virial=o["virial"])
+
+    def eam_force_dev(self):
+        o = self._force()
+        return dict(eatom=torch.from_numpy(o["eatom"]), vatom=torch.from_numpy(o["vatom"]))
+
+    def compute(self, eflag=1, vflag=1, per_atom=False):
+        self.eam_density()
+        o = self._force()
+        out = dict(eng=o["eng"], virial=o["virial"])
+        if per_atom:
+            out.update(eatom=o["eatom"], vatom=o["vatom"])
+        return out

@@ -17,7 +17,7 @@ import torch.multiprocessing as mp  # noqa: E402
 from lammps_b200 import inputs  # noqa: E402
 from lammps_b200.brick import BrickGrid, BrickRun, DistComm, LocalComm, pbc  # noqa: E402
 
-from brick_numpy_engine import NumpyLJ  # noqa: E402
+from brick_numpy_engine import NumpyEAM, NumpyLJ  # noqa: E402
 
 NCELL = 5
 STEPS = 60
@@ -149,3 +149,68 @@ def test_merge_by_gid():
         assert np.array_equal(out[:, _GID], np.arange(na + nb) if na + nb == 1000 else np.sort(gid[:na + nb]))
         assert np.array_equal(out[pa.numpy()], a)
         assert np.array_equal(out[pb.numpy()], b)
+
+
+def _run_eam(comm, grid, ranks=None, steps=30):
+    """EAM over bricks: the density pass, the forward communication of F'
+    to the ghosts, the force pass (PairEAM::compute's passes and
+    forward_comm_pair, src/MANYBODY/pair_eam.cpp:160-303)."""
+    # 8 x 4 x 4 cells at a = 1.6: along x a brick of a 2 x 1 x 1 grid (6.4)
+    # plus its ghost depth (rc + skin = 2.3 each side) does not span the box,
+    # so the outermost ghosts lack part of their neighborhood and their own
+    # densities are wrong: only the forwarded F' gives the right forces
+    a = 1.6
+    x = inputs.lattice("fcc", 8, 4, 4, a)
+    rng = np.random.default_rng(11)
+    x = x + rng.normal(scale=0.03, size=x.shape)
+    v = rng.normal(scale=0.3, size=x.shape)
+    v -= v.mean(axis=0)
+    hi = [8 * a, 4 * a, 4 * a]
+    ranks = comm.ranks if ranks is None else ranks
+    eng = {r: NumpyEAM([0.0] * 3, hi, rc=2.0, every=1, delay=0, check=True) for r in ranks}
+    b = BrickRun(comm, eng, grid)
+    assert b.fp_halo == (comm.world > 1)
+    b.set_atoms(x, None, v)
+    b.setup()
+    rows = b.run(steps, thermo_every=20)
+    return b, rows, b.gather()
+
+
+def test_eam_bricks_reproduce_single_box():
+    """Ghosts carry their owners' F': every decomposition gives the
+    single-box trajectory bit for bit (with the ghosts' own, incomplete
+    densities the forces would differ)."""
+    b1, rows1, ref = _run_eam(LocalComm(1), (1, 1, 1))
+    for grid in ((2, 1, 1), (1, 2, 2)):
+        b, rows, got = _run_eam(LocalComm(int(np.prod(grid))), grid)
+        assert b.ncalls == b1.ncalls, grid
+        for k in ("x", "v", "image"):
+            assert np.array_equal(got[k], ref[k]), (grid, k)
+        for r1, r2 in zip(rows1, rows):
+            for k in ("Temp", "E_pair", "Press"):
+                assert r2[k] == pytest.approx(r1[k], rel=1e-12, abs=1e-12), (grid, k)
+
+
+def _eam_worker(rank, port, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=2)
+    try:
+        b, rows, g = _run_eam(DistComm(), (2, 1, 1), ranks=[rank])
+        if rank == 0:
+            np.savez(out, x=g["x"], v=g["v"], ncalls=b.ncalls, temp=[r["Temp"] for r in rows])
+    finally:
+        dist.destroy_process_group()
+
+
+def test_eam_two_gloo_ranks_reproduce_single_box(tmp_path):
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    out = str(tmp_path / "eam.npz")
+    mp.start_processes(_eam_worker, args=(port, out), nprocs=2, start_method="spawn", join=True)
+    b1, rows1, ref = _run_eam(LocalComm(1), (1, 1, 1))
+    res = np.load(out)
+    assert int(res["ncalls"]) == b1.ncalls
+    assert np.array_equal(res["x"], ref["x"])
+    assert np.array_equal(res["v"], ref["v"])
