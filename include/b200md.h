@@ -118,6 +118,32 @@ int b200_upload_atoms(b200_ctx *ctx, int n, const double *x, const double *v, co
    order (NULL pointers are skipped; image is 3 ints per atom). */
 int b200_download_atoms(b200_ctx *ctx, double *x, double *v, double *f, int *image);
 int b200_natoms(const b200_ctx *ctx);
+
+/* Overlapped transfers, for a caller that runs one atom set after another:
+   each set's host copies overlap the device work of the set before it, as the
+   reference's GPU library overlaps its asynchronous position upload and
+   answer download with the host's work (Atom::add_x_data,
+   lib/gpu/lal_atom.h:282-297; Answer::copy_answers, lib/gpu/lal_answer.cpp:140-162).
+   The context copies on two streams of its own (one per direction) through
+   device buffers of its own; page-locked host memory lets the copies run
+   beside the kernels.
+
+   b200_stage_atoms starts copying an atom set (the arguments of
+   b200_upload_atoms, without tag) into one of two device slots and returns
+   without waiting.  The host arrays must stay unchanged until
+   b200_set_staged_atoms has taken the set.  At most two sets wait at a time
+   (B200_ERR_STATE beyond that).
+   b200_set_staged_atoms makes the oldest staged set the context's atoms:
+   b200_upload_atoms from the slot, once its copy has arrived; its types are
+   checked on the device (B200_ERR_ARG for a type outside 1..ntypes).
+   b200_download_atoms_async forms the arrays of b200_download_atoms on the
+   device now and copies them to the host arrays while later work runs; they
+   are valid after b200_wait_transfers, which waits for every copy started
+   by either call. */
+int b200_stage_atoms(b200_ctx *ctx, int n, const double *x, const double *v, const int *type);
+int b200_set_staged_atoms(b200_ctx *ctx);
+int b200_download_atoms_async(b200_ctx *ctx, double *x, double *v, double *f, int *image);
+int b200_wait_transfers(b200_ctx *ctx);
 /* New positions x[3n] (caller order, host or device memory) for the atoms of
    the last upload, keeping their cells and the neighbor list of the last
    build: the per-step position refresh of a Pair::compute between

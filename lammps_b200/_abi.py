@@ -12,6 +12,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_lib", "libb200md.so")
 
 B200_OK = 0
+B200_ERR_STATE = -4
 STATUS_NAMES = {
     0: "B200_OK", -1: "B200_ERR_ARG", -2: "B200_ERR_CUDA", -3: "B200_ERR_NOMEM",
     -4: "B200_ERR_STATE", -5: "B200_ERR_NEIGH_OVERFLOW", -6: "B200_ERR_BOX",
@@ -41,6 +42,10 @@ SIGNATURES = {
     "b200_upload_atoms": (C.c_int, [_vp, C.c_int, _dp, _dp, _ip, _ip]),
     "b200_download_atoms": (C.c_int, [_vp, _dp, _dp, _dp, _ip]),
     "b200_natoms": (C.c_int, [_vp]),
+    "b200_stage_atoms": (C.c_int, [_vp, C.c_int, _dp, _dp, _ip]),
+    "b200_set_staged_atoms": (C.c_int, [_vp]),
+    "b200_download_atoms_async": (C.c_int, [_vp, _dp, _dp, _dp, _ip]),
+    "b200_wait_transfers": (C.c_int, [_vp]),
     "b200_update_positions": (C.c_int, [_vp, _dp]),
     "b200_gather": (C.c_int, [_vp, C.c_int, C.c_int, _ip, _dp]),
     "b200_set_replica_step": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int]),

@@ -870,6 +870,17 @@ int b200_destroy(b200_ctx *c) {
   if (!c) return B200_OK;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->s_h2d) {
+    cudaStreamSynchronize(c->s_h2d);
+    cudaStreamSynchronize(c->s_d2h);
+    for (auto *s : {&c->in_slot[0], &c->in_slot[1], &c->out_slot[0], &c->out_slot[1]}) {
+      if (s->buf) cudaFree(s->buf);
+      if (s->ready) cudaEventDestroy(s->ready);
+      if (s->done) cudaEventDestroy(s->done);
+    }
+    cudaStreamDestroy(c->s_h2d);
+    cudaStreamDestroy(c->s_d2h);
+  }
   invalidate_graphs(c);
   dfree(c->x4); dfree(c->x4b); dfree(c->v); dfree(c->vb); dfree(c->f);
   dfree(c->orig); dfree(c->origb); dfree(c->image); dfree(c->imageb); dfree(c->cell);
@@ -1115,17 +1126,22 @@ int b200_upload_atoms(b200_ctx *c, int n, const double *x, const double *v, cons
   }
   c->n = n;
   CK(cudaMemsetAsync(c->f, 0, 3 * (size_t)c->stride * sizeof(double), c->stream));
+  // host sources are copied into the staging buffer; device sources are read
+  // by the upload kernel where they are
+  const bool dev_x = is_device_ptr(x), dev_v = v && is_device_ptr(v);
   char *st[3];
-  const size_t sb[3] = {3 * (size_t)n * sizeof(double), v ? 3 * (size_t)n * sizeof(double) : 0,
-                        (size_t)n * sizeof(int)};
+  const size_t b3 = 3 * (size_t)n * sizeof(double);
+  const size_t sb[3] = {dev_x ? 0 : b3, (v && !dev_v) ? b3 : 0,
+                        dev_type ? 0 : (size_t)n * sizeof(int)};
   int rc = xfer_parts(c, 3, sb, st);
   if (rc) return rc;
-  double *dx = reinterpret_cast<double *>(st[0]), *dv = reinterpret_cast<double *>(st[1]);
-  int *dt = reinterpret_cast<int *>(st[2]);
-  // host or device sources (unified addressing)
-  CK(cudaMemcpyAsync(dx, x, 3 * (size_t)n * sizeof(double), cudaMemcpyDefault, c->stream));
-  if (v) CK(cudaMemcpyAsync(dv, v, 3 * (size_t)n * sizeof(double), cudaMemcpyDefault, c->stream));
-  CK(cudaMemcpyAsync(dt, type, (size_t)n * sizeof(int), cudaMemcpyDefault, c->stream));
+  const double *dx = dev_x ? x : reinterpret_cast<const double *>(st[0]);
+  const double *dv = (!v || dev_v) ? v : reinterpret_cast<const double *>(st[1]);
+  const int *dt = dev_type ? type : reinterpret_cast<const int *>(st[2]);
+  if (!dev_x) CK(cudaMemcpyAsync(st[0], x, b3, cudaMemcpyHostToDevice, c->stream));
+  if (v && !dev_v) CK(cudaMemcpyAsync(st[1], v, b3, cudaMemcpyHostToDevice, c->stream));
+  if (!dev_type)
+    CK(cudaMemcpyAsync(st[2], type, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemsetAsync(c->status + ST_BADTYPE, 0, sizeof(int), c->stream));
   k_upload<<<md_blocks(n, 256), 256, 0, c->stream>>>(n, c->stride, c->ntypes, dx, dv, dt, c->x4,
                                                      c->v, c->orig, c->image, c->cell, c->status);
@@ -1228,6 +1244,122 @@ int b200_download_atoms(b200_ctx *c, double *x, double *v, double *f, int *image
   if (f) CK(cudaMemcpyAsync(f, df, 3 * (size_t)n * sizeof(double), cudaMemcpyDefault, c->stream));
   if (image) CK(cudaMemcpyAsync(image, di, 3 * (size_t)n * sizeof(int), cudaMemcpyDefault, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  return B200_OK;
+}
+
+// ---- overlapped transfers ----------------------------------------------------
+
+// the copy streams and the slots' events, made on first use
+static int xfer_streams(b200_ctx *c) {
+  if (c->s_h2d) return B200_OK;
+  CK(cudaStreamCreateWithFlags(&c->s_h2d, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&c->s_d2h, cudaStreamNonBlocking));
+  for (auto *s : {&c->in_slot[0], &c->in_slot[1], &c->out_slot[0], &c->out_slot[1]}) {
+    CK(cudaEventCreateWithFlags(&s->ready, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&s->done, cudaEventDisableTiming));
+  }
+  return B200_OK;
+}
+
+// a slot's device buffer of at least `bytes` (the slot is idle when called)
+static int slot_reserve(b200_ctx *c, b200_ctx::XferSlot &s, size_t bytes) {
+  if (s.bytes >= bytes) return B200_OK;
+  if (s.buf) CK(cudaFree(s.buf));
+  s.buf = nullptr;
+  s.bytes = 0;
+  CK(cudaMalloc((void **)&s.buf, bytes));
+  s.bytes = bytes;
+  return B200_OK;
+}
+
+static size_t part_bytes(size_t b) { return (b + 255) & ~(size_t)255; }
+
+int b200_stage_atoms(b200_ctx *c, int n, const double *x, const double *v, const int *type) {
+  if (!c || n < 1 || !x || !type) return set_err(c, B200_ERR_ARG, "stage: illegal atoms");
+  if (n > MD_MAX_ATOMS) return set_err(c, B200_ERR_ARG, "too many atoms (%d > %d)", n, MD_MAX_ATOMS);
+  if (c->in_count == 2) return set_err(c, B200_ERR_STATE, "stage: two atom sets are staged already");
+  CK(cudaSetDevice(c->device));
+  int rc = xfer_streams(c);
+  if (rc) return rc;
+  b200_ctx::XferSlot &s = c->in_slot[(c->in_head + c->in_count) % 2];
+  const size_t b3 = 3 * (size_t)n * sizeof(double), bt = (size_t)n * sizeof(int);
+  // a free slot: the set it held was taken by b200_set_staged_atoms, which
+  // returns after the upload that read it
+  rc = slot_reserve(c, s, 2 * part_bytes(b3) + part_bytes(bt));
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(s.buf, x, b3, cudaMemcpyDefault, c->s_h2d));
+  if (v) CK(cudaMemcpyAsync(s.buf + part_bytes(b3), v, b3, cudaMemcpyDefault, c->s_h2d));
+  CK(cudaMemcpyAsync(s.buf + 2 * part_bytes(b3), type, bt, cudaMemcpyDefault, c->s_h2d));
+  CK(cudaEventRecord(s.ready, c->s_h2d));
+  s.n = n;
+  s.has_v = v != nullptr;
+  c->in_count++;
+  return B200_OK;
+}
+
+int b200_set_staged_atoms(b200_ctx *c) {
+  if (!c) return B200_ERR_ARG;
+  if (c->in_count == 0) return set_err(c, B200_ERR_STATE, "no staged atom set");
+  CK(cudaSetDevice(c->device));
+  b200_ctx::XferSlot &s = c->in_slot[c->in_head];
+  c->in_head = (c->in_head + 1) % 2;
+  c->in_count--;
+  // the upload waits for the set's copy on the device, then reads the slot
+  // (device memory: the types are checked by the upload kernel)
+  CK(cudaStreamWaitEvent(c->stream, s.ready, 0));
+  const size_t b3 = part_bytes(3 * (size_t)s.n * sizeof(double));
+  return b200_upload_atoms(c, s.n, reinterpret_cast<const double *>(s.buf),
+                           s.has_v ? reinterpret_cast<const double *>(s.buf + b3) : nullptr,
+                           reinterpret_cast<const int *>(s.buf + 2 * b3), nullptr);
+}
+
+int b200_download_atoms_async(b200_ctx *c, double *x, double *v, double *f, int *image) {
+  if (!c) return B200_ERR_ARG;
+  if (!c->have_atoms) return set_err(c, B200_ERR_STATE, "no atoms uploaded");
+  CK(cudaSetDevice(c->device));
+  int rc = xfer_streams(c);
+  if (rc) return rc;
+  const int n = c->n;
+  b200_ctx::XferSlot &s = c->out_slot[c->out_next];
+  c->out_next ^= 1;
+  const size_t d3 = 3 * (size_t)n * sizeof(double), i3 = 3 * (size_t)n * sizeof(int);
+  const size_t pb[4] = {x ? part_bytes(d3) : 0, v ? part_bytes(d3) : 0, f ? part_bytes(d3) : 0,
+                        image ? part_bytes(i3) : 0};
+  const size_t need = pb[0] + pb[1] + pb[2] + pb[3];
+  if (s.used && s.bytes < need) CK(cudaEventSynchronize(s.done));  // before freeing it
+  rc = slot_reserve(c, s, need);
+  if (rc) return rc;
+  // the slot's previous copy to the host ends before the slot is written
+  if (s.used) CK(cudaStreamWaitEvent(c->stream, s.done, 0));
+  char *p[4];
+  size_t off = 0;
+  for (int k = 0; k < 4; k++) {
+    p[k] = pb[k] ? s.buf + off : nullptr;
+    off += pb[k];
+  }
+  k_unsort<<<md_blocks(n, 256), 256, 0, c->stream>>>(
+      n, c->stride, c->orig, c->x4, c->v, c->f, c->image, reinterpret_cast<double *>(p[0]),
+      reinterpret_cast<double *>(p[1]), reinterpret_cast<double *>(p[2]),
+      reinterpret_cast<int *>(p[3]));
+  c->launches++;
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(s.ready, c->stream));
+  CK(cudaStreamWaitEvent(c->s_d2h, s.ready, 0));
+  if (x) CK(cudaMemcpyAsync(x, p[0], d3, cudaMemcpyDefault, c->s_d2h));
+  if (v) CK(cudaMemcpyAsync(v, p[1], d3, cudaMemcpyDefault, c->s_d2h));
+  if (f) CK(cudaMemcpyAsync(f, p[2], d3, cudaMemcpyDefault, c->s_d2h));
+  if (image) CK(cudaMemcpyAsync(image, p[3], i3, cudaMemcpyDefault, c->s_d2h));
+  CK(cudaEventRecord(s.done, c->s_d2h));
+  s.used = true;
+  return B200_OK;
+}
+
+int b200_wait_transfers(b200_ctx *c) {
+  if (!c) return B200_ERR_ARG;
+  if (!c->s_h2d) return B200_OK;
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->s_h2d));
+  CK(cudaStreamSynchronize(c->s_d2h));
   return B200_OK;
 }
 

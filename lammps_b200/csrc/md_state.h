@@ -106,6 +106,20 @@ struct b200_ctx {
   // virial), kept between calls so a call maps no new memory
   char *xfer = nullptr;
   size_t xfer_bytes = 0;
+  // overlapped transfers (b200_stage_atoms, b200_download_atoms_async): one
+  // copy stream per direction, two staged input sets and two download slots
+  struct XferSlot {
+    char *buf = nullptr;
+    size_t bytes = 0;
+    int n = 0;
+    bool has_v = false, used = false;
+    cudaEvent_t ready = nullptr;  // input: copy done; output: caller order formed
+    cudaEvent_t done = nullptr;   // output: copy to the host done
+  };
+  cudaStream_t s_h2d = nullptr, s_d2h = nullptr;
+  XferSlot in_slot[2], out_slot[2];
+  int in_head = 0, in_count = 0;  // oldest staged input set, sets waiting
+  int out_next = 0;
   double *rho = nullptr, *fp = nullptr;
   float *fpf = nullptr;
   // split EAM compute (b200_eam_density, then b200_eam_force): the eflag /

@@ -47,6 +47,8 @@ class System:
         self.box_lo = self.box_hi = None
         self.ntimestep = 0
         self.thermo_rows = []
+        self._staged = []   # (n, type, arrays) of staged atom sets, oldest first
+        self._pending = []  # host arrays of downloads still in flight
 
     def __del__(self):
         try:
@@ -154,6 +156,52 @@ class System:
         self._ck(self._L.b200_download_atoms(self._h, _abi.dptr(out["x"]), _abi.dptr(out["v"]),
                                              _abi.dptr(out["f"]), _abi.iptr(out["image"])))
         return out
+
+    # ---- overlapped transfers: one atom set after another -------------------
+    def stage_atoms(self, x, type_=None, v=None):
+        """Start copying an atom set to the device (b200_stage_atoms); it
+        becomes the context's atoms at set_staged_atoms.  The arrays are held,
+        and must not change, until then.  Page-locked arrays (e.g. the numpy
+        view of a pinned torch tensor) let the copy run beside the steps of
+        the current set."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        n = x.shape[0]
+        t = np.ones(n, np.int32) if type_ is None else np.ascontiguousarray(type_, dtype=np.int32)
+        vv = None if v is None else np.ascontiguousarray(v, dtype=np.float64)
+        self._ck(self._L.b200_stage_atoms(self._h, n, _abi.dptr(x), _abi.dptr(vv), _abi.iptr(t)))
+        self._staged.append((n, t, (x, vv)))
+
+    def set_staged_atoms(self):
+        """The oldest staged set becomes the context's atoms (as set_atoms)."""
+        if not self._staged:
+            raise _abi.B200Error(_abi.B200_ERR_STATE, "no staged atom set")
+        n, t, _ = self._staged.pop(0)
+        self._ck(self._L.b200_set_staged_atoms(self._h))
+        self.n = n
+        self.type = t
+
+    def download_async(self, out):
+        """download() into the caller's arrays `out` without waiting: the
+        arrays are filled while later work runs and are valid after
+        wait_transfers()."""
+        n = self.n
+        for k, dt in (("x", np.float64), ("v", np.float64), ("f", np.float64),
+                      ("image", np.int32)):
+            a = out.get(k)
+            if a is not None and (a.shape != (n, 3) or a.dtype != dt or
+                                  not a.flags["C_CONTIGUOUS"]):
+                raise ValueError(f"download_async: out[{k!r}] must be a C-contiguous ({n}, 3) "
+                                 f"{np.dtype(dt)}")
+        self._ck(self._L.b200_download_atoms_async(
+            self._h, _abi.dptr(out.get("x")), _abi.dptr(out.get("v")), _abi.dptr(out.get("f")),
+            _abi.iptr(out.get("image"))))
+        self._pending.append(out)
+        return out
+
+    def wait_transfers(self):
+        """Wait for every copy of stage_atoms and download_async."""
+        self._ck(self._L.b200_wait_transfers(self._h))
+        self._pending = []
 
     def gather(self, fields=("x", "v", "f", "image"), idx=None):
         """Per-atom columns straight from the device, as a dump writes them:

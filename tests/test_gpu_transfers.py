@@ -14,7 +14,10 @@ pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
 
 
-def _system(edge=20.0):
+def _system(edge=20.0, tpa=None):
+    """An FP64 LJ context; `tpa` fixes the pair kernels' launch shape (without
+    it the first setup picks one by timing, and contexts with different
+    shapes agree to rounding, not bit for bit)."""
     s = System("lj", "fp64")
     s.set_box([0.0, 0.0, 0.0], [edge] * 3)
     p = PairLJCut(2.5)
@@ -22,6 +25,8 @@ def _system(edge=20.0):
     s.set_pair(p)
     s.set_mass([1.0])
     s.set_neighbor(0.3, 20, 0, False)
+    if tpa:
+        s.set_launch(tpa, 128)
     return s
 
 
@@ -88,4 +93,85 @@ def test_device_pointer_upload_download():
     tt[1234] = 7
     with pytest.raises(B200Error, match="atom 1234"):
         s.set_atoms_dev(xt, tt, vt)
+    s.close()
+
+
+def _sets():
+    """Three atom sets: two LJ lattices of one size with different
+    velocities, and a smaller lattice."""
+    a = inputs.lj_lattice_constant("fcc", 0.8442)
+    out = []
+    for cells, seed in ((8, 1), (8, 2), (6, 3)):
+        x = inputs.lattice("fcc", cells, cells, cells, a)
+        v = np.random.default_rng(seed).normal(size=(len(x), 3))
+        out.append((x, v, cells * a))
+    return out
+
+
+def test_overlapped_transfers_match_blocking():
+    """Stage the next set while the current one runs, download without
+    waiting: every set's results equal those of the blocking calls."""
+    keep = []
+
+    def pinned(a):
+        t = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+        keep.append(t)
+        return t.numpy()
+
+    sets = _sets()
+    ref = []
+    for x, v, edge in sets:
+        s = _system(edge, tpa=4)
+        s.set_atoms(x, None, v)
+        s.setup()
+        s.run(10)
+        ref.append(s.download())
+        s.close()
+    got = []
+    s = None
+    for k, (x, v, edge) in enumerate(sets):
+        if s is None or s.box_hi[0] != edge:
+            if s is not None:
+                s.wait_transfers()
+                s.close()
+            s = _system(edge, tpa=4)
+            s.stage_atoms(pinned(x), pinned(np.ones(len(x), np.int32)), pinned(v))
+        s.set_staged_atoms()
+        if k + 1 < len(sets) and sets[k + 1][2] == edge:
+            nx, nv, _ = sets[k + 1]
+            s.stage_atoms(pinned(nx), pinned(np.ones(len(nx), np.int32)), pinned(nv))
+        s.setup()
+        s.run(10)
+        n = len(x)
+        out = {"x": pinned(np.zeros((n, 3))), "v": pinned(np.zeros((n, 3))),
+               "f": pinned(np.zeros((n, 3))), "image": pinned(np.zeros((n, 3), np.int32))}
+        got.append(s.download_async(out))
+    s.wait_transfers()
+    s.close()
+    for k, (r, g) in enumerate(zip(ref, got)):
+        for key in ("x", "v", "f", "image"):
+            assert np.array_equal(g[key], r[key]), (k, key)
+
+
+def test_staging_errors_leave_the_context_usable():
+    x, v, edge = _sets()[0]
+    n = len(x)
+    s = _system(edge)
+    with pytest.raises(B200Error, match="STATE"):
+        s.set_staged_atoms()
+    bad = np.ones(n, np.int32)
+    bad[17] = 3
+    s.stage_atoms(x, bad, v)
+    s.stage_atoms(x, None, v)
+    with pytest.raises(B200Error, match="two atom sets"):
+        s.stage_atoms(x, None, v)
+    with pytest.raises(B200Error, match="atom 17"):
+        s.set_staged_atoms()
+    s.set_staged_atoms()
+    s.setup()
+    s.run(5)
+    out = {k: np.zeros((n, 3)) for k in ("x", "v", "f")}
+    s.download_async(out)
+    s.wait_transfers()
+    assert np.array_equal(out["x"], s.download()["x"])
     s.close()
