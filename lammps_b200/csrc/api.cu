@@ -421,12 +421,33 @@ int default_capacity(const b200_ctx *c) {
   return cap;
 }
 
-int read_status(b200_ctx *c) {
-  CK(cudaMemcpyAsync(c->status_host, c->status, ST_COUNT * sizeof(int), cudaMemcpyDeviceToHost,
-                     c->stream));
+// Small device-to-host reads (status words, energy and virial sums, step
+// counters) go through mapped page-locked memory, written by a one-warp
+// kernel on the context's stream.  A copy engine would queue them behind a
+// bulk transfer in flight in the same direction (b200_download_atoms_async),
+// and the host would wait for that transfer to end.
+constexpr int kBounceBytes = 4096;
+
+__global__ void k_small_read(const int *__restrict__ src, int *__restrict__ dst, int nwords) {
+  for (int k = threadIdx.x; k < nwords; k += blockDim.x) dst[k] = src[k];
+  __threadfence_system();
+}
+
+// `bytes` (a multiple of 4, at most kBounceBytes) from device `dev` into host
+// `host`, after the work already queued on the stream
+int small_read(b200_ctx *c, void *host, const void *dev, size_t bytes) {
+  if (bytes % 4 != 0 || bytes > (size_t)kBounceBytes)
+    return set_err(c, B200_ERR_ARG, "small read of %zu bytes", bytes);
+  k_small_read<<<1, 32, 0, c->stream>>>(reinterpret_cast<const int *>(dev), c->bounce_dev,
+                                        (int)(bytes / 4));
+  c->launches++;
+  CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->stream));
+  std::memcpy(host, c->bounce_host, bytes);
   return B200_OK;
 }
+
+int read_status(b200_ctx *c) { return small_read(c, c->status_host, c->status, ST_COUNT * sizeof(int)); }
 
 int status_errors(b200_ctx *c) {
   if (c->status_host[ST_LOST])
@@ -597,10 +618,9 @@ int tune_replica_step(b200_ctx *c) {
   c->rep_tune_ms[0] = c->rep_tune_ms[1] = 0.0;
   if (!c->nrep || !lj || c->rep_mode == 1) return B200_OK;
   int status_save[ST_COUNT], dcount_save = 0;
-  CK(cudaMemcpyAsync(status_save, c->status, sizeof(status_save), cudaMemcpyDeviceToHost,
-                     c->stream));
-  CK(cudaMemcpyAsync(&dcount_save, c->dec_count, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
+  int rc0 = small_read(c, status_save, c->status, sizeof(status_save));
+  if (!rc0) rc0 = small_read(c, &dcount_save, c->dec_count, sizeof(int));
+  if (rc0) return rc0;
   const int mail_save[2] = {c->mail_host[0], c->mail_host[1]};
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
@@ -713,11 +733,10 @@ int wait_decision(b200_ctx *c, bool *rebuild) {
         std::chrono::steady_clock::now() - t0 > std::chrono::milliseconds(200))
       break;
   }
-  CK(cudaMemcpyAsync(&c->status_host[ST_REBUILD], c->status + ST_REBUILD, sizeof(int),
-                     cudaMemcpyDeviceToHost, c->stream));
   int dc = 0;
-  CK(cudaMemcpyAsync(&dc, c->dec_count, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
+  int rc1 = small_read(c, &c->status_host[ST_REBUILD], c->status + ST_REBUILD, sizeof(int));
+  if (!rc1) rc1 = small_read(c, &dc, c->dec_count, sizeof(int));
+  if (rc1) return rc1;
   c->decisions = (unsigned int)dc;
   *rebuild = c->status_host[ST_REBUILD] != 0;
   return B200_OK;
@@ -850,6 +869,8 @@ int b200_create(int device, int precision, b200_ctx **out) {
     c->mail_host[0] = c->mail_host[1] = 0;
     e = cudaHostGetDevicePointer((void **)&c->mail_dev, c->mail_host, 0);
   }
+  if (e == cudaSuccess) e = cudaHostAlloc((void **)&c->bounce_host, kBounceBytes, cudaHostAllocMapped);
+  if (e == cudaSuccess) e = cudaHostGetDevicePointer((void **)&c->bounce_dev, c->bounce_host, 0);
   if (e == cudaSuccess) e = cudaMalloc((void **)&c->dec_count, sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(c->dec_count, 0, sizeof(int));
   if (e == cudaSuccess) e = cudaMalloc((void **)&c->ev, 8 * sizeof(double));
@@ -904,6 +925,7 @@ int b200_destroy(b200_ctx *c) {
   for (auto ev : c->ev_pool) cudaEventDestroy(ev);
   if (c->status_host) cudaFreeHost(c->status_host);
   if (c->mail_host) cudaFreeHost(c->mail_host);
+  if (c->bounce_host) cudaFreeHost(c->bounce_host);
   dfree(c->dec_count);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -1554,8 +1576,8 @@ int b200_setup(b200_ctx *c, double *row) {
   if (rc) return rc;
   CK(md_ke(c));
   double h[8];
-  CK(cudaMemcpyAsync(h, c->ev, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
+  rc = small_read(c, h, c->ev, sizeof(h));
+  if (rc) return rc;
   if (row) {
     row[0] = 0.0;
     row[1] = h[7];
@@ -1598,9 +1620,8 @@ int b200_run(b200_ctx *c, int nsteps, double dt, double ftm2v, int thermo_every,
   CK(cudaMemsetAsync(c->status + ST_OVERFLOW, 0, sizeof(int), c->stream));
   CK(cudaMemsetAsync(c->status + ST_MAXNEIGH, 0, sizeof(int), c->stream));
   // host view of the current step for the output schedule
-  CK(cudaMemcpyAsync(c->status_host, c->status, ST_COUNT * sizeof(int), cudaMemcpyDeviceToHost,
-                     c->stream));
-  CK(cudaStreamSynchronize(c->stream));
+  int rc2 = read_status(c);
+  if (rc2) return rc2;
   long long step0 = ((long long)(unsigned int)c->status_host[ST_STEP_HI] << 32) |
                     (long long)(unsigned int)c->status_host[ST_STEP_LO];
   const long long last = step0 + nsteps;

@@ -168,6 +168,9 @@ struct b200_ctx {
   // words, which run-chunk snapshots restore) and decisions the host's count
   // of the decisions it has waited for
   int *mail_host = nullptr, *mail_dev = nullptr;
+  // mapped page-locked bounce buffer of the small device-to-host reads
+  // (status words, energy/virial sums), written by a one-warp kernel
+  int *bounce_host = nullptr, *bounce_dev = nullptr;
   int *dec_count = nullptr;
   unsigned int decisions = 0;
   double *rows = nullptr;        // device thermo rows (9 doubles each)
