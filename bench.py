@@ -906,6 +906,73 @@ def eam32k_block(torch, flush, K, W, setfl, clk, no_cpu, oracle=True):
     return out
 
 
+def replica_scripts(steps, every=1):
+    """(atoms, reference input) of every `every`-th replica of the 256-replica
+    batch: the box as the batch builds it (fcc at the replica's density, its
+    Gaussian velocities from its seed with loop geom), lj/cut rc 2.5, skin 0.3,
+    every 20 delay 0 check no, dt 0.005, the first `steps` NVE steps."""
+    from lammps_b200.replicas import replica_batch
+    b = replica_batch()
+    out = []
+    for k in range(0, len(b["natoms"]), every):
+        n = int(b["ncells"][k])
+        out.append((int(b["natoms"][k]), [
+            "units lj", "atom_style atomic", f"lattice fcc {b['rho'][k]:.17g}",
+            f"region box block 0 {n} 0 {n} 0 {n}", "create_box 1 box", "create_atoms 1 box",
+            "mass 1 1.0",
+            f"velocity all create {b['temp'][k]:.17g} {int(b['seeds'][k])} dist gaussian loop geom",
+            "pair_style lj/cut 2.5", "pair_coeff 1 1 1.0 1.0 2.5", "neighbor 0.3 bin",
+            "neigh_modify delay 0 every 20 check no", "fix 1 all nve", "timestep 0.005",
+            f"thermo {steps}", f"run {steps}", "clear"]))
+    return out
+
+
+def reference_cpu_replicas(procs, steps, every=1, timeout=900):
+    """Matom-steps/s of the reference's own binary on the 256-replica batch
+    (or every `every`-th replica): `procs` concurrent single-threaded
+    processes (plain styles), each running its share of the replicas one
+    after another; the rate is the atom-steps of all replicas over the
+    largest per-process sum of Loop times (setup excluded, as elsewhere)."""
+    import re
+    import shutil
+    exe = reference_binary()
+    reps = replica_scripts(steps, every)
+    # largest replicas first, each to the process with the least work so far
+    order = sorted(range(len(reps)), key=lambda k: -reps[k][0])
+    share = [[] for _ in range(procs)]
+    load = [0] * procs
+    for k in order:
+        p = load.index(min(load))
+        share[p].append(k)
+        load[p] += reps[k][0]
+    tmp = tempfile.mkdtemp(prefix="b200rep_")
+    env = dict(os.environ, OMP_NUM_THREADS="1")
+    try:
+        runs = []
+        for p, ks in enumerate(share):
+            if not ks:
+                continue
+            name = f"in.share{p}"
+            with open(os.path.join(tmp, name), "w") as fh:
+                fh.write("\n".join(line for k in ks for line in reps[k][1]) + "\n")
+            runs.append((ks, subprocess.Popen([exe, "-in", name, "-log", "none", "-echo", "none"],
+                                              cwd=tmp, env=env, stdout=subprocess.PIPE,
+                                              stderr=subprocess.STDOUT, text=True)))
+        secs = []
+        for ks, pr in runs:
+            out, _ = pr.communicate(timeout=timeout)
+            t = [float(x) for x in re.findall(r"Loop time of (\S+) on", out)]
+            if pr.returncode != 0 or len(t) != len(ks):
+                raise RuntimeError(f"lmp_serial replica share failed ({pr.returncode}): {out[-500:]}")
+            secs.append(sum(t))
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    atoms = sum(r[0] for r in reps)
+    return {"value": atoms * steps / max(secs) / 1e6, "unit": "Matom-steps/s", "processes": procs,
+            "replicas": len(reps), "atoms": atoms, "steps": steps,
+            "replica_steps_per_s": len(reps) * steps / max(secs)}
+
+
 def cpu_rows(setfl):
     """The reference's own CPU path on each configuration that runs on a
     CPU in seconds: one core (plain styles) and all cores (-sf omp)."""
@@ -915,6 +982,11 @@ def cpu_rows(setfl):
                       "all_cores": reference_cpu("lj32k", host["cores"], 3)["value"]}
     rows["eam_32k"] = {"one_core": reference_cpu("eam32k", 1, 1, setfl=setfl)["value"],
                        "all_cores": reference_cpu("eam32k", host["cores"], 3, setfl=setfl)["value"]}
+    rows["replicas_256"] = {
+        "one_core": reference_cpu_replicas(1, MD_STEPS, every=4),
+        "all_cores": reference_cpu_replicas(host["cores"], MD_STEPS),
+        "note": "the first 100 steps of each replica; one core: every 4th replica in one "
+                "process; all cores: all 256 replicas over one single-threaded process per core"}
     rows["note"] = ("Matom-steps/s of fresh runs of the first 100 steps from the seeded state "
                     "(median of the all-core runs); lj_4M is in cpu_baseline")
     return rows
