@@ -49,15 +49,18 @@ enum b200_status {
   B200_ERR_NOMEM = -3,          /* device allocation failed */
   B200_ERR_STATE = -4,          /* call out of order (e.g. compute before atoms) */
   B200_ERR_NEIGH_OVERFLOW = -5, /* "Neighbor list overflow, boost neigh_modify one" */
-  B200_ERR_BOX = -6,            /* box edge not larger than the ghost cutoff */
+  B200_ERR_BOX = -6,            /* box edge not larger than the ghost cutoff (mixed form:
+                                   not longer than twice the list cutoff) */
   B200_ERR_LOST_ATOMS = -7,     /* non-finite coordinate or atom beyond one box image */
   B200_ERR_TIMEOUT = -8         /* a bounded device wait expired */
 };
 
 enum b200_precision {
   B200_PREC_FP64 = 0,  /* all pair arithmetic in FP64: the drop-in form */
-  B200_PREC_MIXED = 1  /* FP32 pair math on cell-relative coordinates,
-                          FP64 positions, per-atom force sums and global sums */
+  B200_PREC_MIXED = 1  /* FP32 pair math on separations from 32-bit fixed-point
+                          coordinates (box edges must exceed twice the list
+                          cutoff), FP64 positions, per-atom force sums and
+                          global sums */
 };
 
 enum b200_pair_style { B200_PAIR_NONE = 0, B200_PAIR_LJ_CUT = 1, B200_PAIR_EAM = 2 };

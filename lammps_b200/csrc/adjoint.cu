@@ -18,8 +18,9 @@
 // not differentiated: a pair that crosses r = rc under a parameter change
 // contributes a jump that finite differences see and this gradient does not.
 //
-// MIXED: FP32 pair arithmetic on the cell-relative FP32 coordinates (as the
-// mixed force kernels), FP64 accumulation of forces, gradients and sums.
+// MIXED: FP32 pair arithmetic on separations formed from the fixed-point
+// coordinates (md_xq, as the mixed force kernels), FP64 accumulation of
+// forces, gradients and sums.
 #include "md_state.h"
 
 namespace {
@@ -35,21 +36,22 @@ struct AdjTables {
 template <bool MIXED>
 __device__ __forceinline__ void pair_geom(const AdjTables &T, int i, unsigned e,
                                           const double4 *__restrict__ x4,
-                                          const float4 *__restrict__ xr, const Shift3 &sx,
-                                          const Shift3 &sy, const Shift3 &sz, float csx,
-                                          float csy, float csz, double &dx, double &dy,
+                                          const int4 *__restrict__ xq, const Shift3 &sx,
+                                          const Shift3 &sy, const Shift3 &sz, const float *qh,
+                                          const float *ql, double &dx, double &dy,
                                           double &dz, double &rsq, int &tt) {
   const int j = md_entry_j(e);
   if (MIXED) {
-    const float4 xi = xr[i], xj = xr[j];
-    const float fx = fmaf(-md_code_dx(e), csx, xi.x - xj.x);
-    const float fy = fmaf(-md_code_dy4(e), 0.25f * csy, xi.y - xj.y);
-    const float fz = fmaf(-md_code_dz16(e), 0.0625f * csz, xi.z - xj.z);
+    // minimum-image separation from the fixed-point coordinates
+    const int4 xi = xq[i], xj = xq[j];
+    const float fx = md_qlen(md_qdiff(xi.x, xj.x), qh[0], ql[0]);
+    const float fy = md_qlen(md_qdiff(xi.y, xj.y), qh[1], ql[1]);
+    const float fz = md_qlen(md_qdiff(xi.z, xj.z), qh[2], ql[2]);
     dx = fx;
     dy = fy;
     dz = fz;
     rsq = (double)(fx * fx + fy * fy + fz * fz);
-    tt = (__float_as_int(xi.w) - 1) * T.ntypes + (__float_as_int(xj.w) - 1);
+    tt = (xi.w - 1) * T.ntypes + (xj.w - 1);
   } else {
     const double4 xi = x4[i], xj = x4[j];
     int jj, ex, ey, ez;
@@ -66,7 +68,7 @@ __device__ __forceinline__ void pair_geom(const AdjTables &T, int i, unsigned e,
 template <bool MIXED>
 __global__ void __launch_bounds__(kAdjThreads)
     k_adj_forward(int n, int stride, AdjTables T, BoxGeom box, const double4 *__restrict__ x4,
-                  const float4 *__restrict__ xr, const int *__restrict__ cell,
+                  const int4 *__restrict__ xq, const int *__restrict__ cell,
                   const int *__restrict__ nlist, const int *__restrict__ numneigh,
                   const int *__restrict__ orig, double *__restrict__ f) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -76,14 +78,13 @@ __global__ void __launch_bounds__(kAdjThreads)
   const Shift3 sx = shifts(cx, box.ncell[0], box.prd[0]);
   const Shift3 sy = shifts(cy, box.ncell[1], box.prd[1]);
   const Shift3 sz = shifts(cz, box.ncell[2], box.prd[2]);
-  const float csx = (float)box.cs[0], csy = (float)box.cs[1], csz = (float)box.cs[2];
   const int num = numneigh[i];
   double fx = 0.0, fy = 0.0, fz = 0.0;
   for (int k = 0; k < num; k++) {
     const unsigned e = (unsigned)nlist[md_slab(k, i, stride)];
     double dx, dy, dz, rsq;
     int tt;
-    pair_geom<MIXED>(T, i, e, x4, xr, sx, sy, sz, csx, csy, csz, dx, dy, dz, rsq, tt);
+    pair_geom<MIXED>(T, i, e, x4, xq, sx, sy, sz, box.qs, box.qs_lo, dx, dy, dz, rsq, tt);
     if (rsq < T.cutsq[tt]) {
       double phi;
       if (MIXED) {
@@ -118,7 +119,7 @@ __global__ void k_adj_gather(int n, const int *__restrict__ orig, const double *
 template <bool MIXED>
 __global__ void __launch_bounds__(kAdjThreads)
     k_adj_backward(int n, int stride, AdjTables T, BoxGeom box, const double4 *__restrict__ x4,
-                   const float4 *__restrict__ xr, const int *__restrict__ cell,
+                   const int4 *__restrict__ xq, const int *__restrict__ cell,
                    const int *__restrict__ nlist, const int *__restrict__ numneigh,
                    const int *__restrict__ orig, const double *__restrict__ gs,
                    double *__restrict__ gx, double *partial, unsigned int *counter,
@@ -136,8 +137,7 @@ __global__ void __launch_bounds__(kAdjThreads)
     const Shift3 sx = shifts(cx, box.ncell[0], box.prd[0]);
     const Shift3 sy = shifts(cy, box.ncell[1], box.prd[1]);
     const Shift3 sz = shifts(cz, box.ncell[2], box.prd[2]);
-    const float csx = (float)box.cs[0], csy = (float)box.cs[1], csz = (float)box.cs[2];
-    const double gix = gs[3 * i], giy = gs[3 * i + 1], giz = gs[3 * i + 2];
+      const double gix = gs[3 * i], giy = gs[3 * i + 1], giz = gs[3 * i + 2];
     const int num = numneigh[i];
     double hx = 0.0, hy = 0.0, hz = 0.0;
     for (int k = 0; k < num; k++) {
@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(kAdjThreads)
       const int j = md_entry_j(e);
       double dx, dy, dz, rsq;
       int tt;
-      pair_geom<MIXED>(T, i, e, x4, xr, sx, sy, sz, csx, csy, csz, dx, dy, dz, rsq, tt);
+      pair_geom<MIXED>(T, i, e, x4, xq, sx, sy, sz, box.qs, box.qs_lo, dx, dy, dz, rsq, tt);
       if (rsq < T.cutsq[tt]) {
         const double wx = gix - gs[3 * j], wy = giy - gs[3 * j + 1], wz = giz - gs[3 * j + 2];
         double phi, phis, r14, r8;
@@ -208,11 +208,11 @@ cudaError_t md_adj_forward(b200_ctx *c, const double *lj1, const double *lj2, co
   const int grid = md_blocks(c->n, kAdjThreads);
   if (c->prec == B200_PREC_MIXED)
     k_adj_forward<true><<<grid, kAdjThreads, 0, c->stream>>>(c->n, c->stride, T, c->box, c->x4,
-                                                             c->xr, c->cell, c->nlist,
+                                                             c->xq, c->cell, c->nlist,
                                                              c->numneigh, c->orig, f);
   else
     k_adj_forward<false><<<grid, kAdjThreads, 0, c->stream>>>(c->n, c->stride, T, c->box, c->x4,
-                                                              c->xr, c->cell, c->nlist,
+                                                              c->xq, c->cell, c->nlist,
                                                               c->numneigh, c->orig, f);
   c->launches++;
   return cudaGetLastError();
@@ -226,11 +226,11 @@ cudaError_t md_adj_backward(b200_ctx *c, const double *lj1, const double *lj2,
   k_adj_gather<<<md_blocks(c->n, 256), 256, 0, c->stream>>>(c->n, c->orig, g, gs);
   if (c->prec == B200_PREC_MIXED)
     k_adj_backward<true><<<grid, kAdjThreads, 0, c->stream>>>(
-        c->n, c->stride, T, c->box, c->x4, c->xr, c->cell, c->nlist, c->numneigh, c->orig, gs, gx,
+        c->n, c->stride, T, c->box, c->x4, c->xq, c->cell, c->nlist, c->numneigh, c->orig, gs, gx,
         c->partial, c->counter, gtab);
   else
     k_adj_backward<false><<<grid, kAdjThreads, 0, c->stream>>>(
-        c->n, c->stride, T, c->box, c->x4, c->xr, c->cell, c->nlist, c->numneigh, c->orig, gs, gx,
+        c->n, c->stride, T, c->box, c->x4, c->xq, c->cell, c->nlist, c->numneigh, c->orig, gs, gx,
         c->partial, c->counter, gtab);
   c->launches += 2;
   return cudaGetLastError();

@@ -222,6 +222,28 @@ int check_ready(b200_ctx *c) {
 // The cell grid of one periodic box for neighbor cutoff cutneighmax: cells
 // at least cutneighmax wide, one periodic image per side
 // (CommBrick::setup, src/comm_brick.cpp:128-170).
+// Fixed-point scale of the mixed form's coordinates (md_xq): 2^32 units per
+// box edge.  A listed pair must sit at its minimum image, so the mixed form
+// needs every edge longer than twice the list cutoff.
+int box_fixed_point(b200_ctx *c, BoxGeom &b) {
+  for (int d = 0; d < 3; d++) {
+    if (c->prec == B200_PREC_MIXED && !(b.prd[d] > 2.0 * c->cutneighmax))
+      return set_err(c, B200_ERR_BOX,
+                     "mixed precision needs box edges longer than twice the list cutoff: edge "
+                     "%g in dim %d, list cutoff %g",
+                     b.prd[d], d, c->cutneighmax);
+    b.qinv[d] = 4294967296.0 / b.prd[d];
+    const double u = b.prd[d] / 4294967296.0;  // exact: a power-of-two scale
+    b.qs[d] = (float)u;
+    b.qs_lo[d] = (float)(u - (double)b.qs[d]);
+  }
+  const double q2 = 1.0 / ((b.prd[0] / 4294967296.0) * (b.prd[0] / 4294967296.0));
+  b.q2inv = (float)q2;
+  b.q2inv_lo = (float)(q2 - (double)b.q2inv);
+  b.qiso = b.prd[0] == b.prd[1] && b.prd[1] == b.prd[2];
+  return B200_OK;
+}
+
 int box_cells(b200_ctx *c, BoxGeom &b, long long *ncells) {
   *ncells = 1;
   for (int d = 0; d < 3; d++) {
@@ -237,7 +259,7 @@ int box_cells(b200_ctx *c, BoxGeom &b, long long *ncells) {
     b.cinv[d] = nc / b.prd[d];
     *ncells *= nc;
   }
-  return B200_OK;
+  return box_fixed_point(c, b);
 }
 
 // Cell grids, cell and builder-tile offsets of every replica, and their
@@ -337,6 +359,7 @@ int init_cutoffs_and_cells(b200_ctx *c) {
     c->box.cinv[d] = nc / c->box.prd[d];
     ncells *= nc;
   }
+  if (int rc = box_fixed_point(c, c->box)) return rc;
   if (ncells > (long long)4096 * 4096 - 1)
     return set_err(c, B200_ERR_ARG, "too many cells (%lld)", ncells);
   if ((int)ncells != c->ncells) invalidate_graphs(c);  // scan launch shape changes
@@ -808,7 +831,7 @@ int snapshot(b200_ctx *c, bool save) {
     CK(dalloc(&c->snap_orig, s));
     CK(dalloc(&c->snap_image, s));
     CK(dalloc(&c->snap_cell, s));
-    CK(dalloc(&c->snap_xr, s));
+    CK(dalloc(&c->snap_xq, s));
     if (!c->snap_status) CK(cudaMalloc((void **)&c->snap_status, ST_COUNT * sizeof(int)));
     c->snap_alloc = c->stride;
   }
@@ -824,7 +847,7 @@ int snapshot(b200_ctx *c, bool save) {
   CK(cp(c->image, c->snap_image, n * sizeof(int)));
   CK(cp(c->cell, c->snap_cell, n * sizeof(int)));
   if (c->check) CK(cp(c->xhold, c->snap_xhold, n * sizeof(double4)));
-  if (c->prec == B200_PREC_MIXED) CK(cp(c->xr, c->snap_xr, n * sizeof(float4)));
+  if (c->prec == B200_PREC_MIXED) CK(cp(c->xq, c->snap_xq, n * sizeof(int4)));
   CK(cp(c->status, c->snap_status, ST_COUNT * sizeof(int)));
   if (!save) CK(md_where(c));
   return B200_OK;
@@ -906,7 +929,7 @@ int b200_destroy(b200_ctx *c) {
   dfree(c->x4); dfree(c->x4b); dfree(c->v); dfree(c->vb); dfree(c->f);
   dfree(c->orig); dfree(c->origb); dfree(c->image); dfree(c->imageb); dfree(c->cell);
   dfree(c->where); dfree(c->ghost);
-  dfree(c->xr); dfree(c->xhold); dfree(c->xfer); dfree(c->rho); dfree(c->fp); dfree(c->fpf); dfree(c->mass_dev);
+  dfree(c->xq); dfree(c->xhold); dfree(c->xfer); dfree(c->rho); dfree(c->fp); dfree(c->fpf); dfree(c->mass_dev);
   dfree(c->eam_eatom); dfree(c->d_rep_grp_first); dfree(c->d_rep_ranges);
   dfree(c->cell_count); dfree(c->cell_start); dfree(c->scan_tmp);
   dfree(c->slot); dfree(c->perm); dfree(c->cell_tmp);
@@ -916,7 +939,7 @@ int b200_destroy(b200_ctx *c) {
   dfree(c->d_rep_tile_base); 
   dfree(c->status); dfree(c->rows); dfree(c->tables_dev);
   dfree(c->snap_x4); dfree(c->snap_xhold); dfree(c->snap_v); dfree(c->snap_f);
-  dfree(c->snap_orig); dfree(c->snap_image); dfree(c->snap_cell); dfree(c->snap_xr);
+  dfree(c->snap_orig); dfree(c->snap_image); dfree(c->snap_cell); dfree(c->snap_xq);
   dfree(c->snap_status);
   dfree(c->eam.frho); dfree(c->eam.rhor); dfree(c->eam.z2r);
   dfree(c->eam.frho_f); dfree(c->eam.rhor_f); dfree(c->eam.z2r_f); dfree(c->eam.fz_f);
@@ -1128,7 +1151,7 @@ int b200_upload_atoms(b200_ctx *c, int n, const double *x, const double *v, cons
     CK(dalloc(&c->cell, stride));
     CK(dalloc(&c->where, stride));
     CK(dalloc(&c->ghost, stride));
-    CK(dalloc(&c->xr, stride));
+    CK(dalloc(&c->xq, stride));
     CK(dalloc(&c->xhold, stride));
     CK(dalloc(&c->rho, stride));
     CK(dalloc(&c->fp, stride));

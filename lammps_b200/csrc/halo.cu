@@ -14,25 +14,17 @@
 
 namespace {
 
-// new coordinates of sorted slot k, with the cell-relative FP32 copy (mixed
-// form) formed as the integrator forms it, from the cell of the last build
+// new coordinates of sorted slot k, with the fixed-point copy (mixed form)
+// formed as the integrator forms it
 __device__ __forceinline__ void set_position(int k, double x, double y, double z,
-                                             double4 *__restrict__ x4, float4 *__restrict__ xr,
-                                             const int *__restrict__ cell, const BoxGeom &box) {
+                                             double4 *__restrict__ x4, int4 *__restrict__ xq,
+                                             const BoxGeom &box) {
   double4 p = x4[k];
   p.x = x;
   p.y = y;
   p.z = z;
   x4[k] = p;
-  if (xr) {
-    int cx, cy, cz;
-    md_cell_unpack(cell[k], cx, cy, cz);
-    const double ox = box.lo[0] + (cx + 0.5) * box.cs[0];
-    const double oy = box.lo[1] + (cy + 0.5) * box.cs[1];
-    const double oz = box.lo[2] + (cz + 0.5) * box.cs[2];
-    xr[k] = make_float4((float)(p.x - ox), (float)(p.y - oy), (float)(p.z - oz),
-                        __int_as_float((int)p.w));
-  }
+  if (xq) xq[k] = md_xq(p, box);
 }
 
 __global__ void k_where(int n, const int *__restrict__ orig, int *__restrict__ where) {
@@ -62,8 +54,7 @@ __global__ void k_halo_pack(int m, int n, const int *__restrict__ idx,
 __global__ void k_halo_unpack(int m, int n, const int *__restrict__ idx,
                               const int *__restrict__ where, const int *__restrict__ ghost,
                               const double *__restrict__ buf, double4 *__restrict__ x4,
-                              float4 *__restrict__ xr, const int *__restrict__ cell, BoxGeom box,
-                              int *__restrict__ status) {
+                              int4 *__restrict__ xq, BoxGeom box, int *__restrict__ status) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m) return;
   const int j = idx[i];
@@ -76,18 +67,20 @@ __global__ void k_halo_unpack(int m, int n, const int *__restrict__ idx,
     return;
   }
   const int k = where[j];
-  set_position(k, buf[3 * (size_t)i], buf[3 * (size_t)i + 1], buf[3 * (size_t)i + 2], x4, xr,
-               cell, box);
+  set_position(k, buf[3 * (size_t)i], buf[3 * (size_t)i + 1], buf[3 * (size_t)i + 2], x4, xq,
+               box);
 }
 
-// every atom: x of sorted slot k = x[orig[k]] (caller order)
+// every atom: x of sorted slot k = x[orig[k]] (caller order); a batched
+// context forms each atom's fixed-point copy in its own replica's box
 __global__ void k_positions(int n, const int *__restrict__ orig, const double *__restrict__ x,
-                            double4 *__restrict__ x4, float4 *__restrict__ xr,
-                            const int *__restrict__ cell, BoxGeom box) {
+                            double4 *__restrict__ x4, int4 *__restrict__ xq, BoxGeom box,
+                            Reps reps, int batch) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   const size_t o = (size_t)orig[k];
-  set_position(k, x[3 * o], x[3 * o + 1], x[3 * o + 2], x4, xr, cell, box);
+  set_position(k, x[3 * o], x[3 * o + 1], x[3 * o + 2], x4, xq,
+               batch ? reps.box[reps.rep_of_atom[k]] : box);
 }
 
 }  // namespace
@@ -111,7 +104,7 @@ cudaError_t md_halo_unpack(b200_ctx *c, int m, const int *idx, const double *buf
   if (m < 1) return cudaSuccess;
   k_halo_unpack<<<md_blocks(m, 256), 256, 0, c->stream>>>(
       m, c->n, idx, c->where, c->ghosts_on ? c->ghost : nullptr, buf, c->x4,
-      c->prec == B200_PREC_MIXED ? c->xr : nullptr, c->cell, c->box, c->status);
+      c->prec == B200_PREC_MIXED ? c->xq : nullptr, c->box, c->status);
   c->launches++;
   return cudaGetLastError();
 }
@@ -119,7 +112,8 @@ cudaError_t md_halo_unpack(b200_ctx *c, int m, const int *idx, const double *buf
 cudaError_t md_set_positions(b200_ctx *c, const double *x) {
   if (c->n < 1) return cudaSuccess;
   k_positions<<<md_blocks(c->n, 256), 256, 0, c->stream>>>(
-      c->n, c->orig, x, c->x4, c->prec == B200_PREC_MIXED ? c->xr : nullptr, c->cell, c->box);
+      c->n, c->orig, x, c->x4, c->prec == B200_PREC_MIXED ? c->xq : nullptr, c->box, c->reps(),
+      c->nrep > 0);
   c->launches++;
   return cudaGetLastError();
 }

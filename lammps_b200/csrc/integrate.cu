@@ -3,8 +3,8 @@
 //
 // FixNVE::initial_integrate / final_integrate (src/fix_nve.cpp:65-142) with
 // dtfm = dtf / mass[type]; every product and sum is rounded separately as in
-// the reference.  The initial half-kick also refreshes the FP32
-// cell-relative copy used by the mixed-precision pair kernels and flags any
+// the reference.  The initial half-kick also refreshes the fixed-point
+// coordinates used by the mixed-precision pair kernels (md_xq) and flags any
 // atom that moved more than half the skin since the last build
 // (Neighbor::check_distance, src/neighbor.cpp:1322-1372).
 #include "md_state.h"
@@ -25,8 +25,7 @@ __global__ void __launch_bounds__(256) k_nve_initial(int n, int stride, double d
                                                       double4 *__restrict__ x4,
                                                       double *__restrict__ v,
                                                       const double *__restrict__ f,
-                                                      float4 *__restrict__ xr,
-                                                      const int *__restrict__ cell, BoxGeom box1,
+                                                      int4 *__restrict__ xq, BoxGeom box1,
                                                       Reps reps,
                                                       const double4 *__restrict__ xhold,
                                                       double triggersq, int *__restrict__ status,
@@ -49,16 +48,7 @@ __global__ void __launch_bounds__(256) k_nve_initial(int n, int stride, double d
     v[stride + i] = vy;
     v[2 * stride + i] = vz;
     x4[i] = p;
-    if (xr) {
-      const BoxGeom &box = BATCH ? reps.box[reps.rep_of_atom[i]] : box1;
-      int cx, cy, cz;
-      md_cell_unpack(cell[i], cx, cy, cz);
-      const double ox = box.lo[0] + (cx + 0.5) * box.cs[0];
-      const double oy = box.lo[1] + (cy + 0.5) * box.cs[1];
-      const double oz = box.lo[2] + (cz + 0.5) * box.cs[2];
-      xr[i] = make_float4((float)(p.x - ox), (float)(p.y - oy), (float)(p.z - oz),
-                          __int_as_float((int)p.w));
-    }
+    if (xq) xq[i] = md_xq(p, BATCH ? reps.box[reps.rep_of_atom[i]] : box1);
     if (xhold) {
       const double4 h = xhold[i];
       const double rsq = dsq3(__dsub_rn(p.x, h.x), __dsub_rn(p.y, h.y), __dsub_rn(p.z, h.z));
@@ -109,8 +99,7 @@ __global__ void __launch_bounds__(256) k_nve_fused(int n, int stride, double dtv
                                                     double4 *__restrict__ x4,
                                                     double *__restrict__ v,
                                                     const double *__restrict__ f,
-                                                    float4 *__restrict__ xr,
-                                                    const int *__restrict__ cell, BoxGeom box1,
+                                                    int4 *__restrict__ xq, BoxGeom box1,
                                                     Reps reps, const double4 *__restrict__ xhold,
                                                     double triggersq, int *__restrict__ status,
                                                     double *partial, unsigned int *counter,
@@ -124,7 +113,7 @@ __global__ void __launch_bounds__(256) k_nve_fused(int n, int stride, double dtv
   bool moved = false;
   if (i < n) {
     const BoxGeom &box = BATCH ? reps.box[reps.rep_of_atom[i]] : box1;
-    moved = md_nve_fused_atom<KE>(i, stride, dtv, dtf, mass, x4, v, f, xr, cell, box, xhold,
+    moved = md_nve_fused_atom<KE>(i, stride, dtv, dtf, mass, x4, v, f, xq, box, xhold,
                                   triggersq, acc[0]);
   }
   if (xhold && __any_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0) {
@@ -178,13 +167,13 @@ cudaError_t md_nve_initial(b200_ctx *c, double dtv, double dtf) {
   if (c->nrep)
     k_nve_initial<true><<<md_blocks(c->n, B), B, 0, c->stream>>>(
         c->n, c->stride, dtv, dtf, c->mass_dev, c->x4, c->v, c->f,
-        c->prec == B200_PREC_MIXED ? c->xr : nullptr, c->cell, c->box, c->reps(),
+        c->prec == B200_PREC_MIXED ? c->xq : nullptr, c->box, c->reps(),
         c->check ? c->xhold : nullptr, triggersq, c->status, c->ghosts_on ? c->ghost : nullptr,
         c->orig);
   else
     k_nve_initial<false><<<md_blocks(c->n, B), B, 0, c->stream>>>(
         c->n, c->stride, dtv, dtf, c->mass_dev, c->x4, c->v, c->f,
-        c->prec == B200_PREC_MIXED ? c->xr : nullptr, c->cell, c->box, c->reps(),
+        c->prec == B200_PREC_MIXED ? c->xq : nullptr, c->box, c->reps(),
         c->check ? c->xhold : nullptr, triggersq, c->status, c->ghosts_on ? c->ghost : nullptr,
         c->orig);
   c->launches++;
@@ -211,7 +200,7 @@ cudaError_t md_nve_fused(b200_ctx *c, double dtv, double dtf, bool ke) {
   const double triggersq = 0.25 * c->skin * c->skin;  // src/neighbor.cpp:239
 #define MD_FUSED_ARGS                                                                           \
   c->n, c->stride, dtv, dtf, c->mass_dev, c->x4, c->v, c->f,                                  \
-      c->prec == B200_PREC_MIXED ? c->xr : nullptr, c->cell, c->box, c->reps(),               \
+      c->prec == B200_PREC_MIXED ? c->xq : nullptr, c->box, c->reps(),                        \
       c->check ? c->xhold : nullptr, triggersq, c->status, c->partial, c->counter, c->ev,     \
       c->rows, c->rows_cap, c->every, c->delay, c->check, c->dec_count, c->mail_dev
   const int grid = md_blocks(c->n, B);

@@ -4,7 +4,8 @@
 //   x4[i]      double4 (x, y, z, type)       -- FP64 positions, gathered per pair
 //   v[3][n]    double SoA                     -- velocities
 //   f[3][n]    double SoA                     -- forces (owner-summed; no ghosts)
-//   xr[i]      float4 (cell-relative x,y,z, type bits) -- mixed precision only
+//   xq[i]      int4 (x, y, z as 32-bit fixed-point fractions of the box edge,
+//              type) -- mixed precision only (md_xq)
 //   cell[i]    packed cell coordinates cx | cy<<10 | cz<<20 of the last build
 //   nlist      neighbor list in int4 slabs (md_slab): bits 6..31 = neighbor
 //              atom index, bits 0..5 = offset of the neighbor's cell from the
@@ -49,6 +50,13 @@ struct BoxGeom {
   double lo[3], hi[3], prd[3];
   double cinv[3];    // cells per unit length: ncell/prd
   double cs[3];      // cell edge prd/ncell
+  double qinv[3];    // fixed-point units per unit length: 2^32/prd (md_xq)
+  // length of one fixed-point unit, prd/2^32, as an FP32 pair hi + lo (a
+  // single FP32 value would scale every separation by the same rounding
+  // error); and 1/unit^2 the same way, for one unit in every dimension
+  float qs[3], qs_lo[3];
+  float q2inv, q2inv_lo;
+  int qiso;          // the three edges are equal (one fixed-point unit)
   int ncell[3];
 };
 
@@ -116,21 +124,33 @@ __device__ __forceinline__ double pick(const Shift3 &s, int d) {
   return d < 0 ? s.m : (d > 0 ? s.p : 0.0);
 }
 
-// Cell offset of an entry along x, y, z as a float, without an
-// integer-to-float conversion: the code bits are ORed into the low mantissa
-// of 2^23 (exact) and 2^23 plus the bias is subtracted (exact).  With
-// d = bits - 1 (-1, 0, +1; +2 for the pad entry) they return d, 4 d and
-// 16 d, to be multiplied by cs, cs/4 and cs/16: the products are exact, so
-// fmaf(-offset, scaled cs, x) rounds once, like x - d * cs.
-__device__ __forceinline__ float md_code_dx(unsigned e) {
-  return __int_as_float((int)(0x4B000000u | (e & 3u))) - 8388609.0f;
+// Coordinates of the mixed form.  Each coordinate is a 32-bit fixed-point
+// fraction of its periodic box edge: 2^32 units per edge, taken modulo 2^32.
+// The difference of two such coordinates in 32-bit two's-complement
+// arithmetic is the separation along that edge reduced to the minimum image
+// (exact, with no periodic shift to decode), and one conversion turns it into
+// an FP32 number of units.  A listed pair is at its minimum image whenever
+// the box edge exceeds twice the list cutoff, which the mixed form requires.
+// The quantisation step is prd / 2^32 (3.9e-8 sigma on the 168-sigma edge of
+// a 4M-atom LJ box), below the FP32 rounding of a separation of one sigma.
+__device__ __forceinline__ int md_fix(double x, double lo, double qinv) {
+  return (int)(unsigned int)(unsigned long long)__double2ll_rn(__dmul_rn(x - lo, qinv));
 }
-__device__ __forceinline__ float md_code_dy4(unsigned e) {
-  return __int_as_float((int)(0x4B000000u | (e & 12u))) - 8388612.0f;
+__device__ __forceinline__ int4 md_xq(const double4 &p, const BoxGeom &b) {
+  return make_int4(md_fix(p.x, b.lo[0], b.qinv[0]), md_fix(p.y, b.lo[1], b.qinv[1]),
+                   md_fix(p.z, b.lo[2], b.qinv[2]), (int)p.w);
 }
-__device__ __forceinline__ float md_code_dz16(unsigned e) {
-  return __int_as_float((int)(0x4B000000u | (e & 48u))) - 8388624.0f;
+// separation a - b along one edge in fixed-point units, as an FP32 number
+__device__ __forceinline__ float md_qdiff(int a, int b) {
+  return (float)(int)((unsigned int)a - (unsigned int)b);
 }
+// u units in length units: u * (hi + lo) rounded once (the small product
+// u * lo first, then one fused multiply-add; rounding u * hi first and adding
+// the correction after would leave a bias of a fraction of an ulp)
+__device__ __forceinline__ float md_qlen(float u, float hi, float lo) {
+  return fmaf(u, hi, u * lo);
+}
+
 __host__ __device__ inline void md_entry(unsigned int e, int &j, int &dx, int &dy, int &dz) {
   j = (int)(e >> 6);
   dx = (int)(e & 3u) - 1;
@@ -318,16 +338,15 @@ __device__ __forceinline__ void md_record_row_dev(int *status, const double *ev,
 // FixNVE::final_integrate of this step for sorted atom i, the kinetic-energy
 // term of the thermo output (KE, into ke), then FixNVE::initial_integrate of
 // the next step (src/fix_nve.cpp:65-142): every product and sum rounded
-// separately as in the reference.  Refreshes the FP32 cell-relative copy
-// (xr, mixed form) and returns whether the atom moved more than half the skin
-// since the last build (xhold, check yes).
+// separately as in the reference.  Refreshes the fixed-point copy (xq, mixed
+// form) and returns whether the atom moved more than half the skin since the
+// last build (xhold, check yes).
 template <bool KE>
 __device__ __forceinline__ bool md_nve_fused_atom(int i, int stride, double dtv, double dtf,
                                                   const double *__restrict__ mass,
                                                   double4 *__restrict__ x4, double *__restrict__ v,
                                                   const double *__restrict__ f,
-                                                  float4 *__restrict__ xr,
-                                                  const int *__restrict__ cell, const BoxGeom &box,
+                                                  int4 *__restrict__ xq, const BoxGeom &box,
                                                   const double4 *__restrict__ xhold,
                                                   double triggersq, double &ke) {
   double4 p = x4[i];
@@ -349,15 +368,7 @@ __device__ __forceinline__ bool md_nve_fused_atom(int i, int stride, double dtv,
   v[stride + i] = vy;
   v[2 * stride + i] = vz;
   x4[i] = p;
-  if (xr) {
-    int cx, cy, cz;
-    md_cell_unpack(cell[i], cx, cy, cz);
-    const double ox = box.lo[0] + (cx + 0.5) * box.cs[0];
-    const double oy = box.lo[1] + (cy + 0.5) * box.cs[1];
-    const double oz = box.lo[2] + (cz + 0.5) * box.cs[2];
-    xr[i] = make_float4((float)(p.x - ox), (float)(p.y - oy), (float)(p.z - oz),
-                        __int_as_float((int)p.w));
-  }
+  if (xq) xq[i] = md_xq(p, box);
   if (xhold) {
     const double4 h = xhold[i];
     const double rsq = dsq3(__dsub_rn(p.x, h.x), __dsub_rn(p.y, h.y), __dsub_rn(p.z, h.z));

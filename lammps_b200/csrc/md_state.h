@@ -100,7 +100,7 @@ struct b200_ctx {
   // another rank owns; such atoms are neither integrated nor distance-checked
   int *ghost = nullptr;
   bool ghosts_on = false;
-  float4 *xr = nullptr;       // mixed: cell-relative coordinates
+  int4 *xq = nullptr;         // mixed: fixed-point coordinates (md_xq)
   double4 *xhold = nullptr;   // positions at the last build (check yes)
   // device staging of host transfers (upload, download, per-atom energy and
   // virial), kept between calls so a call maps no new memory
@@ -145,7 +145,7 @@ struct b200_ctx {
   double4 *snap_x4 = nullptr, *snap_xhold = nullptr;
   double *snap_v = nullptr, *snap_f = nullptr;
   int *snap_orig = nullptr, *snap_image = nullptr, *snap_cell = nullptr;
-  float4 *snap_xr = nullptr;
+  int4 *snap_xq = nullptr;
   int *snap_status = nullptr;
   int snap_alloc = 0;
   int overflow_replays = 0;
@@ -216,6 +216,15 @@ struct b200_ctx {
   long long phase_steps = 0;
 };
 
+// The mixed form's fixed-point unit is the same in every dimension of the box
+// (of every replica box, for a batch): the pair kernels then work in units.
+inline bool md_q_iso(const b200_ctx *c) {
+  if (!c->nrep) return c->box.qiso != 0;
+  for (int r = 0; r < c->nrep; r++)
+    if (!c->rep_box[r].qiso) return false;
+  return true;
+}
+
 // ---- launchers (neigh.cu) -------------------------------------------------
 // full rebuild: wrap, cell counting sort, permute, neighbor list
 cudaError_t md_rebuild(b200_ctx *c, const int *d_flag);
@@ -229,7 +238,7 @@ cudaError_t md_half_list(b200_ctx *c, int *d_num, int *d_jowner, int *d_jimage, 
 cudaError_t md_where(b200_ctx *c);
 // buf[3i..3i+2] = x of caller atom idx[i]; idx, buf on the device
 cudaError_t md_halo_pack(b200_ctx *c, int m, const int *idx, double *buf);
-// x of caller atom idx[i] = buf[3i..3i+2] (and its cell-relative FP32 copy)
+// x of caller atom idx[i] = buf[3i..3i+2] (and its fixed-point copy)
 cudaError_t md_halo_unpack(b200_ctx *c, int m, const int *idx, const double *buf);
 // x of every atom from x[3n] in caller order (device), keeping cells and list
 cudaError_t md_set_positions(b200_ctx *c, const double *x);

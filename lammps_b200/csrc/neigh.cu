@@ -9,7 +9,7 @@
 //   2 k_scan_*      exclusive scan of the counts -> cell_start
 //   3 k_scatter     counting-sort scatter of atom indices; zeroes the counts
 //   4 k_sort_cells  order each cell by caller index (deterministic order)
-//   5 k_gather      permute x, v, ids; cell-relative FP32 copy; xhold
+//   5 k_gather      permute x, v, ids; fixed-point copy (mixed); xhold
 //   6 k_copyback    permuted arrays back into the primary buffers, the
 //                   caller-index -> slot map; ago = 0
 //   7 k_neigh_tiles full list over the 27 neighbor cells (cell >= rc+skin),
@@ -195,7 +195,7 @@ __global__ void k_gather(int n, int stride, BoxGeom box1, Reps reps, const int *
                          const int *__restrict__ orig, int *__restrict__ origb,
                          const int *__restrict__ image, int *__restrict__ imageb,
                          const int *__restrict__ cell_tmp, int *__restrict__ cell,
-                         float4 *__restrict__ xr, double4 *__restrict__ xhold, const int *flag) {
+                         int4 *__restrict__ xq, double4 *__restrict__ xhold, const int *flag) {
   if (!rebuild_on(flag)) return;
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
@@ -216,13 +216,7 @@ __global__ void k_gather(int n, int stride, BoxGeom box1, Reps reps, const int *
   int cz = c / (box.ncell[0] * box.ncell[1]);
   cell[k] = md_cell_pack(cx, cy, cz);
   if (xhold) xhold[k] = p;
-  if (xr) {
-    double ox = box.lo[0] + (cx + 0.5) * box.cs[0];
-    double oy = box.lo[1] + (cy + 0.5) * box.cs[1];
-    double oz = box.lo[2] + (cz + 0.5) * box.cs[2];
-    xr[k] = make_float4((float)(p.x - ox), (float)(p.y - oy), (float)(p.z - oz),
-                        __int_as_float((int)p.w));
-  }
+  if (xq) xq[k] = md_xq(p, box);
 }
 
 __global__ void k_copyback(int n, int stride, const double4 *__restrict__ x4b,
@@ -499,8 +493,12 @@ __global__ void __launch_bounds__(kNeighThreads, 8) k_neigh_tiles(
         // the stored count never exceeds the capacity, so readers stay in
         // bounds; an overflow is reported through the status word
         numneigh[i] = count < capacity ? count : capacity;
-        atomicMax(&status[ST_MAXNEIGH], count);
-        if (count > capacity) atomicExch(&status[ST_OVERFLOW], 1);
+      }
+      // one status update per warp
+      const int cmax = __reduce_max_sync(0xffffffffu, act ? count : 0);
+      if (lane == 0) {
+        atomicMax(&status[ST_MAXNEIGH], cmax);
+        if (cmax > capacity) atomicExch(&status[ST_OVERFLOW], 1);
       }
     }
     return;
@@ -724,12 +722,12 @@ cudaError_t md_rebuild(b200_ctx *c, const int *d_flag) {
   if (c->nrep)
     k_gather<true><<<md_blocks(n, B), B, 0, c->stream>>>(
         n, c->stride, c->box, R, c->perm, c->x4, c->x4b, c->v, c->vb, c->orig, c->origb, c->image,
-        c->imageb, c->cell_tmp, c->cell, c->prec == 1 ? c->xr : nullptr,
+        c->imageb, c->cell_tmp, c->cell, c->prec == 1 ? c->xq : nullptr,
         c->check ? c->xhold : nullptr, d_flag);
   else
     k_gather<false><<<md_blocks(n, B), B, 0, c->stream>>>(
         n, c->stride, c->box, R, c->perm, c->x4, c->x4b, c->v, c->vb, c->orig, c->origb, c->image,
-        c->imageb, c->cell_tmp, c->cell, c->prec == 1 ? c->xr : nullptr,
+        c->imageb, c->cell_tmp, c->cell, c->prec == 1 ? c->xq : nullptr,
         c->check ? c->xhold : nullptr, d_flag);
   k_copyback<<<md_blocks(n, B), B, 0, c->stream>>>(n, c->stride, c->x4b, c->x4, c->vb, c->v,
                                                    c->origb, c->orig, c->imageb, c->image,

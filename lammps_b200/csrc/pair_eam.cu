@@ -16,8 +16,9 @@
 // clamps are the reference's: m = min(m, nr-1), p = min(p, 1) for r and
 // m = max(1, min(m, nrho-1)) for rho.
 // Mixed form: FP32 tables reordered per knot as [c3 c4 c5 c6 | c0 c1 c2 -]
-// so one float4 load gives a value and one a derivative; distances from the
-// FP32 cell-relative coordinates; fp_j gathered as FP32; sums in FP64.  The
+// so one float4 load gives a value and one a derivative; separations from the
+// fixed-point coordinates (md_xq: one 32-bit subtraction and one conversion
+// per component, at the minimum image); fp_j gathered as FP32; sums in FP64.  The
 // embedding step F(rho) stays FP64 in both forms.  Each thread reads four
 // list entries with one 16-byte load and issues their gathers together; the
 // mixed kernels load the next slab's entries before using the current one.
@@ -90,7 +91,7 @@ __device__ __forceinline__ void embed(const EamArgs &a, int itype_frho, double r
 
 template <int TPA, bool EV, bool ATOM, bool MIXED, bool SINGLE>
 __global__ void __launch_bounds__(128) k_eam_rho(EamArgs a, const double4 *__restrict__ x4,
-                                                 const float4 *__restrict__ xr) {
+                                                 const int4 *__restrict__ xq) {
   __shared__ int s_t2rhor[TABSZ];
   __shared__ int s_t2frho[MD_MAXTYPES + 1];
   __shared__ double red[7 * 4];
@@ -154,10 +155,10 @@ __global__ void __launch_bounds__(128) k_eam_rho(EamArgs a, const double4 *__res
         }
       }
     } else {
-      const float4 xi = xr[i];
-      ti = __float_as_int(xi.w);
-      const float csx = (float)a.box.cs[0], csy4 = 0.25f * (float)a.box.cs[1],
-                  csz16 = 0.0625f * (float)a.box.cs[2];
+      const int4 xi = xq[i];
+      ti = xi.w;
+      const float qx = a.box.qs[0], qy = a.box.qs[1], qz = a.box.qs[2];
+      const float qxl = a.box.qs_lo[0], qyl = a.box.qs_lo[1], qzl = a.box.qs_lo[2];
       const float cutf = (float)a.cutforcesq, rdrf = (float)a.rdr;
       // one element: the density spline row of every pair
       const float *rrow =
@@ -169,26 +170,28 @@ __global__ void __launch_bounds__(128) k_eam_rho(EamArgs a, const double4 *__res
       for (int c4 = lane; c4 < nslab; c4 += TPA) {
         const int4 e4 = en;
         if (c4 + TPA < nslab) en = __ldcs(&nl4[(size_t)(c4 + TPA) * a.stride + i]);
-        // whole slabs: pad entries in the last slab fail the cutoff test
+        // whole slabs: pad entries in the last slab name the atom itself
+        // (zero separation), which the r^2 > 0 test rejects
         const unsigned int ee[4] = {(unsigned int)e4.x, (unsigned int)e4.y, (unsigned int)e4.z,
                                     (unsigned int)e4.w};
-        float4 xq[4];
+        int4 xs[4];
 #pragma unroll
-        for (int u = 0; u < 4; u++) xq[u] = xr[md_entry_j(ee[u])];
+        for (int u = 0; u < 4; u++) xs[u] = xq[md_entry_j(ee[u])];
         float crho = 0.f;  // FP32 slab sum, added to the FP64 density
 #pragma unroll
         for (int u = 0; u < 4; u++) {
-          const float4 xj = xq[u];
-          const float delx = fmaf(-md_code_dx(ee[u]), csx, xi.x - xj.x);
-          const float dely = fmaf(-md_code_dy4(ee[u]), csy4, xi.y - xj.y);
-          const float delz = fmaf(-md_code_dz16(ee[u]), csz16, xi.z - xj.z);
+          const int4 xj = xs[u];
+          // minimum-image separation from the fixed-point coordinates
+          const float delx = md_qlen(md_qdiff(xi.x, xj.x), qx, qxl);
+          const float dely = md_qlen(md_qdiff(xi.y, xj.y), qy, qyl);
+          const float delz = md_qlen(md_qdiff(xi.z, xj.z), qz, qzl);
           const float rsq = delx * delx + dely * dely + delz * delz;
-          if (rsq < cutf) {
+          if (rsq < cutf && rsq > 0.f) {
             int m;
             float p;
             knot_f(rsq * rsqrtf(rsq) * rdrf + 1.0f, a.nr - 1, m, p);
             const float *row = SINGLE ? rrow
-                                      : a.rhor_f + (size_t)s_t2rhor[__float_as_int(xj.w) * a.ntp1 + ti] *
+                                      : a.rhor_f + (size_t)s_t2rhor[xj.w * a.ntp1 + ti] *
                                                        (a.nr + 1) * 8;
             const float4 c = __ldg(reinterpret_cast<const float4 *>(row + (size_t)m * 8));
             crho += ((c.x * p + c.y) * p + c.z) * p + c.w;
@@ -216,7 +219,7 @@ __global__ void __launch_bounds__(128) k_eam_rho(EamArgs a, const double4 *__res
 
 template <int TPA, bool EV, bool ATOM, bool MIXED, bool SINGLE>
 __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__restrict__ x4,
-                                                   const float4 *__restrict__ xr) {
+                                                   const int4 *__restrict__ xq) {
   __shared__ int s_t2rhor[TABSZ];
   __shared__ int s_t2z2r[TABSZ];
   __shared__ double red[7 * 4];
@@ -321,11 +324,11 @@ __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__r
        }
       }
     } else {
-      const float4 xi = xr[i];
-      const int ti = __float_as_int(xi.w);
+      const int4 xi = xq[i];
+      const int ti = xi.w;
       const float fpi = a.fpf[i];
-      const float csx = (float)a.box.cs[0], csy4 = 0.25f * (float)a.box.cs[1],
-                  csz16 = 0.0625f * (float)a.box.cs[2];
+      const float qx = a.box.qs[0], qy = a.box.qs[1], qz = a.box.qs[2];
+      const float qxl = a.box.qs_lo[0], qyl = a.box.qs_lo[1], qzl = a.box.qs_lo[2];
       const float cutf = (float)a.cutforcesq, rdrf = (float)a.rdr;
       // one element: the density-derivative and pair spline rows of every pair
       const float *drow1 = SINGLE ? a.fz_f + 4 : nullptr;
@@ -337,28 +340,30 @@ __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__r
       for (int c4 = lane; c4 < nslab; c4 += TPA) {
        const int4 e4 = en;
        if (c4 + TPA < nslab) en = __ldcs(&nl4[(size_t)(c4 + TPA) * a.stride + i]);
-       // whole slabs: pad entries in the last slab fail the cutoff test
+       // whole slabs: pad entries in the last slab name the atom itself
+       // (zero separation), which the r^2 > 0 test rejects
        const unsigned int ee[4] = {(unsigned int)e4.x, (unsigned int)e4.y, (unsigned int)e4.z,
                                    (unsigned int)e4.w};
-       float4 xq[4];
+       int4 xs[4];
        float fpq[4];
 #pragma unroll
        for (int u = 0; u < 4; u++) {
          const int jj = md_entry_j(ee[u]);
-         xq[u] = xr[jj];
+         xs[u] = xq[jj];
          fpq[u] = a.fpf[jj];
        }
        // FP32 sum of the slab's pair forces, added to the FP64 accumulator
        float cfx = 0.f, cfy = 0.f, cfz = 0.f;
 #pragma unroll
        for (int u = 0; u < 4; u++) {
-        const float4 xj = xq[u];
-        const float delx = fmaf(-md_code_dx(ee[u]), csx, xi.x - xj.x);
-        const float dely = fmaf(-md_code_dy4(ee[u]), csy4, xi.y - xj.y);
-        const float delz = fmaf(-md_code_dz16(ee[u]), csz16, xi.z - xj.z);
+        const int4 xj = xs[u];
+        // minimum-image separation from the fixed-point coordinates
+        const float delx = md_qlen(md_qdiff(xi.x, xj.x), qx, qxl);
+        const float dely = md_qlen(md_qdiff(xi.y, xj.y), qy, qyl);
+        const float delz = md_qlen(md_qdiff(xi.z, xj.z), qz, qzl);
         const float rsq = delx * delx + dely * dely + delz * delz;
-        if (rsq < cutf) {
-          const int tj = __float_as_int(xj.w);
+        if (rsq < cutf && rsq > 0.f) {
+          const int tj = xj.w;
           const float recip = rsqrtf(rsq);
           const float r = rsq * recip;
           int m;
@@ -457,17 +462,17 @@ void launch_t(b200_ctx *c, const EamArgs &a, cudaEvent_t mid, int stage) {
   const int grid = md_blocks((long long)a.n * TPA, B);
   if (stage != EAM_FORCE) {
     if (c->prec == B200_PREC_MIXED)
-      k_eam_rho<TPA, EV, ATOM, true, SINGLE><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
+      k_eam_rho<TPA, EV, ATOM, true, SINGLE><<<grid, B, 0, c->stream>>>(a, c->x4, c->xq);
     else
-      k_eam_rho<TPA, EV, ATOM, false, SINGLE><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
+      k_eam_rho<TPA, EV, ATOM, false, SINGLE><<<grid, B, 0, c->stream>>>(a, c->x4, c->xq);
     c->launches++;
   }
   record_mid(c, mid);
   if (stage != EAM_DENSITY) {
     if (c->prec == B200_PREC_MIXED)
-      k_eam_force<TPA, EV, ATOM, true, SINGLE><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
+      k_eam_force<TPA, EV, ATOM, true, SINGLE><<<grid, B, 0, c->stream>>>(a, c->x4, c->xq);
     else
-      k_eam_force<TPA, EV, ATOM, false, SINGLE><<<grid, B, 0, c->stream>>>(a, c->x4, c->xr);
+      k_eam_force<TPA, EV, ATOM, false, SINGLE><<<grid, B, 0, c->stream>>>(a, c->x4, c->xq);
     c->launches++;
   }
 }

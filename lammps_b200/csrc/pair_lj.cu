@@ -9,9 +9,11 @@
 // FP64 form: arithmetic identical to the reference per pair; the periodic
 // image is x_j + s*L and rsq is rounded after every operation, so the
 // rsq < cutsq decision is the reference's.
-// Mixed form: positions are read as FP32 offsets from the centre of the
-// atom's cell (float4, 16 B per gather); the pair force is FP32 and each
-// atom's force, energy and virial are summed in FP64.
+// Mixed form: positions are read as 32-bit fixed-point fractions of the box
+// edge (md_xq, int4, 16 B per gather); a separation is one integer
+// subtraction and one conversion per component, already at the minimum
+// image; the pair force is FP32 and each atom's force, energy and virial are
+// summed in FP64.
 //
 // Memory-level parallelism: each thread reads four list entries with one
 // 16-byte load (slab layout, md_slab).  The FP64 kernel issues a slab's four
@@ -176,28 +178,46 @@ __device__ __forceinline__ void lj_atom_fp64(const PairArgs &a, const double4 *_
 }
 
 // One atom's pair forces in the mixed form (FP32 pair math, FP64 sums), as
-// lj_atom_fp64.  `tabf` is the per-type table in shared memory.
-template <int TPA, bool EV, bool SINGLE, bool BATCH>
-__device__ __forceinline__ void lj_atom_mixed(const PairArgs &a, const float4 *__restrict__ xr,
+// lj_atom_fp64.  `tabf` is the per-type table in shared memory.  Separations
+// come from the fixed-point coordinates (md_xq): per component one 32-bit
+// subtraction and one conversion give the minimum-image separation in units
+// of prd/2^32, so no periodic offset is decoded.
+//   ISO (equal box edges: one unit in every dimension): the pair arithmetic
+//   runs on separations in units; 1/r^2 is brought to length units by the
+//   FP32 pair hi + lo of 1/unit^2 (md_qlen), and an FP32 force sum (units x
+//   force/length) is scaled by the exact FP64 unit length as it joins the
+//   FP64 accumulator.
+//   Otherwise each component is scaled to length units first (md_qlen).
+// The scale constants are never a single rounded FP32 value, which would
+// bias every pair term the same way.
+// A pad entry names the atom itself (zero separation), which the r^2 > 0
+// test rejects.
+template <int TPA, bool EV, bool SINGLE, bool BATCH, bool ISO>
+__device__ __forceinline__ void lj_atom_mixed(const PairArgs &a, const int4 *__restrict__ xq,
                                               const float *tabf, int nt2, int i, int lane,
                                               bool active, double &fx, double &fy, double &fz,
                                               double (&acc)[7]) {
   if (active) {
+    const BoxGeom &box = BATCH ? a.reps.box[a.reps.rep_of_atom[i]] : a.box;
+    const float qx = box.qs[0], qy = box.qs[1], qz = box.qs[2];
+    const float qxl = box.qs_lo[0], qyl = box.qs_lo[1], qzl = box.qs_lo[2];
+    // ISO: 1/r^2 in units times (q2h + q2l) is 1/r^2 in length units, and a
+    // force sum in units times qd (exact) is the force
+    const float q2h = box.q2inv, q2l = box.q2inv_lo;
+    const double qd = box.prd[0] * (1.0 / 4294967296.0);
     float cutsq1 = 0, lj1 = 0, lj2 = 0, lj3 = 0, lj4 = 0, off = 0;
     if (SINGLE) {
       const int k11 = a.ntp1 + 1;
-      cutsq1 = (float)__ldg(&a.tables[TAB_CUTSQ * TABSZ + k11]);
+      const double cs = __ldg(&a.tables[TAB_CUTSQ * TABSZ + k11]);
+      cutsq1 = ISO ? (float)(cs / (qd * qd)) : (float)cs;
       lj1 = (float)__ldg(&a.tables[TAB_LJ1 * TABSZ + k11]);
       lj2 = (float)__ldg(&a.tables[TAB_LJ2 * TABSZ + k11]);
       lj3 = (float)__ldg(&a.tables[TAB_LJ3 * TABSZ + k11]);
       lj4 = (float)__ldg(&a.tables[TAB_LJ4 * TABSZ + k11]);
       off = (float)__ldg(&a.tables[TAB_OFFSET * TABSZ + k11]);
     }
-    const float4 xi = xr[i];
-    const int ti = __float_as_int(xi.w);
-    const BoxGeom &box = BATCH ? a.reps.box[a.reps.rep_of_atom[i]] : a.box;
-    const float csx = (float)box.cs[0], csy4 = 0.25f * (float)box.cs[1],
-                csz16 = 0.0625f * (float)box.cs[2];
+    const int4 xi = xq[i];
+    const int ti = xi.w;
     const int nslab = (a.numneigh[i] + 3) >> 2;
     const int4 *nl4 = reinterpret_cast<const int4 *>(a.nlist);
     // Four slabs (16 entries) per iteration: the sixteen gathers are in
@@ -205,7 +225,7 @@ __device__ __forceinline__ void lj_atom_mixed(const PairArgs &a, const float4 *_
     // (streaming, evict-first) before these are used, so the list's DRAM
     // latency overlaps the gathers and the arithmetic of the slabs before
     // them.  Slabs past the atom's count, and the tail of its last slab, hold
-    // pad entries, which the cutoff test rejects, so no per-entry count check
+    // pad entries, which the r^2 > 0 test rejects, so no per-entry count check
     // is needed.
     const int pe = md_pad_entry(i);
     const int4 pad4 = make_int4(pe, pe, pe, pe);
@@ -222,30 +242,35 @@ __device__ __forceinline__ void lj_atom_mixed(const PairArgs &a, const float4 *_
                                      (unsigned)a1.x, (unsigned)a1.y, (unsigned)a1.z, (unsigned)a1.w,
                                      (unsigned)a2.x, (unsigned)a2.y, (unsigned)a2.z, (unsigned)a2.w,
                                      (unsigned)a3.x, (unsigned)a3.y, (unsigned)a3.z, (unsigned)a3.w};
-      float4 xall[16];
+      int4 xall[16];
 #pragma unroll
-      for (int u = 0; u < 16; u++) xall[u] = __ldg(&xr[md_entry_j(eall[u])]);
+      for (int u = 0; u < 16; u++) xall[u] = __ldg(&xq[md_entry_j(eall[u])]);
       // the pair forces of each group of eight entries are summed in FP32,
       // the group sum is added to the atom's FP64 accumulator
 #pragma unroll
       for (int h = 0; h < 2; h++) {
-        const unsigned int *ee = eall + 8 * h;
-        const float4 *xj = xall + 8 * h;
+        const int4 *xj = xall + 8 * h;
         float cfx = 0.f, cfy = 0.f, cfz = 0.f;
 #pragma unroll
         for (int u = 0; u < 8; u++) {
-          // x_i - (x_j + image shift) = (xr_i - xr_j) - d * cell edge, with d
-          // the offset of the neighbour's cell from the atom's cell
-          const float delx = fmaf(-md_code_dx(ee[u]), csx, xi.x - xj[u].x);
-          const float dely = fmaf(-md_code_dy4(ee[u]), csy4, xi.y - xj[u].y);
-          const float delz = fmaf(-md_code_dz16(ee[u]), csz16, xi.z - xj[u].z);
+          // x_i - x_j at the minimum image, in units (ISO) or lengths
+          float delx = md_qdiff(xi.x, xj[u].x);
+          float dely = md_qdiff(xi.y, xj[u].y);
+          float delz = md_qdiff(xi.z, xj[u].z);
+          if (!ISO) {
+            delx = md_qlen(delx, qx, qxl);
+            dely = md_qlen(dely, qy, qyl);
+            delz = md_qlen(delz, qz, qzl);
+          }
           const float rsq = delx * delx + dely * dely + delz * delz;
-          const int tt = ti * a.ntp1 + __float_as_int(xj[u].w);
-          const float cs = SINGLE ? cutsq1 : tabf[0 * nt2 + tt];
+          const int tt = ti * a.ntp1 + xj[u].w;
+          // (the cutoff in units only selects pairs: its rounding biases no term)
+          const float cs = SINGLE ? cutsq1 : (ISO ? tabf[0 * nt2 + tt] * q2h : tabf[0 * nt2 + tt]);
           const float c1 = SINGLE ? lj1 : tabf[1 * nt2 + tt];
           const float c2 = SINGLE ? lj2 : tabf[2 * nt2 + tt];
-          const bool in = rsq < cs;
-          const float r2inv = rcp_approx_f32(rsq);
+          const bool in = rsq < cs && rsq > 0.f;
+          const float r2inv =
+              ISO ? md_qlen(rcp_approx_f32(rsq), q2h, q2l) : rcp_approx_f32(rsq);
           const float r6inv = r2inv * r2inv * r2inv;
           const float fpair = in ? r6inv * (c1 * r6inv - c2) * r2inv : 0.f;
           cfx = fmaf(delx, fpair, cfx);
@@ -257,18 +282,28 @@ __device__ __forceinline__ void lj_atom_mixed(const PairArgs &a, const float4 *_
             const float co = SINGLE ? off : tabf[5 * nt2 + tt];
             const float evdwl = in ? r6inv * (c3 * r6inv - c4) - co : 0.f;
             acc[0] += 0.5 * (double)evdwl;
+            // the virial wants separations in length units
+            const float lx = ISO ? md_qlen(delx, qx, qxl) : delx,
+                        ly = ISO ? md_qlen(dely, qx, qxl) : dely,
+                        lz = ISO ? md_qlen(delz, qx, qxl) : delz;
             const float hf = 0.5f * fpair;
-            acc[1] += (double)(delx * delx * hf);
-            acc[2] += (double)(dely * dely * hf);
-            acc[3] += (double)(delz * delz * hf);
-            acc[4] += (double)(delx * dely * hf);
-            acc[5] += (double)(delx * delz * hf);
-            acc[6] += (double)(dely * delz * hf);
+            acc[1] += (double)(lx * lx * hf);
+            acc[2] += (double)(ly * ly * hf);
+            acc[3] += (double)(lz * lz * hf);
+            acc[4] += (double)(lx * ly * hf);
+            acc[5] += (double)(lx * lz * hf);
+            acc[6] += (double)(ly * lz * hf);
           }
         }
-        fx += (double)cfx;
-        fy += (double)cfy;
-        fz += (double)cfz;
+        if (ISO) {
+          fx = fma((double)cfx, qd, fx);
+          fy = fma((double)cfy, qd, fy);
+          fz = fma((double)cfz, qd, fz);
+        } else {
+          fx += (double)cfx;
+          fy += (double)cfy;
+          fz += (double)cfz;
+        }
       }
       a0 = b0;
       a1 = b1;
@@ -299,8 +334,8 @@ __global__ void __launch_bounds__(128) k_lj_fp64(PairArgs a, const double4 *__re
   if (EV) block_partials_finish<7>(acc, red, a.partial, a.counter, a.ev, false);
 }
 
-template <int TPA, bool EV, bool ATOM, bool SINGLE, bool BATCH>
-__global__ void __launch_bounds__(128) k_lj_mixed(PairArgs a, const float4 *__restrict__ xr) {
+template <int TPA, bool EV, bool ATOM, bool SINGLE, bool BATCH, bool ISO>
+__global__ void __launch_bounds__(128) k_lj_mixed(PairArgs a, const int4 *__restrict__ xq) {
   __shared__ float tabf[6 * TABSZ];
   __shared__ double red[7 * 4];
   const int nt2 = a.ntp1 * a.ntp1;
@@ -314,7 +349,7 @@ __global__ void __launch_bounds__(128) k_lj_mixed(PairArgs a, const float4 *__re
   const bool active = i < a.n;
   double fx = 0.0, fy = 0.0, fz = 0.0;
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-  lj_atom_mixed<TPA, EV, SINGLE, BATCH>(a, xr, tabf, nt2, i, lane, active, fx, fy, fz, acc);
+  lj_atom_mixed<TPA, EV, SINGLE, BATCH, ISO>(a, xq, tabf, nt2, i, lane, active, fx, fy, fz, acc);
   lj_atom_store<TPA, EV, ATOM>(a, i, lane, active, fx, fy, fz, acc);
   if (EV) block_partials_finish<7>(acc, red, a.partial, a.counter, a.ev, false);
 }
@@ -339,7 +374,6 @@ struct RepStepArgs {
   const double *mass;
   double4 *x4;
   double *v;
-  const int *cell;
   const double4 *xhold;
   int *status, *dcount, *mail;
   unsigned int *counter;
@@ -356,9 +390,9 @@ __device__ __forceinline__ int rep_atom(const int2 *__restrict__ ranges, int r0,
   return -1;
 }
 
-template <int TPA, bool MIXED, bool SINGLE>
+template <int TPA, bool MIXED, bool SINGLE, bool ISO>
 __global__ void __launch_bounds__(512) k_rep_step(PairArgs a, const double4 *__restrict__ x4,
-                                                   const float4 *__restrict__ xr, RepStepArgs s) {
+                                                   const int4 *__restrict__ xq, RepStepArgs s) {
   namespace cg = cooperative_groups;
   __shared__ double tab[6 * TABSZ];
   __shared__ bool last;
@@ -390,7 +424,8 @@ __global__ void __launch_bounds__(512) k_rep_step(PairArgs a, const double4 *__r
     double fx = 0.0, fy = 0.0, fz = 0.0;
     double acc[7] = {0, 0, 0, 0, 0, 0, 0};
     if (MIXED)
-      lj_atom_mixed<TPA, false, SINGLE, true>(a, xr, tabf, nt2, i, lane, active, fx, fy, fz, acc);
+      lj_atom_mixed<TPA, false, SINGLE, true, ISO>(a, xq, tabf, nt2, i, lane, active, fx, fy, fz,
+                                                   acc);
     else
       lj_atom_fp64<TPA, false, SINGLE, true>(a, x4, tab, nt2, i, lane, active, fx, fy, fz, acc);
     lj_atom_store<TPA, false, false>(a, i, lane, active, fx, fy, fz, acc);
@@ -403,7 +438,7 @@ __global__ void __launch_bounds__(512) k_rep_step(PairArgs a, const double4 *__r
     const int i = rep_atom(s.ranges, r0, r1, k);
     double ke = 0.0;
     moved |= md_nve_fused_atom<false>(i, a.stride, s.dtv, s.dtf, s.mass, const_cast<double4 *>(x4),
-                                      s.v, a.f, MIXED ? const_cast<float4 *>(xr) : nullptr, s.cell,
+                                      s.v, a.f, MIXED ? const_cast<int4 *>(xq) : nullptr,
                                       a.reps.box[a.reps.rep_of_atom[i]], s.xhold, s.triggersq, ke);
   }
   if (s.xhold && __any_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0) {
@@ -424,7 +459,7 @@ __global__ void __launch_bounds__(512) k_rep_step(PairArgs a, const double4 *__r
   }
 }
 
-template <int TPA, bool MIXED>
+template <int TPA, bool MIXED, bool ISO>
 cudaError_t launch_rep_t(b200_ctx *c, const PairArgs &a, const RepStepArgs &s) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)(c->rep_groups * c->rep_cs), 1, 1);
@@ -439,18 +474,20 @@ cudaError_t launch_rep_t(b200_ctx *c, const PairArgs &a, const RepStepArgs &s) {
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   if (c->ntypes == 1)
-    return cudaLaunchKernelEx(&cfg, k_rep_step<TPA, MIXED, true>, a, (const double4 *)c->x4,
-                              (const float4 *)c->xr, s);
-  return cudaLaunchKernelEx(&cfg, k_rep_step<TPA, MIXED, false>, a, (const double4 *)c->x4,
-                            (const float4 *)c->xr, s);
+    return cudaLaunchKernelEx(&cfg, k_rep_step<TPA, MIXED, true, ISO>, a, (const double4 *)c->x4,
+                              (const int4 *)c->xq, s);
+  return cudaLaunchKernelEx(&cfg, k_rep_step<TPA, MIXED, false, ISO>, a, (const double4 *)c->x4,
+                            (const int4 *)c->xq, s);
 }
 
 template <int TPA, bool EV, bool ATOM, bool SINGLE, bool BATCH>
 void launch_t(b200_ctx *c, const PairArgs &a) {
   const int B = 128;
   const int grid = md_blocks((long long)a.n * TPA, B);
-  if (c->prec == B200_PREC_MIXED)
-    k_lj_mixed<TPA, EV, ATOM, SINGLE, BATCH><<<grid, B, 0, c->stream>>>(a, c->xr);
+  if (c->prec == B200_PREC_MIXED && md_q_iso(c))
+    k_lj_mixed<TPA, EV, ATOM, SINGLE, BATCH, true><<<grid, B, 0, c->stream>>>(a, c->xq);
+  else if (c->prec == B200_PREC_MIXED)
+    k_lj_mixed<TPA, EV, ATOM, SINGLE, BATCH, false><<<grid, B, 0, c->stream>>>(a, c->xq);
   else
     k_lj_fp64<TPA, EV, ATOM, SINGLE, BATCH><<<grid, B, 0, c->stream>>>(a, c->x4);
   c->launches++;
@@ -510,7 +547,6 @@ cudaError_t md_rep_step(b200_ctx *c, double dtv, double dtf) {
   s.mass = c->mass_dev;
   s.x4 = c->x4;
   s.v = c->v;
-  s.cell = c->cell;
   s.xhold = c->check ? c->xhold : nullptr;
   s.status = c->status;
   s.dcount = c->dec_count;
@@ -519,12 +555,24 @@ cudaError_t md_rep_step(b200_ctx *c, double dtv, double dtf) {
   s.every = c->every;
   s.delay = c->delay;
   s.check = c->check;
-  const bool mixed = c->prec == B200_PREC_MIXED;
+  const bool mixed = c->prec == B200_PREC_MIXED, iso = md_q_iso(c);
   cudaError_t e;
   switch (c->rep_tpa) {
-    case 1: e = mixed ? launch_rep_t<1, true>(c, a, s) : launch_rep_t<1, false>(c, a, s); break;
-    case 2: e = mixed ? launch_rep_t<2, true>(c, a, s) : launch_rep_t<2, false>(c, a, s); break;
-    default: e = mixed ? launch_rep_t<4, true>(c, a, s) : launch_rep_t<4, false>(c, a, s); break;
+    case 1:
+      e = !mixed ? launch_rep_t<1, false, false>(c, a, s)
+          : iso  ? launch_rep_t<1, true, true>(c, a, s)
+                 : launch_rep_t<1, true, false>(c, a, s);
+      break;
+    case 2:
+      e = !mixed ? launch_rep_t<2, false, false>(c, a, s)
+          : iso  ? launch_rep_t<2, true, true>(c, a, s)
+                 : launch_rep_t<2, true, false>(c, a, s);
+      break;
+    default:
+      e = !mixed ? launch_rep_t<4, false, false>(c, a, s)
+          : iso  ? launch_rep_t<4, true, true>(c, a, s)
+                 : launch_rep_t<4, true, false>(c, a, s);
+      break;
   }
   c->launches++;
   if (e != cudaSuccess) return e;

@@ -15,8 +15,9 @@ The cutoff of a type pair is `cut_factor * sigma` (2.5 sigma by default) and
 is not differentiated: a pair that crosses the cutoff under a parameter
 change contributes a jump that finite differences see and a gradient cannot.
 
-With precision "mixed" the pair arithmetic is FP32 on cell-relative
-coordinates and every sum is FP64; "fp64" is the FP64 reference form.
+With precision "mixed" the pair arithmetic is FP32 on separations formed from
+32-bit fixed-point coordinates and every sum is FP64; "fp64" is the FP64
+reference form.
 """
 from __future__ import annotations
 

@@ -65,6 +65,25 @@ def test_non_finite_coordinate_is_lost_atom():
     assert e.value.code == -7
 
 
+def test_mixed_box_not_longer_than_twice_the_list_cutoff():
+    # 3 x 3 x 3 fcc cells: edge 5.04 sigma, longer than the list cutoff (2.8)
+    # but not twice it.  The mixed form forms separations at the minimum
+    # image of 32-bit fixed-point coordinates, which needs the longer box.
+    a = inputs.lj_lattice_constant("fcc", 0.8442)
+    x = inputs.lattice("fcc", 3, 3, 3, a)
+    s = System("lj", "mixed")
+    s.set_box([0, 0, 0], [3 * a] * 3)
+    p = PairLJCut(2.5)
+    p.coeff(1, 1, 1.0, 1.0, 2.5)
+    s.set_pair(p)
+    s.set_mass([1.0])
+    s.set_atoms(x)
+    with pytest.raises(B200Error) as e:
+        s.setup()
+    assert e.value.code == -6
+    assert "twice the list cutoff" in str(e.value)
+
+
 def test_box_smaller_than_ghost_cutoff():
     a = inputs.lj_lattice_constant("fcc", 0.8442)
     x = inputs.lattice("fcc", 1, 1, 1, a)
