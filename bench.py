@@ -269,6 +269,7 @@ def load_traffic():
         return {}
 
 
+STEP_BYTES_PER_ATOM = 120.0  # one-launch LJ step: x, v read and written, f written (FP64)
 EAM_BYTES_PER_ATOM_STEP = 200.0   # x, v, f, rho, fp traffic of one EAM step (FP64 state)
 EAM_HALF_PAIRS = 21.0             # half pairs inside 4.95 A per atom on the fcc lattice
 EAM_FLOP_PER_ATOM_STEP = 80.0 * EAM_HALF_PAIRS + 15.0
@@ -775,10 +776,12 @@ def profile_case(args):
     ext = torch.cuda.ExternalStream(s.stream)
     device_time_run(s, torch, ext, flush, MD_STEPS, (x, v))
     ph = s.timing(reset=True)
+    pieces = piece_times(s, torch, flush, (x, v), runs=1)
     print(json.dumps({"case": args.case, "atoms": s.n, "steps": args.steps,
                       "matom_steps_per_s": s.n * MD_STEPS * args.steps / (total * 1e3),
                       "launch": s.launch(), "neigh": s.neigh_stats(),
-                      "phases_ms_per_md_step": {k: ph[k] / max(ph["steps"], 1) for k in s.PHASES}}))
+                      "phases_ms_per_md_step": {k: ph[k] / max(ph["steps"], 1) for k in s.PHASES},
+                      "pieces_ms_per_md_step": pieces}))
     s.close()
 
 
@@ -818,6 +821,22 @@ def phase_times(s, torch, flush, start, runs=2):
     ph = s.timing(reset=True)
     s.set_timing(False)
     return {k: ph[k] / max(ph["steps"], 1) for k in s.PHASES}
+
+
+def piece_times(s, torch, flush, start, runs=2):
+    """Per-MD-step device time of whole step pieces with the run's own step
+    form (timing mode 2: two stream events around each piece): "initial"
+    (chunk starts), "neigh" (rebuilds) and "pair1" (forces with both
+    half-steps: the one-launch step kernel for lj/cut)."""
+    ext = torch.cuda.ExternalStream(s.stream)
+    s.set_timing(2)
+    device_time_run(s, torch, ext, flush, MD_STEPS, start)
+    s.timing(reset=True)
+    for _ in range(runs):
+        device_time_run(s, torch, ext, flush, MD_STEPS, start)
+    ph = s.timing(reset=True)
+    s.set_timing(False)
+    return {k: ph[k] / max(ph["steps"], 1) for k in ("initial", "neigh", "pair1")}
 
 
 def e2e_block(torch, s, x, v, K, ws=1):
@@ -1068,13 +1087,21 @@ def main():
     sysm = make_lj("mixed", x4, v4, hi4)
     value, total_ms, launches, clk = headline_timed(sysm, torch, flush, K, W, start, ws, dev)
     phases = phase_times(sysm, torch, flush, start)
+    pieces = piece_times(sysm, torch, flush, start)
     peak, peak_kind = load_peaks()
-    # algorithmic bytes of the dominant kernel (k_lj_mixed): x read (24 B)
-    # and f written (24 B) per atom, FP64 state
-    achieved = 48.0 * n4 / (phases["pair1"] * 1e-3) / 1e9
+    # the dominant kernel is the one-launch step k_lj_step (forces, this
+    # step's final and the next initial half-step); its algorithmic bytes per
+    # atom, FP64 state: x read and written (48 B), v read and written (48 B),
+    # f written (24 B).  Its time is the step piece's (with the one-thread
+    # k_decide after it), from events around the piece.
+    achieved = STEP_BYTES_PER_ATOM * n4 / (pieces["pair1"] * 1e-3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": load_traffic().get("lj4m_mixed_pair1"),
-                "kernel": "k_lj_mixed", "kernel_ms": phases["pair1"],
+                "frac": achieved / peak, "traffic": load_traffic().get("lj4m_mixed_step"),
+                "kernel": "k_lj_step", "kernel_ms": pieces["pair1"],
+                "alg_bytes_per_atom": STEP_BYTES_PER_ATOM,
+                "pair_kernel": {"kernel": "k_lj_mixed (phase-timed steps)",
+                                "ms": phases["pair1"],
+                                "achieved_gbs": 48.0 * n4 / (phases["pair1"] * 1e-3) / 1e9},
                 "peak_source": f"{peak_kind} hbm_gbs",
                 # whole-step figures from the headline runs (timing events off),
                 # so that they follow from `value`
@@ -1087,11 +1114,13 @@ def main():
     s64 = make_lj("fp64", x4, v4, hi4)
     v64, t64, _, _ = headline_timed(s64, torch, flush, K, W, start, ws, dev)
     ph64 = phase_times(s64, torch, flush, start)
+    pc64 = piece_times(s64, torch, flush, start)
     s64.close()
 
     extras = {"fp64": v64, "mixed_over_fp64": value / v64,
               "ms_per_md_step": {"mixed": total_ms / (K * MD_STEPS), "fp64": t64 / (K * MD_STEPS)},
-              "phases_ms_per_md_step": {"mixed": phases, "fp64": ph64}}
+              "phases_ms_per_md_step": {"mixed": phases, "fp64": ph64},
+              "pieces_ms_per_md_step": {"mixed": pieces, "fp64": pc64}}
     if not args.no_extras:
         if rank == 0:  # the oracle uses every host core: one rank at a time
             ref = lj4m_oracle_state(hi4)

@@ -234,7 +234,11 @@ int b200_get_launch(const b200_ctx *ctx, int *threads_per_atom, int *block_size)
      2 pair pass 1 (LJ force; EAM density + embedding)
      3 pair pass 2 (EAM force; zero for LJ)
      4 fix nve final half-step (+ kinetic energy and thermo row on output steps)
-   b200_get_timing returns milliseconds summed over the timed steps. */
+   b200_get_timing returns milliseconds summed over the timed steps.
+   on = 2 times whole pieces instead, with the run's own step form kept
+   (lj/cut forces and both half-steps in one launch): two stream events around
+   each piece; phase 0 = initial half-steps at chunk starts, 1 = rebuilds,
+   2 = forces with their half-steps; 3 and 4 stay zero. */
 int b200_set_timing(b200_ctx *ctx, int on);
 /* on = 1 (default): b200_run replays captured CUDA graphs of the step's
    pieces (initial half-step + decision, rebuild, forces + final half-step).

@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <algorithm>
 #include <vector>
 
 #include <atomic>
@@ -50,7 +51,7 @@ void dfree(T *&p) {
 }
 
 void invalidate_graphs(b200_ctx *c) {
-  for (int k = 0; k < MD_NPIECES; k++) {
+  for (int k = 0; k < MD_NGRAPHS; k++) {
     if (c->step_exec[k]) cudaGraphExecDestroy(c->step_exec[k]);
     if (c->step_graph[k]) cudaGraphDestroy(c->step_graph[k]);
     c->step_exec[k] = nullptr;
@@ -515,33 +516,41 @@ int rebuild_sync(b200_ctx *c) {
 
 int autotune(b200_ctx *c) {
   // Launch-shape search: time the force pass for each threads-per-atom
-  // value and keep the fastest (ties to fewer threads per atom).
+  // value and keep the fastest (ties to fewer threads per atom).  Each
+  // candidate is timed in three rounds of five passes, the rounds
+  // interleaved across the candidates, and its fastest round counts: at a
+  // few microseconds per pass a single short timing picked different shapes
+  // from run to run.
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
-  float best = 1e30f;
-  int best_tpa = 1;
   const int cand[6] = {1, 2, 4, 8, 16, 32};
-  for (int k = 0; k < 6; k++) {
-    c->tpa = cand[k];
-    int rc = pair_compute_dev(c, false, false, nullptr, nullptr);
-    if (rc) return rc;
-    CK(cudaEventRecord(e0, c->stream));
-    for (int r = 0; r < 3; r++) {
-      rc = pair_compute_dev(c, false, false, nullptr, nullptr);
+  float tmin[6] = {1e30f, 1e30f, 1e30f, 1e30f, 1e30f, 1e30f};
+  for (int round = 0; round < 3; round++)
+    for (int k = 0; k < 6; k++) {
+      c->tpa = cand[k];
+      int rc = pair_compute_dev(c, false, false, nullptr, nullptr);
       if (rc) return rc;
+      CK(cudaEventRecord(e0, c->stream));
+      for (int r = 0; r < 5; r++) {
+        rc = pair_compute_dev(c, false, false, nullptr, nullptr);
+        if (rc) return rc;
+      }
+      CK(cudaEventRecord(e1, c->stream));
+      CK(cudaEventSynchronize(e1));
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, e0, e1));
+      if (ms < tmin[k]) tmin[k] = ms;
     }
-    CK(cudaEventRecord(e1, c->stream));
-    CK(cudaEventSynchronize(e1));
-    float ms = 0;
-    CK(cudaEventElapsedTime(&ms, e0, e1));
-    if (ms < best * 0.97f) {
-      best = ms;
-      best_tpa = cand[k];
-    }
-  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  float best = 1e30f;
+  int best_tpa = 1;
+  for (int k = 0; k < 6; k++)
+    if (tmin[k] < best * 0.97f) {
+      best = tmin[k];
+      best_tpa = cand[k];
+    }
   c->tpa = best_tpa;
   c->tuned = true;
   return B200_OK;
@@ -605,6 +614,12 @@ cudaError_t launch_piece(b200_ctx *c, int kind, double dtv, double dtf, cudaEven
   } else {
     const bool out = kind == PIECE_POST_OUT || kind == PIECE_FUSED_OUT;
     const bool fused = kind == PIECE_FUSED_OUT || kind == PIECE_FUSED;
+    if (fused && md_lj_step_ok(c)) {
+      // lj/cut: this step's forces, final half-step and thermo row and the
+      // next step's initial half-step and decision in one launch (the caller
+      // swaps the position buffers after it)
+      return md_lj_step(c, dtv, dtf, out);
+    }
     if (ev) e = record(c, ev[0]);
     if (kind == PIECE_FUSED && c->rep_onelaunch && c->nrep && c->pstyle == B200_PAIR_LJ_CUT) {
       // replicas: this step's forces, final half-step and the next step's
@@ -701,7 +716,10 @@ int tune_replica_step(b200_ctx *c) {
   return B200_OK;
 }
 
+// captures piece `kind` for the current position buffers, in graph slot
+// kind + MD_NPIECES * pos_parity
 int capture_piece(b200_ctx *c, int kind, double dtv, double dtf) {
+  const int slot = kind + MD_NPIECES * c->pos_parity;
   const bool tm = c->timing && kind != PIECE_REBUILD;
   const long long launches0 = c->launches;
   cudaGraph_t g = nullptr;
@@ -715,25 +733,25 @@ int capture_piece(b200_ctx *c, int kind, double dtv, double dtf) {
                    cudaGetErrorString(e2));
   }
   int kernels = 0;
-  c->ev_nodes[kind].clear();
-  int rc = count_kernels(c, g, &kernels, &c->ev_nodes[kind]);
+  c->ev_nodes[slot].clear();
+  int rc = count_kernels(c, g, &kernels, &c->ev_nodes[slot]);
   if (rc) {
     cudaGraphDestroy(g);
     return rc;
   }
   const size_t want = !tm ? 0 : (kind == PIECE_PRE ? 2 : 4);
-  if (c->ev_nodes[kind].size() != want) {
+  if (c->ev_nodes[slot].size() != want) {
     cudaGraphDestroy(g);
     return set_err(c, B200_ERR_CUDA, "graph capture: expected %zu event nodes, found %zu", want,
-                   c->ev_nodes[kind].size());
+                   c->ev_nodes[slot].size());
   }
-  e = cudaGraphInstantiate(&c->step_exec[kind], g, 0);
+  e = cudaGraphInstantiate(&c->step_exec[slot], g, 0);
   if (e != cudaSuccess) {
     cudaGraphDestroy(g);
     return set_err(c, B200_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
   }
-  c->step_graph[kind] = g;
-  c->step_kernels[kind] = kernels;
+  c->step_graph[slot] = g;
+  c->step_kernels[slot] = kernels;
   return B200_OK;
 }
 
@@ -765,29 +783,44 @@ int wait_decision(b200_ctx *c, bool *rebuild) {
   return B200_OK;
 }
 
-// run one piece: graph replay, or the kernels themselves with graphs off
+// run one piece: graph replay, or the kernels themselves with graphs off.  A
+// fused piece that ran md_lj_step leaves the new positions in the other
+// buffer, which becomes current.
 int run_piece(b200_ctx *c, int kind, double dtv, double dtf, cudaEvent_t *ev) {
+  const bool swap = (kind == PIECE_FUSED || kind == PIECE_FUSED_OUT) && md_lj_step_ok(c);
   if (!c->use_graphs) {
     CK(launch_piece(c, kind, dtv, dtf, ev));
-    return B200_OK;
+  } else {
+    const int slot = kind + MD_NPIECES * c->pos_parity;
+    if (ev)
+      for (size_t k = 0; k < c->ev_nodes[slot].size(); k++)
+        CK(cudaGraphExecEventRecordNodeSetEvent(c->step_exec[slot], c->ev_nodes[slot][k], ev[k]));
+    CK(cudaGraphLaunch(c->step_exec[slot], c->stream));
+    c->launches += c->step_kernels[slot];
   }
-  if (ev)
-    for (size_t k = 0; k < c->ev_nodes[kind].size(); k++)
-      CK(cudaGraphExecEventRecordNodeSetEvent(c->step_exec[kind], c->ev_nodes[kind][k], ev[k]));
-  CK(cudaGraphLaunch(c->step_exec[kind], c->stream));
-  c->launches += c->step_kernels[kind];
+  if (swap) md_swap_positions(c);
   return B200_OK;
 }
 
 int ensure_graphs(b200_ctx *c, double dtv, double dtf, double ftm2v) {
   if (!c->use_graphs) return B200_OK;
   if (c->graph_valid) return B200_OK;
-  for (int kind = 0; kind < MD_NPIECES; kind++) {
-    // the fused pieces are not used with phase timers on (their events
-    // would mix two steps)
-    if (c->timing && (kind == PIECE_FUSED || kind == PIECE_FUSED_OUT)) continue;
-    int rc = capture_piece(c, kind, dtv, dtf);
-    if (rc) return rc;
+  // with md_lj_step the position buffers alternate from step to step: every
+  // piece is captured for both (the pointer swap is host state only)
+  const int sets = md_lj_step_ok(c) ? 2 : 1;
+  for (int set = 0; set < sets; set++) {
+    if (set) md_swap_positions(c);
+    for (int kind = 0; kind < MD_NPIECES; kind++) {
+      // the fused pieces are not used with phase timers on (their events
+      // would mix two steps)
+      if (c->timing && (kind == PIECE_FUSED || kind == PIECE_FUSED_OUT)) continue;
+      int rc = capture_piece(c, kind, dtv, dtf);
+      if (rc) {
+        if (set) md_swap_positions(c);
+        return rc;
+      }
+    }
+    if (set) md_swap_positions(c);
   }
   c->graph_valid = true;
   c->graph_dt = dtv;
@@ -929,7 +962,7 @@ int b200_destroy(b200_ctx *c) {
   dfree(c->x4); dfree(c->x4b); dfree(c->v); dfree(c->vb); dfree(c->f);
   dfree(c->orig); dfree(c->origb); dfree(c->image); dfree(c->imageb); dfree(c->cell);
   dfree(c->where); dfree(c->ghost);
-  dfree(c->xq); dfree(c->xhold); dfree(c->xfer); dfree(c->rho); dfree(c->fp); dfree(c->fpf); dfree(c->mass_dev);
+  dfree(c->xq); dfree(c->xqb); dfree(c->xhold); dfree(c->xfer); dfree(c->rho); dfree(c->fp); dfree(c->fpf); dfree(c->mass_dev);
   dfree(c->eam_eatom); dfree(c->d_rep_grp_first); dfree(c->d_rep_ranges);
   dfree(c->cell_count); dfree(c->cell_start); dfree(c->scan_tmp);
   dfree(c->slot); dfree(c->perm); dfree(c->cell_tmp);
@@ -1152,6 +1185,7 @@ int b200_upload_atoms(b200_ctx *c, int n, const double *x, const double *v, cons
     CK(dalloc(&c->where, stride));
     CK(dalloc(&c->ghost, stride));
     CK(dalloc(&c->xq, stride));
+    CK(dalloc(&c->xqb, stride));
     CK(dalloc(&c->xhold, stride));
     CK(dalloc(&c->rho, stride));
     CK(dalloc(&c->fp, stride));
@@ -1635,6 +1669,13 @@ int b200_run(b200_ctx *c, int nsteps, double dt, double ftm2v, int thermo_every,
     int rc = ensure_events(c, (size_t)(MD_NPHASE + 1) * chunk);
     if (rc) return rc;
   }
+  // timing mode 2: two events around each piece, at most four pieces a step
+  std::vector<signed char> piece_kind;
+  if (c->timing_pieces) {
+    int rc = ensure_events(c, (size_t)8 * chunk);
+    if (rc) return rc;
+    piece_kind.assign((size_t)4 * chunk, -1);
+  }
   {
     int rc = ensure_graphs(c, dtv, dtf, ftm2v);
     if (rc) return rc;
@@ -1670,9 +1711,21 @@ int b200_run(b200_ctx *c, int nsteps, double dt, double ftm2v, int thermo_every,
     // starts with its own initial half-step, so snapshots and replays see
     // whole steps.
     bool pre_done = false;
+    if (c->timing_pieces) std::fill(piece_kind.begin(), piece_kind.end(), (signed char)-1);
     for (long long t = s; t <= s_end; t++) {
       cudaEvent_t *ev = c->timing ? &c->ev_pool[(size_t)(t - s) * (MD_NPHASE + 1)] : nullptr;
-      if (!pre_done) rc = run_piece(c, PIECE_PRE, dtv, dtf, ev);
+      // piece k of step t; timing mode 2 brackets it with two stream events
+      auto piece = [&](int k, int kind, cudaEvent_t *pev) -> int {
+        if (!c->timing_pieces) return run_piece(c, kind, dtv, dtf, pev);
+        const size_t slot = (size_t)(t - s) * 4 + k;
+        CK(cudaEventRecord(c->ev_pool[2 * slot], c->stream));
+        const int r = run_piece(c, kind, dtv, dtf, nullptr);
+        if (r) return r;
+        CK(cudaEventRecord(c->ev_pool[2 * slot + 1], c->stream));
+        piece_kind[slot] = (signed char)kind;
+        return B200_OK;
+      };
+      if (!pre_done) rc = piece(0, PIECE_PRE, ev);
       if (rc) return rc;
       ago++;
       bool rebuild = false;
@@ -1691,14 +1744,14 @@ int b200_run(b200_ctx *c, int nsteps, double dt, double ftm2v, int thermo_every,
         }
       }
       if (rebuild) {
-        rc = run_piece(c, PIECE_REBUILD, dtv, dtf, nullptr);
+        rc = piece(1, PIECE_REBUILD, nullptr);
         if (rc) return rc;
         ago = 0;
       }
       const bool fuse = !c->timing && t < s_end;
       const int post = fuse ? (is_out(t) ? PIECE_FUSED_OUT : PIECE_FUSED)
                             : (is_out(t) ? PIECE_POST_OUT : PIECE_POST);
-      rc = run_piece(c, post, dtv, dtf, ev ? ev + 2 : nullptr);
+      rc = piece(2, post, ev ? ev + 2 : nullptr);
       if (rc) return rc;
       pre_done = fuse;
     }
@@ -1737,6 +1790,25 @@ int b200_run(b200_ctx *c, int nsteps, double dt, double ftm2v, int thermo_every,
       rc = grow_list(c, cap, true);
       if (!rc) rc = ensure_graphs(c, dtv, dtf, ftm2v);
       if (rc) return rc;
+    }
+    if (c->timing_pieces) {
+      // mode 2: phase 0 the initial half-step pieces (chunk starts), 1 the
+      // rebuilds, 2 the force pieces with their half-steps (the one-launch
+      // step for lj/cut)
+      for (long long t = s; t <= s_end; t++) {
+        float step = 0.f;
+        for (int k = 0; k < 4; k++) {
+          const size_t slot = (size_t)(t - s) * 4 + k;
+          const int kind = piece_kind[slot];
+          if (kind < 0) continue;
+          float ms = 0.f;
+          CK(cudaEventElapsedTime(&ms, c->ev_pool[2 * slot], c->ev_pool[2 * slot + 1]));
+          c->phase_ms[kind == PIECE_PRE ? 0 : (kind == PIECE_REBUILD ? 1 : 2)] += ms;
+          step += ms;
+        }
+        c->step_ms.push_back(step);
+      }
+      c->phase_steps += s_end - s + 1;
     }
     if (c->timing) {
       for (long long t = s; t <= s_end; t++) {
@@ -1865,8 +1937,9 @@ int b200_get_launch(const b200_ctx *c, int *tpa, int *block) {
 long long b200_kernel_launches(const b200_ctx *c) { return c ? c->launches : 0; }
 
 int b200_set_timing(b200_ctx *c, int on) {
-  if (!c) return B200_ERR_ARG;
-  c->timing = on != 0;
+  if (!c || on < 0 || on > 2) return B200_ERR_ARG;
+  c->timing = on == 1;
+  c->timing_pieces = on == 2;
   invalidate_graphs(c);
   return B200_OK;
 }

@@ -335,24 +335,25 @@ __device__ __forceinline__ void md_record_row_dev(int *status, const double *ev,
   status[ST_ROW] = r + 1;
 }
 
-// FixNVE::final_integrate of this step for sorted atom i, the kinetic-energy
-// term of the thermo output (KE, into ke), then FixNVE::initial_integrate of
-// the next step (src/fix_nve.cpp:65-142): every product and sum rounded
-// separately as in the reference.  Refreshes the fixed-point copy (xq, mixed
-// form) and returns whether the atom moved more than half the skin since the
-// last build (xhold, check yes).
+// FixNVE::final_integrate of this step for sorted atom i with its force
+// (fx, fy, fz), the kinetic-energy term of the thermo output (KE, into ke),
+// then FixNVE::initial_integrate of the next step (src/fix_nve.cpp:65-142):
+// every product and sum rounded separately as in the reference.  The new
+// position goes to x4_out (x4_in itself for an update in place) and, in the
+// mixed form, its fixed-point copy to xq_out.  Returns whether the atom moved
+// more than half the skin since the last build (xhold, check yes).
 template <bool KE>
-__device__ __forceinline__ bool md_nve_fused_atom(int i, int stride, double dtv, double dtf,
-                                                  const double *__restrict__ mass,
-                                                  double4 *__restrict__ x4, double *__restrict__ v,
-                                                  const double *__restrict__ f,
-                                                  int4 *__restrict__ xq, const BoxGeom &box,
-                                                  const double4 *__restrict__ xhold,
-                                                  double triggersq, double &ke) {
-  double4 p = x4[i];
+__device__ __forceinline__ bool md_nve_step_atom(int i, int stride, double dtv, double dtf,
+                                                 const double *__restrict__ mass,
+                                                 const double4 *x4_in, double4 *x4_out,
+                                                 double *__restrict__ v, double fx, double fy,
+                                                 double fz, int4 *__restrict__ xq_out,
+                                                 const BoxGeom &box,
+                                                 const double4 *__restrict__ xhold,
+                                                 double triggersq, double &ke) {
+  double4 p = x4_in[i];
   const double m = mass[(int)p.w];
   const double dtfm = dtf / m;
-  const double fx = f[i], fy = f[stride + i], fz = f[2 * stride + i];
   double vx = __dadd_rn(v[i], __dmul_rn(dtfm, fx));
   double vy = __dadd_rn(v[stride + i], __dmul_rn(dtfm, fy));
   double vz = __dadd_rn(v[2 * stride + i], __dmul_rn(dtfm, fz));
@@ -367,12 +368,26 @@ __device__ __forceinline__ bool md_nve_fused_atom(int i, int stride, double dtv,
   v[i] = vx;
   v[stride + i] = vy;
   v[2 * stride + i] = vz;
-  x4[i] = p;
-  if (xq) xq[i] = md_xq(p, box);
+  x4_out[i] = p;
+  if (xq_out) xq_out[i] = md_xq(p, box);
   if (xhold) {
     const double4 h = xhold[i];
     const double rsq = dsq3(__dsub_rn(p.x, h.x), __dsub_rn(p.y, h.y), __dsub_rn(p.z, h.z));
     return rsq > triggersq;
   }
   return false;
+}
+
+// The same step for atom i with its force read from f and its position
+// updated in place (k_nve_fused, the replica step).
+template <bool KE>
+__device__ __forceinline__ bool md_nve_fused_atom(int i, int stride, double dtv, double dtf,
+                                                  const double *__restrict__ mass,
+                                                  double4 *__restrict__ x4, double *__restrict__ v,
+                                                  const double *__restrict__ f,
+                                                  int4 *__restrict__ xq, const BoxGeom &box,
+                                                  const double4 *__restrict__ xhold,
+                                                  double triggersq, double &ke) {
+  return md_nve_step_atom<KE>(i, stride, dtv, dtf, mass, x4, x4, v, f[i], f[stride + i],
+                              f[2 * stride + i], xq, box, xhold, triggersq, ke);
 }

@@ -12,6 +12,8 @@
 // forces + final half-step (with / without thermo output), and the same two
 // with the next step's initial half-step and decision fused in
 #define MD_NPIECES 6
+// graph slots: every piece for each of the two position buffers (md_lj_step)
+#define MD_NGRAPHS (2 * MD_NPIECES)
 #include "../../include/b200md.h"
 
 // timer phases of one step
@@ -101,6 +103,8 @@ struct b200_ctx {
   int *ghost = nullptr;
   bool ghosts_on = false;
   int4 *xq = nullptr;         // mixed: fixed-point coordinates (md_xq)
+  int4 *xqb = nullptr;        // mixed: second buffer of xq (md_lj_step)
+  int pos_parity = 0;         // md_lj_step buffer swaps since allocation, mod 2
   double4 *xhold = nullptr;   // positions at the last build (check yes)
   // device staging of host transfers (upload, download, per-atom energy and
   // virial), kept between calls so a call maps no new memory
@@ -196,9 +200,9 @@ struct b200_ctx {
   // CUDA graph of one MD step (captured lazily by b200_run)
   // graphs of the step pieces: [0] initial half-step + decision, [1] rebuild,
   // [2] forces + final half-step with thermo output, [3] the same without
-  cudaGraphExec_t step_exec[MD_NPIECES] = {};
-  cudaGraph_t step_graph[MD_NPIECES] = {};
-  int step_kernels[MD_NPIECES] = {};                    // kernel nodes per graph
+  cudaGraphExec_t step_exec[MD_NGRAPHS] = {};
+  cudaGraph_t step_graph[MD_NGRAPHS] = {};
+  int step_kernels[MD_NGRAPHS] = {};                    // kernel nodes per graph
   bool graph_valid = false;
   double graph_dt = 0, graph_ftm2v = 0;
   int graph_tpa = 0;
@@ -208,8 +212,9 @@ struct b200_ctx {
   // phase timers (Timer categories of the reference, src/timer.h:19-20):
   // event-record nodes at the phase boundaries of every step graph
   bool timing = false;
+  bool timing_pieces = false;  // b200_set_timing(ctx, 2): device time of whole pieces
   cudaEvent_t ph_event[MD_NPHASE + 1] = {};           // placeholders used at capture
-  std::vector<cudaGraphNode_t> ev_nodes[MD_NPIECES];   // event-record nodes per graph
+  std::vector<cudaGraphNode_t> ev_nodes[MD_NGRAPHS];   // event-record nodes per graph
   std::vector<cudaEvent_t> ev_pool;                    // per-step events of a chunk
   double phase_ms[MD_NPHASE] = {0};
   std::vector<float> step_ms;  // device time of each timed step (first to last phase event)
@@ -258,6 +263,13 @@ cudaError_t md_eam_fp_halo(b200_ctx *c, int m, const int *idx, double *buf, bool
 // half-step and the next step's initial half-step and rebuild decision, for
 // every replica, in one cluster launch (non-output steps)
 cudaError_t md_rep_step(b200_ctx *c, double dtv, double dtf);
+// one MD step of lj/cut in one launch (pair forces, this step's final and the
+// next step's initial half-step, thermo row, rebuild decision), reading the
+// current positions and writing the other position buffer; md_swap_positions
+// makes that buffer current.  md_lj_step_ok: the context can use it.
+bool md_lj_step_ok(const b200_ctx *c);
+cudaError_t md_lj_step(b200_ctx *c, double dtv, double dtf, bool out);
+void md_swap_positions(b200_ctx *c);
 // group plan of the one-launch step: cluster size cs, block size, groups
 int md_rep_plan(b200_ctx *c, int cs, int block, int tpa);
 // ---- integration (integrate.cu) --------------------------------------------

@@ -354,6 +354,117 @@ __global__ void __launch_bounds__(128) k_lj_mixed(PairArgs a, const int4 *__rest
   if (EV) block_partials_finish<7>(acc, red, a.partial, a.counter, a.ev, false);
 }
 
+// One MD step of lj/cut after the neighbor list, in one launch: each atom's
+// pair forces (lj_atom_mixed / lj_atom_fp64, the same code and order as
+// k_lj_mixed / k_lj_fp64), then, by the atom's first lane, the final
+// half-step of this step, its kinetic-energy term on an output step and the
+// initial half-step of the next (md_nve_step_atom, the arithmetic of
+// k_nve_fused).  The neighbours' positions are gathered from `cur` while the
+// new positions go to `nxt`, a second buffer, so no update can reach a gather
+// of the same launch; the host swaps the two buffers after the launch.  Mixed
+// form: cur/nxt are the fixed-point coordinates and the FP64 positions are
+// updated in place (the mixed gathers never read them); FP64 form: cur/nxt
+// are the FP64 positions.  On an output step the last block to finish adds
+// the energy, virial and kinetic energy in block order, records the thermo row
+// and makes the next step's rebuild decision, as k_nve_fused does.  Other
+// steps end with no block-completion count: one returning atomic per block
+// lengthens every block's life (with that count on every step the 4M-atom LJ
+// step ran at 5,020 Matom-steps/s, without it at 5,723), so the decision is a
+// one-thread kernel after this one (md_lj_step).
+struct StepArgs {
+  double dtv, dtf, triggersq;
+  const double *mass;
+  double4 *x4;      // mixed form: FP64 positions, updated in place
+  const void *cur;  // positions the gathers read: int4 (mixed) or double4
+  void *nxt;        // positions after the next initial half-step
+  double *v;
+  const double4 *xhold;
+  int *status, *dcount, *mail;
+  double *rows;
+  int rows_cap, every, delay, check;
+};
+
+template <int TPA, bool OUT, bool SINGLE, bool MIXED>
+__global__ void __launch_bounds__(128) k_lj_step(PairArgs a, StepArgs s) {
+  __shared__ double tab[6 * TABSZ];
+  __shared__ double red[8 * 4];
+  __shared__ bool last;
+  float *tabf = reinterpret_cast<float *>(tab);
+  const int nt2 = a.ntp1 * a.ntp1;
+  if (!SINGLE) {
+    for (int k = threadIdx.x; k < 6 * nt2; k += blockDim.x) {
+      const double t = a.tables[(TAB_CUTSQ + k / nt2) * TABSZ + k % nt2];
+      if (MIXED) tabf[k] = (float)t;
+      else tab[k] = t;
+    }
+    __syncthreads();
+  }
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = t / TPA, lane = t % TPA;
+  const bool active = i < a.n;
+  double fx = 0.0, fy = 0.0, fz = 0.0;
+  double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+  if (MIXED)
+    lj_atom_mixed<TPA, OUT, SINGLE, false, true>(a, static_cast<const int4 *>(s.cur), tabf, nt2,
+                                                  i, lane, active, fx, fy, fz, acc);
+  else
+    lj_atom_fp64<TPA, OUT, SINGLE, false>(a, static_cast<const double4 *>(s.cur), tab, nt2, i,
+                                          lane, active, fx, fy, fz, acc);
+  fx = lane_sum<TPA>(fx);
+  fy = lane_sum<TPA>(fy);
+  fz = lane_sum<TPA>(fz);
+  double ke = 0.0;
+  bool moved = false;
+  if (active && lane == 0) {
+    a.f[i] = fx;
+    a.f[a.stride + i] = fy;
+    a.f[2 * a.stride + i] = fz;
+    if (MIXED)
+      moved = md_nve_step_atom<OUT>(i, a.stride, s.dtv, s.dtf, s.mass, s.x4, s.x4, s.v, fx, fy,
+                                    fz, static_cast<int4 *>(s.nxt), a.box, s.xhold, s.triggersq,
+                                    ke);
+    else
+      moved = md_nve_step_atom<OUT>(i, a.stride, s.dtv, s.dtf, s.mass,
+                                    static_cast<const double4 *>(s.cur),
+                                    static_cast<double4 *>(s.nxt), s.v, fx, fy, fz, nullptr,
+                                    a.box, s.xhold, s.triggersq, ke);
+  }
+  if (s.xhold && __any_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0) {
+    atomicOr(&s.status[ST_MOVED], 1);
+    if (OUT) __threadfence();  // the flag is visible before this block counts itself done
+  }
+  if (!OUT) return;
+  double v8[8];
+#pragma unroll
+  for (int k = 0; k < 7; k++) v8[k] = acc[k];
+  v8[7] = ke;
+  block_sum<8>(v8, red);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < 8; k++) a.partial[(size_t)blockIdx.x * 8 + k] = v8[k];
+    __threadfence();
+    last = atomicAdd(a.counter, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  // block partials added in a fixed order: reproducible run to run
+  double sum[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (unsigned int b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+#pragma unroll
+    for (int k = 0; k < 8; k++) sum[k] += __ldcg(&a.partial[(size_t)b * 8 + k]);
+  __syncthreads();
+  block_sum<8>(sum, red);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < 8; k++) a.ev[k] = sum[k];
+    md_record_row_dev(s.status, a.ev, s.rows, s.rows_cap);
+    md_decide_dev(s.status, s.every, s.delay, s.check, s.dcount, s.mail);
+    *a.counter = 0u;
+  }
+}
+
 // One MD step of every replica of a batched context in one launch.  Cluster g
 // (rep_cs CTAs) owns a fixed set of whole replicas: the concatenation of the
 // atom ranges ranges[first[g] .. first[g+1]).  Each CTA takes an equal share
@@ -658,4 +769,77 @@ cudaError_t md_lj_compute(b200_ctx *c, bool ev, bool atom_ev, double *eatom, dou
     default: launch_tpa<32>(c, a, ev, atom_ev, single); break;
   }
   return cudaGetLastError();
+}
+
+// ---- one launch per MD step (k_lj_step) ---------------------------------
+
+namespace {
+template <int TPA, bool OUT, bool SINGLE>
+void launch_step_t(b200_ctx *c, const PairArgs &a, const StepArgs &s) {
+  const int B = 128;
+  const int grid = md_blocks((long long)a.n * TPA, B);
+  if (c->prec == B200_PREC_MIXED)
+    k_lj_step<TPA, OUT, SINGLE, true><<<grid, B, 0, c->stream>>>(a, s);
+  else
+    k_lj_step<TPA, OUT, SINGLE, false><<<grid, B, 0, c->stream>>>(a, s);
+}
+
+template <int TPA>
+void launch_step_tpa(b200_ctx *c, const PairArgs &a, const StepArgs &s, bool out) {
+  const bool single = c->ntypes == 1;
+  if (out) single ? launch_step_t<TPA, true, true>(c, a, s) : launch_step_t<TPA, true, false>(c, a, s);
+  else single ? launch_step_t<TPA, false, true>(c, a, s) : launch_step_t<TPA, false, false>(c, a, s);
+}
+}  // namespace
+
+// One box only: a replica batch keeps its tuned step (the graph of the pair
+// kernel and k_nve_fused, or k_rep_step), which measured 5 % faster than
+// k_lj_step for the 256-replica batch.
+bool md_lj_step_ok(const b200_ctx *c) {
+  return c->pstyle == B200_PAIR_LJ_CUT && c->tpa >= 1 && c->tpa <= 8 &&
+         (c->prec != B200_PREC_MIXED || md_q_iso(c)) && c->nrep == 0 && !c->ghosts_on;
+}
+
+cudaError_t md_lj_step(b200_ctx *c, double dtv, double dtf, bool out) {
+  const PairArgs a = pair_args(c, nullptr, nullptr);
+  StepArgs s;
+  s.dtv = dtv;
+  s.dtf = dtf;
+  s.triggersq = 0.25 * c->skin * c->skin;  // src/neighbor.cpp:239
+  s.mass = c->mass_dev;
+  s.x4 = c->x4;
+  if (c->prec == B200_PREC_MIXED) {
+    s.cur = c->xq;
+    s.nxt = c->xqb;
+  } else {
+    s.cur = c->x4;
+    s.nxt = c->x4b;
+  }
+  s.v = c->v;
+  s.xhold = c->check ? c->xhold : nullptr;
+  s.status = c->status;
+  s.dcount = c->dec_count;
+  s.mail = c->mail_dev;
+  s.rows = c->rows;
+  s.rows_cap = c->rows_cap;
+  s.every = c->every;
+  s.delay = c->delay;
+  s.check = c->check;
+  switch (c->tpa) {
+    case 1: launch_step_tpa<1>(c, a, s, out); break;
+    case 2: launch_step_tpa<2>(c, a, s, out); break;
+    case 4: launch_step_tpa<4>(c, a, s, out); break;
+    default: launch_step_tpa<8>(c, a, s, out); break;
+  }
+  c->launches++;
+  cudaError_t e = cudaGetLastError();
+  // the next step's rebuild decision (an output step's last block made it)
+  if (e == cudaSuccess && !out) e = md_decide(c);
+  return e;
+}
+
+void md_swap_positions(b200_ctx *c) {
+  if (c->prec == B200_PREC_MIXED) std::swap(c->xq, c->xqb);
+  else std::swap(c->x4, c->x4b);
+  c->pos_parity ^= 1;
 }

@@ -473,6 +473,8 @@ class System:
         self._ck(self._L.b200_set_graphs(self._h, int(on)))
 
     def set_timing(self, on=True):
+        """True (1): phase events inside every step's pieces; 2: events around
+        whole pieces with the run's own step form kept."""
         self._ck(self._L.b200_set_timing(self._h, int(on)))
 
     def timing(self, reset=False):

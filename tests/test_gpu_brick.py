@@ -132,10 +132,14 @@ def test_bricks_match_oracle(style):
 
 
 @pytest.mark.parametrize("style", ["lj", "eam"])
-def test_one_brick_matches_graph_run(style):
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_one_brick_matches_graph_run(style, precision):
     """The per-call path of one brick and b200_run's step graphs take the same
-    rounded steps: same trajectory, same thermo."""
-    make, x, v, steps = (_lj if style == "lj" else _eam)("fp64")
+    rounded steps: same trajectory, same thermo.  For lj/cut b200_run steps
+    through the one-launch step kernel (forces and both half-steps, with the
+    position buffers alternating), the per-call path through separate
+    pair and half-step kernels."""
+    make, x, v, steps = (_lj if style == "lj" else _eam)(precision)
     b1, rows1, ref = _brick((make, x, v, steps), (1, 1, 1))
     s = make()
     s.set_atoms(x, None, v)

@@ -136,3 +136,25 @@ def test_eager_launches_match_graph_replay():
         for col in ("Temp", "E_pair", "Press"):
             assert x[col] == y[col]
     assert a.neigh_stats()["ncalls"] == b.neigh_stats()["ncalls"]
+
+
+def test_piece_timing_keeps_the_step_form():
+    """Timing mode 2 brackets whole pieces with stream events and keeps the
+    run's own step form (the one-launch lj/cut step): the thermo equals an
+    untimed run's, every step is timed, and the force pieces carry the time."""
+    case = LOGS["potentials_lj"]
+    a = device_case(case, "fp64")
+    b = device_case(case, "fp64")
+    b.set_timing(2)
+    ra = [a.setup()] + a.run(case["run"])
+    rb = [b.setup()] + b.run(case["run"])
+    for x, y in zip(ra, rb):
+        for col in ("Temp", "E_pair", "Press"):
+            assert x[col] == y[col]
+    ph = b.timing()
+    assert ph["steps"] == case["run"]
+    assert ph["pair1"] > 0 and ph["neigh"] > 0 and ph["initial"] > 0
+    assert ph["pair2"] == 0 and ph["final"] == 0
+    ms = b.step_times()
+    assert len(ms) == case["run"]
+    assert abs(sum(ms) - (ph["initial"] + ph["neigh"] + ph["pair1"])) <= 1e-6 * sum(ms)
