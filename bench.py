@@ -269,7 +269,7 @@ def load_traffic():
         return {}
 
 
-STEP_BYTES_PER_ATOM = 120.0  # one-launch LJ step: x, v read and written, f written (FP64)
+STEP_BYTES_PER_ATOM = 96.0  # one-launch LJ step: x and v read and written (FP64)
 EAM_BYTES_PER_ATOM_STEP = 200.0   # x, v, f, rho, fp traffic of one EAM step (FP64 state)
 EAM_HALF_PAIRS = 21.0             # half pairs inside 4.95 A per atom on the fcc lattice
 EAM_FLOP_PER_ATOM_STEP = 80.0 * EAM_HALF_PAIRS + 15.0
@@ -1091,9 +1091,9 @@ def main():
     peak, peak_kind = load_peaks()
     # the dominant kernel is the one-launch step k_lj_step (forces, this
     # step's final and the next initial half-step); its algorithmic bytes per
-    # atom, FP64 state: x read and written (48 B), v read and written (48 B),
-    # f written (24 B).  Its time is the step piece's (with the one-thread
-    # k_decide after it), from events around the piece.
+    # atom, FP64 state: x read and written (48 B), v read and written (48 B);
+    # the forces stay in registers.  Its time is the step piece's (with the
+    # one-thread k_decide after it), from events around the piece.
     achieved = STEP_BYTES_PER_ATOM * n4 / (pieces["pair1"] * 1e-3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": load_traffic().get("lj4m_mixed_step"),

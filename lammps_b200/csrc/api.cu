@@ -620,6 +620,7 @@ cudaError_t launch_piece(b200_ctx *c, int kind, double dtv, double dtf, cudaEven
       // swaps the position buffers after it)
       return md_lj_step(c, dtv, dtf, out);
     }
+    if (fused && md_eam_step_ok(c)) return md_eam_step(c, dtv, dtf, out);  // the same for eam
     if (ev) e = record(c, ev[0]);
     if (kind == PIECE_FUSED && c->rep_onelaunch && c->nrep && c->pstyle == B200_PAIR_LJ_CUT) {
       // replicas: this step's forces, final half-step and the next step's
@@ -787,7 +788,7 @@ int wait_decision(b200_ctx *c, bool *rebuild) {
 // fused piece that ran md_lj_step leaves the new positions in the other
 // buffer, which becomes current.
 int run_piece(b200_ctx *c, int kind, double dtv, double dtf, cudaEvent_t *ev) {
-  const bool swap = (kind == PIECE_FUSED || kind == PIECE_FUSED_OUT) && md_lj_step_ok(c);
+  const bool swap = (kind == PIECE_FUSED || kind == PIECE_FUSED_OUT) && md_step_ok(c);
   if (!c->use_graphs) {
     CK(launch_piece(c, kind, dtv, dtf, ev));
   } else {
@@ -807,7 +808,7 @@ int ensure_graphs(b200_ctx *c, double dtv, double dtf, double ftm2v) {
   if (c->graph_valid) return B200_OK;
   // with md_lj_step the position buffers alternate from step to step: every
   // piece is captured for both (the pointer swap is host state only)
-  const int sets = md_lj_step_ok(c) ? 2 : 1;
+  const int sets = md_step_ok(c) ? 2 : 1;
   for (int set = 0; set < sets; set++) {
     if (set) md_swap_positions(c);
     for (int kind = 0; kind < MD_NPIECES; kind++) {

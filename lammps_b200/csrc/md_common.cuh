@@ -391,3 +391,102 @@ __device__ __forceinline__ bool md_nve_fused_atom(int i, int stride, double dtv,
   return md_nve_step_atom<KE>(i, stride, dtv, dtf, mass, x4, x4, v, f[i], f[stride + i],
                               f[2 * stride + i], xq, box, xhold, triggersq, ke);
 }
+
+// ---- one-launch MD steps (k_lj_step, k_eam_force with STEP) ---------------
+// A force kernel that also advances the atoms: after its pair loop each
+// atom's first lane applies this step's final half-step and the next step's
+// initial half-step.  The neighbour gathers read the positions in `cur`; the
+// new positions go to `nxt`, a second buffer, so no update can reach a gather
+// of the same launch; the host swaps the two buffers after the launch.  Mixed
+// form: cur/nxt are the fixed-point coordinates and the FP64 positions x4
+// are updated in place (the mixed gathers never read them); FP64 form:
+// cur/nxt are the FP64 positions.
+struct StepArgs {
+  double dtv, dtf, triggersq;
+  const double *mass;
+  double4 *x4;      // mixed form: FP64 positions, updated in place
+  const void *cur;  // positions the gathers read: int4 (mixed) or double4
+  void *nxt;        // positions after the next initial half-step
+  double *v;
+  const double4 *xhold;
+  int *status, *dcount, *mail;
+  double *rows;
+  int rows_cap, every, delay, check;
+};
+
+// The atom's half-steps, by its first lane, with its summed force.  The
+// forces stay in registers on an ordinary step: within a run chunk nothing
+// reads them (a chunk's last step is the two-kernel form, which stores them
+// for the next chunk's first half-step and for downloads); an output step
+// stores them all the same.
+template <bool OUT, bool MIXED>
+__device__ __forceinline__ bool md_step_atom(const StepArgs &s, int i, int stride, double *f,
+                                             double fx, double fy, double fz,
+                                             const BoxGeom &box, double &ke) {
+  if (OUT) {
+    f[i] = fx;
+    f[stride + i] = fy;
+    f[2 * stride + i] = fz;
+  }
+  if (MIXED)
+    return md_nve_step_atom<OUT>(i, stride, s.dtv, s.dtf, s.mass, s.x4, s.x4, s.v, fx, fy, fz,
+                                 static_cast<int4 *>(s.nxt), box, s.xhold, s.triggersq, ke);
+  return md_nve_step_atom<OUT>(i, stride, s.dtv, s.dtf, s.mass,
+                               static_cast<const double4 *>(s.cur),
+                               static_cast<double4 *>(s.nxt), s.v, fx, fy, fz, nullptr, box,
+                               s.xhold, s.triggersq, ke);
+}
+
+// The end of a one-launch step (every thread of the block).  The
+// displacement flag goes to the status word.  On an output step the last
+// block to finish adds the energy and virial (ev[0..6]: written, or added to
+// what an earlier pass of the step left there) and the kinetic energy
+// (ev[7]) in block order, records the thermo row and makes the next step's
+// rebuild decision, as k_nve_fused does.  Other steps end with no
+// block-completion count: one returning atomic per block lengthens every
+// block's life (with that count on every step the 4M-atom LJ step ran at
+// 5,020 Matom-steps/s, without it at 5,723), so their decision is a
+// one-thread kernel launched after the step kernel.  red: 8 x (warps per
+// block) doubles of shared memory.
+template <bool OUT>
+__device__ __forceinline__ void md_step_tail(const StepArgs &s, bool moved, const double (&acc)[7],
+                                             double ke, double *red, double *partial,
+                                             unsigned int *counter, double *ev,
+                                             bool accumulate) {
+  if (s.xhold && __any_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0) {
+    atomicOr(&s.status[ST_MOVED], 1);
+    if (OUT) __threadfence();  // the flag is visible before this block counts itself done
+  }
+  if (!OUT) return;
+  __shared__ bool last;
+  double v8[8];
+#pragma unroll
+  for (int k = 0; k < 7; k++) v8[k] = acc[k];
+  v8[7] = ke;
+  block_sum<8>(v8, red);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < 8; k++) partial[(size_t)blockIdx.x * 8 + k] = v8[k];
+    __threadfence();
+    last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  // block partials added in a fixed order: reproducible run to run
+  double sum[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (unsigned int b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+#pragma unroll
+    for (int k = 0; k < 8; k++) sum[k] += __ldcg(&partial[(size_t)b * 8 + k]);
+  __syncthreads();
+  block_sum<8>(sum, red);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < 7; k++) ev[k] = accumulate ? ev[k] + sum[k] : sum[k];
+    ev[7] = sum[7];
+    md_record_row_dev(s.status, ev, s.rows, s.rows_cap);
+    md_decide_dev(s.status, s.every, s.delay, s.check, s.dcount, s.mail);
+    *counter = 0u;
+  }
+}

@@ -270,6 +270,11 @@ cudaError_t md_rep_step(b200_ctx *c, double dtv, double dtf);
 bool md_lj_step_ok(const b200_ctx *c);
 cudaError_t md_lj_step(b200_ctx *c, double dtv, double dtf, bool out);
 void md_swap_positions(b200_ctx *c);
+// the same for eam: the density pass, then the force pass with the half-steps
+bool md_eam_step_ok(const b200_ctx *c);
+cudaError_t md_eam_step(b200_ctx *c, double dtv, double dtf, bool out);
+// the context runs a one-launch step kernel in its fused pieces
+inline bool md_step_ok(const b200_ctx *c) { return md_lj_step_ok(c) || md_eam_step_ok(c); }
 // group plan of the one-launch step: cluster size cs, block size, groups
 int md_rep_plan(b200_ctx *c, int cs, int block, int tpa);
 // ---- integration (integrate.cu) --------------------------------------------

@@ -49,6 +49,7 @@ struct EamArgs {
   unsigned int *counter;
   double *ev;
   double *eatom, *vatom;
+  StepArgs step;  // k_eam_force with STEP: the half-steps after the forces
 };
 
 __device__ __forceinline__ void decode(unsigned int e, int &j, int &dx, int &dy, int &dz) {
@@ -217,12 +218,15 @@ __global__ void __launch_bounds__(128) k_eam_rho(EamArgs a, const double4 *__res
   if (EV) block_partials_finish<7>(acc, red, a.partial, a.counter, a.ev, false);
 }
 
-template <int TPA, bool EV, bool ATOM, bool MIXED, bool SINGLE>
+// STEP: a one-launch step (md_step_atom / md_step_tail): after the forces
+// each atom's first lane applies this step's final half-step and the next
+// step's initial half-step, writing the new positions to the other buffer.
+template <int TPA, bool EV, bool ATOM, bool MIXED, bool SINGLE, bool STEP = false>
 __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__restrict__ x4,
                                                    const int4 *__restrict__ xq) {
   __shared__ int s_t2rhor[TABSZ];
   __shared__ int s_t2z2r[TABSZ];
-  __shared__ double red[7 * 4];
+  __shared__ double red[8 * 4];
   const int nt2 = a.ntp1 * a.ntp1;
   for (int k = threadIdx.x; k < nt2; k += blockDim.x) {
     s_t2rhor[k] = a.t2rhor[k];
@@ -421,6 +425,15 @@ __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__r
   fx = lane_sum<TPA>(fx);
   fy = lane_sum<TPA>(fy);
   fz = lane_sum<TPA>(fz);
+  if (STEP) {
+    double ke = 0.0;
+    bool moved = false;
+    if (active && lane == 0)
+      moved = md_step_atom<EV, MIXED>(a.step, i, a.stride, a.f, fx, fy, fz, a.box, ke);
+    // ev[0..6] already hold the density pass's embedding energy: add to it
+    md_step_tail<EV>(a.step, moved, acc, ke, red, a.partial, a.counter, a.ev, true);
+    return;
+  }
   if (active && lane == 0) {
     a.f[i] = fx;
     a.f[a.stride + i] = fy;
@@ -457,7 +470,7 @@ void record_mid(b200_ctx *c, cudaEvent_t mid) {
 
 // stage: EAM_BOTH, or EAM_DENSITY (passes 1-2) / EAM_FORCE (pass 3) alone
 template <int TPA, bool EV, bool ATOM, bool SINGLE>
-void launch_t(b200_ctx *c, const EamArgs &a, cudaEvent_t mid, int stage) {
+void launch_t(b200_ctx *c, const EamArgs &a, cudaEvent_t mid, int stage, bool step = false) {
   const int B = 128;
   const int grid = md_blocks((long long)a.n * TPA, B);
   if (stage != EAM_FORCE) {
@@ -469,6 +482,17 @@ void launch_t(b200_ctx *c, const EamArgs &a, cudaEvent_t mid, int stage) {
   }
   record_mid(c, mid);
   if (stage != EAM_DENSITY) {
+    if constexpr (!ATOM) {
+      if (step) {
+        if (c->prec == B200_PREC_MIXED)
+          k_eam_force<TPA, EV, false, true, SINGLE, true><<<grid, B, 0, c->stream>>>(a, c->x4, c->xq);
+        else
+          k_eam_force<TPA, EV, false, false, SINGLE, true><<<grid, B, 0, c->stream>>>(a, c->x4,
+                                                                                      c->xq);
+        c->launches++;
+        return;
+      }
+    }
     if (c->prec == B200_PREC_MIXED)
       k_eam_force<TPA, EV, ATOM, true, SINGLE><<<grid, B, 0, c->stream>>>(a, c->x4, c->xq);
     else
@@ -542,8 +566,7 @@ cudaError_t md_eam_fp_halo(b200_ctx *c, int m, const int *idx, double *buf, bool
   return cudaGetLastError();
 }
 
-cudaError_t md_eam_compute(b200_ctx *c, bool ev, bool atom_ev, double *eatom, double *vatom,
-                           cudaEvent_t mid, int stage) {
+static EamArgs eam_args(b200_ctx *c, double *eatom, double *vatom) {
   EamArgs a;
   a.n = c->n;
   a.stride = c->stride;
@@ -580,6 +603,12 @@ cudaError_t md_eam_compute(b200_ctx *c, bool ev, bool atom_ev, double *eatom, do
   a.ev = c->ev;
   a.eatom = eatom;
   a.vatom = vatom;
+  return a;
+}
+
+cudaError_t md_eam_compute(b200_ctx *c, bool ev, bool atom_ev, double *eatom, double *vatom,
+                           cudaEvent_t mid, int stage) {
+  EamArgs a = eam_args(c, eatom, vatom);
   switch (c->tpa) {
     case 1: launch_tpa<1>(c, a, ev, atom_ev, mid, stage); break;
     case 2: launch_tpa<2>(c, a, ev, atom_ev, mid, stage); break;
@@ -589,4 +618,61 @@ cudaError_t md_eam_compute(b200_ctx *c, bool ev, bool atom_ev, double *eatom, do
     default: launch_tpa<32>(c, a, ev, atom_ev, mid, stage); break;
   }
   return cudaGetLastError();
+}
+
+// ---- one launch per EAM force pass and half-steps --------------------------
+
+namespace {
+template <int TPA>
+void launch_step_tpa(b200_ctx *c, const EamArgs &a, bool out) {
+  if (c->ntypes == 1) {
+    if (out) launch_t<TPA, true, false, true>(c, a, nullptr, EAM_BOTH, true);
+    else launch_t<TPA, false, false, true>(c, a, nullptr, EAM_BOTH, true);
+  } else {
+    if (out) launch_t<TPA, true, false, false>(c, a, nullptr, EAM_BOTH, true);
+    else launch_t<TPA, false, false, false>(c, a, nullptr, EAM_BOTH, true);
+  }
+}
+}  // namespace
+
+bool md_eam_step_ok(const b200_ctx *c) {
+  return c->pstyle == B200_PAIR_EAM && c->tpa >= 1 && c->tpa <= 8 && c->nrep == 0 &&
+         !c->ghosts_on;
+}
+
+cudaError_t md_eam_step(b200_ctx *c, double dtv, double dtf, bool out) {
+  EamArgs a = eam_args(c, nullptr, nullptr);
+  StepArgs &s = a.step;
+  s.dtv = dtv;
+  s.dtf = dtf;
+  s.triggersq = 0.25 * c->skin * c->skin;  // src/neighbor.cpp:239
+  s.mass = c->mass_dev;
+  s.x4 = c->x4;
+  if (c->prec == B200_PREC_MIXED) {
+    s.cur = c->xq;
+    s.nxt = c->xqb;
+  } else {
+    s.cur = c->x4;
+    s.nxt = c->x4b;
+  }
+  s.v = c->v;
+  s.xhold = c->check ? c->xhold : nullptr;
+  s.status = c->status;
+  s.dcount = c->dec_count;
+  s.mail = c->mail_dev;
+  s.rows = c->rows;
+  s.rows_cap = c->rows_cap;
+  s.every = c->every;
+  s.delay = c->delay;
+  s.check = c->check;
+  switch (c->tpa) {
+    case 1: launch_step_tpa<1>(c, a, out); break;
+    case 2: launch_step_tpa<2>(c, a, out); break;
+    case 4: launch_step_tpa<4>(c, a, out); break;
+    default: launch_step_tpa<8>(c, a, out); break;
+  }
+  cudaError_t e = cudaGetLastError();
+  // the next step's rebuild decision (an output step's last block made it)
+  if (e == cudaSuccess && !out) e = md_decide(c);
+  return e;
 }

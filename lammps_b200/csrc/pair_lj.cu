@@ -358,37 +358,13 @@ __global__ void __launch_bounds__(128) k_lj_mixed(PairArgs a, const int4 *__rest
 // pair forces (lj_atom_mixed / lj_atom_fp64, the same code and order as
 // k_lj_mixed / k_lj_fp64), then, by the atom's first lane, the final
 // half-step of this step, its kinetic-energy term on an output step and the
-// initial half-step of the next (md_nve_step_atom, the arithmetic of
-// k_nve_fused).  The neighbours' positions are gathered from `cur` while the
-// new positions go to `nxt`, a second buffer, so no update can reach a gather
-// of the same launch; the host swaps the two buffers after the launch.  Mixed
-// form: cur/nxt are the fixed-point coordinates and the FP64 positions are
-// updated in place (the mixed gathers never read them); FP64 form: cur/nxt
-// are the FP64 positions.  On an output step the last block to finish adds
-// the energy, virial and kinetic energy in block order, records the thermo row
-// and makes the next step's rebuild decision, as k_nve_fused does.  Other
-// steps end with no block-completion count: one returning atomic per block
-// lengthens every block's life (with that count on every step the 4M-atom LJ
-// step ran at 5,020 Matom-steps/s, without it at 5,723), so the decision is a
-// one-thread kernel after this one (md_lj_step).
-struct StepArgs {
-  double dtv, dtf, triggersq;
-  const double *mass;
-  double4 *x4;      // mixed form: FP64 positions, updated in place
-  const void *cur;  // positions the gathers read: int4 (mixed) or double4
-  void *nxt;        // positions after the next initial half-step
-  double *v;
-  const double4 *xhold;
-  int *status, *dcount, *mail;
-  double *rows;
-  int rows_cap, every, delay, check;
-};
-
+// initial half-step of the next (md_step_atom, the arithmetic of
+// k_nve_fused), with the position buffers and the step's end described at
+// StepArgs and md_step_tail.
 template <int TPA, bool OUT, bool SINGLE, bool MIXED>
 __global__ void __launch_bounds__(128) k_lj_step(PairArgs a, StepArgs s) {
   __shared__ double tab[6 * TABSZ];
   __shared__ double red[8 * 4];
-  __shared__ bool last;
   float *tabf = reinterpret_cast<float *>(tab);
   const int nt2 = a.ntp1 * a.ntp1;
   if (!SINGLE) {
@@ -415,54 +391,9 @@ __global__ void __launch_bounds__(128) k_lj_step(PairArgs a, StepArgs s) {
   fz = lane_sum<TPA>(fz);
   double ke = 0.0;
   bool moved = false;
-  if (active && lane == 0) {
-    a.f[i] = fx;
-    a.f[a.stride + i] = fy;
-    a.f[2 * a.stride + i] = fz;
-    if (MIXED)
-      moved = md_nve_step_atom<OUT>(i, a.stride, s.dtv, s.dtf, s.mass, s.x4, s.x4, s.v, fx, fy,
-                                    fz, static_cast<int4 *>(s.nxt), a.box, s.xhold, s.triggersq,
-                                    ke);
-    else
-      moved = md_nve_step_atom<OUT>(i, a.stride, s.dtv, s.dtf, s.mass,
-                                    static_cast<const double4 *>(s.cur),
-                                    static_cast<double4 *>(s.nxt), s.v, fx, fy, fz, nullptr,
-                                    a.box, s.xhold, s.triggersq, ke);
-  }
-  if (s.xhold && __any_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0) {
-    atomicOr(&s.status[ST_MOVED], 1);
-    if (OUT) __threadfence();  // the flag is visible before this block counts itself done
-  }
-  if (!OUT) return;
-  double v8[8];
-#pragma unroll
-  for (int k = 0; k < 7; k++) v8[k] = acc[k];
-  v8[7] = ke;
-  block_sum<8>(v8, red);
-  __syncthreads();
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int k = 0; k < 8; k++) a.partial[(size_t)blockIdx.x * 8 + k] = v8[k];
-    __threadfence();
-    last = atomicAdd(a.counter, 1u) == gridDim.x - 1;
-  }
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-  // block partials added in a fixed order: reproducible run to run
-  double sum[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  for (unsigned int b = threadIdx.x; b < gridDim.x; b += blockDim.x)
-#pragma unroll
-    for (int k = 0; k < 8; k++) sum[k] += __ldcg(&a.partial[(size_t)b * 8 + k]);
-  __syncthreads();
-  block_sum<8>(sum, red);
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int k = 0; k < 8; k++) a.ev[k] = sum[k];
-    md_record_row_dev(s.status, a.ev, s.rows, s.rows_cap);
-    md_decide_dev(s.status, s.every, s.delay, s.check, s.dcount, s.mail);
-    *a.counter = 0u;
-  }
+  if (active && lane == 0)
+    moved = md_step_atom<OUT, MIXED>(s, i, a.stride, a.f, fx, fy, fz, a.box, ke);
+  md_step_tail<OUT>(s, moved, acc, ke, red, a.partial, a.counter, a.ev, false);
 }
 
 // One MD step of every replica of a batched context in one launch.  Cluster g
