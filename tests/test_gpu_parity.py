@@ -11,6 +11,9 @@ import os
 import numpy as np
 import pytest
 
+import oracle
+from lammps_b200 import PairLJCut, System, inputs
+
 from gpu_cases import (device_case, device_from_snapshot, force_errors, half_sets,
                        oracle_snapshot, virial_errors)
 
@@ -158,3 +161,64 @@ def test_piece_timing_keeps_the_step_form():
     ms = b.step_times()
     assert len(ms) == case["run"]
     assert abs(sum(ms) - (ph["initial"] + ph["neigh"] + ph["pair1"])) <= 1e-6 * sum(ms)
+
+
+def _noncubic_oracle(steps, thermo):
+    """fcc 6 x 7 x 8 cells at rho* 0.8442: three different box edges (10.1,
+    11.8 and 13.4 sigma), Gaussian velocities at T* 1.44; the oracle run for
+    `steps` steps with thermo rows every `thermo`."""
+    a = inputs.lj_lattice_constant("fcc", 0.8442)
+    x = inputs.lattice("fcc", 6, 7, 8, a)
+    hi = np.array([6 * a, 7 * a, 8 * a])
+    v = inputs.velocity_create(x, np.ones(len(x), np.int32), np.array([0.0, 1.0]), 1.44, 4928,
+                               "lj", gaussian=True, loop="geom")
+    o = oracle.OracleSim("lj", threads=4)
+    o.box([0.0, 0.0, 0.0], hi)
+    o.atoms(x, v)
+    o.mass(1, 1.0)
+    o.lj_cut(2.5)
+    o.lj_coeff(1, 1, 1.0, 1.0, 2.5)
+    o.neighbor(0.3, 10, 0, False, 0)
+    o.thermo(thermo)
+    o.setup()
+    o.run(steps)
+    return o, x, v, hi
+
+
+def _noncubic_device(prec, hi):
+    s = System("lj", prec)
+    s.set_box([0.0, 0.0, 0.0], hi)
+    p = PairLJCut(2.5)
+    p.coeff(1, 1, 1.0, 1.0, 2.5)
+    s.set_pair(p)
+    s.set_mass([1.0])
+    s.set_neighbor(0.3, 10, 0, False)
+    return s
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("mixed", MIXED_TOL)])
+def test_noncubic_box_forces_and_run(prec, tol):
+    """Unequal box edges: the mixed form scales each fixed-point component by
+    its own unit (no common unit, the two-kernel step), the FP64 form takes
+    the one-launch step.  Forces after 10 oracle steps within the form's bar,
+    and a 30-step device run's thermo rows against the oracle's."""
+    o, x, v, hi = _noncubic_oracle(10, 0)
+    o.compute(1, 1)
+    dev = _noncubic_device(prec, hi)
+    dev.set_atoms(o.x, None, o.v)
+    dev.neigh_build()
+    dev.compute(1, 1)
+    rel, _ = force_errors(dev.download()["f"], o.f)
+    assert rel <= tol, rel
+    o2, _, _, _ = _noncubic_oracle(30, 10)
+    want = o2.thermo_rows()
+    dev = _noncubic_device(prec, hi)
+    dev.set_thermo(10)
+    dev.set_atoms(x, None, v)
+    rows = [dev.setup()] + dev.run(30)
+    assert len(rows) == len(want)
+    rtol = 1e-9 if prec == "fp64" else 1e-5
+    for got, ref in zip(rows, want):
+        assert got["Step"] == int(ref[0])
+        for key, col in (("Temp", 1), ("E_pair", 2), ("Press", 4)):
+            assert got[key] == pytest.approx(ref[col], rel=rtol, abs=rtol), (got["Step"], key)
