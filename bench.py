@@ -1099,6 +1099,9 @@ def main():
                 "frac": achieved / peak, "traffic": load_traffic().get("lj4m_mixed_step"),
                 "kernel": "k_lj_step", "kernel_ms": pieces["pair1"],
                 "alg_bytes_per_atom": STEP_BYTES_PER_ATOM,
+                # what bounds the kernel: the L1 data pipe of its neighbour
+                # gathers (ncu capture in profiles/k_lj_step_lj4m.md)
+                "l1tex_pct_of_peak": load_traffic().get("lj4m_mixed_step_l1tex_pct"),
                 "pair_kernel": {"kernel": "k_lj_mixed (phase-timed steps)",
                                 "ms": phases["pair1"],
                                 "achieved_gbs": 48.0 * n4 / (phases["pair1"] * 1e-3) / 1e9},

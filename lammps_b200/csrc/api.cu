@@ -918,6 +918,9 @@ int b200_create(int device, int precision, b200_ctx **out) {
   c->prec = precision;
   cudaError_t e = cudaSetDevice(device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->s_aux, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaMalloc((void **)&c->status, ST_COUNT * sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(c->status, 0, ST_COUNT * sizeof(int));
   if (e == cudaSuccess) e = cudaMallocHost((void **)&c->status_host, ST_COUNT * sizeof(int));
@@ -984,6 +987,9 @@ int b200_destroy(b200_ctx *c) {
   if (c->mail_host) cudaFreeHost(c->mail_host);
   if (c->bounce_host) cudaFreeHost(c->bounce_host);
   dfree(c->dec_count);
+  if (c->s_aux) cudaStreamDestroy(c->s_aux);
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return B200_OK;

@@ -51,6 +51,10 @@ struct b200_ctx {
   int device = 0;
   int prec = 0;
   cudaStream_t stream = nullptr;
+  // side stream of the rebuild: a replica batch's second builder launch runs
+  // beside the first (fork and join events)
+  cudaStream_t s_aux = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   std::string err;
   long long launches = 0;
 

@@ -753,27 +753,38 @@ cudaError_t md_rebuild(b200_ctx *c, const int *d_flag) {
     }
     const int cap = md_stage_cap(c);
     const int cap2 = md_stage_cap2(c);  // a batch's densest tiles, or 0
-    auto launch = [&](int stage_cap, int pass) {
+    auto launch = [&](int stage_cap, int pass, cudaStream_t st) {
       const size_t smem = neigh_smem(stage_cap);
 #define MD_NEIGH_ARGS                                                                         \
   n, c->stride, c->capacity, stage_cap, c->box, R, c->ntypes + 1, c->cutneighsq_dev, c->x4,  \
       c->cell_start, c->nlist, c->numneigh, c->status, d_flag, pass, cap
       if (c->ntypes == 1 && !c->nrep)
-        k_neigh_tiles<true, false><<<tiles, kNeighThreads, smem, c->stream>>>(MD_NEIGH_ARGS);
+        k_neigh_tiles<true, false><<<tiles, kNeighThreads, smem, st>>>(MD_NEIGH_ARGS);
       else if (c->ntypes == 1)
-        k_neigh_tiles<true, true><<<tiles, kNeighThreads, smem, c->stream>>>(MD_NEIGH_ARGS);
+        k_neigh_tiles<true, true><<<tiles, kNeighThreads, smem, st>>>(MD_NEIGH_ARGS);
       else if (!c->nrep)
-        k_neigh_tiles<false, false><<<tiles, kNeighThreads, smem, c->stream>>>(MD_NEIGH_ARGS);
+        k_neigh_tiles<false, false><<<tiles, kNeighThreads, smem, st>>>(MD_NEIGH_ARGS);
       else
-        k_neigh_tiles<false, true><<<tiles, kNeighThreads, smem, c->stream>>>(MD_NEIGH_ARGS);
+        k_neigh_tiles<false, true><<<tiles, kNeighThreads, smem, st>>>(MD_NEIGH_ARGS);
 #undef MD_NEIGH_ARGS
       c->launches++;
     };
     if (cap2 > 0) {
-      launch(cap, 1);
-      launch(cap2, 2);
+      // The two passes build disjoint tiles, so the second (the densest
+      // tiles, large staging, few blocks per SM) runs on the side stream
+      // beside the first instead of after it; the join makes the main stream
+      // wait for both.  Inside a graph capture the fork and join become
+      // graph dependencies.
+      cudaError_t e = cudaEventRecord(c->ev_fork, c->stream);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(c->s_aux, c->ev_fork, 0);
+      if (e != cudaSuccess) return e;
+      launch(cap, 1, c->stream);
+      launch(cap2, 2, c->s_aux);
+      e = cudaEventRecord(c->ev_join, c->s_aux);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, c->ev_join, 0);
+      if (e != cudaSuccess) return e;
     } else {
-      launch(cap, 0);
+      launch(cap, 0, c->stream);
     }
   }
   c->launches += 3;
