@@ -358,6 +358,7 @@ __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__r
        }
        // FP32 sum of the slab's pair forces, added to the FP64 accumulator
        float cfx = 0.f, cfy = 0.f, cfz = 0.f;
+       float ce[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // EV: the slab's FP32 sums
 #pragma unroll
        for (int u = 0; u < 4; u++) {
         const int4 xj = xs[u];
@@ -405,20 +406,25 @@ __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__r
           cfy += dely * fpair;
           cfz += delz * fpair;
           if (EV) {
-            acc[0] += 0.5 * (double)phi;
+            ce[0] = fmaf(0.5f, phi, ce[0]);
             const float hf = 0.5f * fpair;
-            acc[1] += (double)(delx * delx * hf);
-            acc[2] += (double)(dely * dely * hf);
-            acc[3] += (double)(delz * delz * hf);
-            acc[4] += (double)(delx * dely * hf);
-            acc[5] += (double)(delx * delz * hf);
-            acc[6] += (double)(dely * delz * hf);
+            ce[1] = fmaf(delx * delx, hf, ce[1]);
+            ce[2] = fmaf(dely * dely, hf, ce[2]);
+            ce[3] = fmaf(delz * delz, hf, ce[3]);
+            ce[4] = fmaf(delx * dely, hf, ce[4]);
+            ce[5] = fmaf(delx * delz, hf, ce[5]);
+            ce[6] = fmaf(dely * delz, hf, ce[6]);
           }
         }
        }
        fx += (double)cfx;
        fy += (double)cfy;
        fz += (double)cfz;
+       // the energy and virial terms join the FP64 sums once per slab, as the
+       // forces do
+       if (EV)
+#pragma unroll
+         for (int k = 0; k < 7; k++) acc[k] += (double)ce[k];
       }
     }
   }

@@ -251,6 +251,7 @@ __device__ __forceinline__ void lj_atom_mixed(const PairArgs &a, const int4 *__r
       for (int h = 0; h < 2; h++) {
         const int4 *xj = xall + 8 * h;
         float cfx = 0.f, cfy = 0.f, cfz = 0.f;
+        float ce[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // EV: this group's FP32 sums
 #pragma unroll
         for (int u = 0; u < 8; u++) {
           // x_i - x_j at the minimum image, in units (ISO) or lengths
@@ -281,20 +282,25 @@ __device__ __forceinline__ void lj_atom_mixed(const PairArgs &a, const int4 *__r
             const float c4 = SINGLE ? lj4 : tabf[4 * nt2 + tt];
             const float co = SINGLE ? off : tabf[5 * nt2 + tt];
             const float evdwl = in ? r6inv * (c3 * r6inv - c4) - co : 0.f;
-            acc[0] += 0.5 * (double)evdwl;
+            ce[0] = fmaf(0.5f, evdwl, ce[0]);
             // the virial wants separations in length units
             const float lx = ISO ? md_qlen(delx, qx, qxl) : delx,
                         ly = ISO ? md_qlen(dely, qx, qxl) : dely,
                         lz = ISO ? md_qlen(delz, qx, qxl) : delz;
             const float hf = 0.5f * fpair;
-            acc[1] += (double)(lx * lx * hf);
-            acc[2] += (double)(ly * ly * hf);
-            acc[3] += (double)(lz * lz * hf);
-            acc[4] += (double)(lx * ly * hf);
-            acc[5] += (double)(lx * lz * hf);
-            acc[6] += (double)(ly * lz * hf);
+            ce[1] = fmaf(lx * lx, hf, ce[1]);
+            ce[2] = fmaf(ly * ly, hf, ce[2]);
+            ce[3] = fmaf(lz * lz, hf, ce[3]);
+            ce[4] = fmaf(lx * ly, hf, ce[4]);
+            ce[5] = fmaf(lx * lz, hf, ce[5]);
+            ce[6] = fmaf(ly * lz, hf, ce[6]);
           }
         }
+        // the energy and virial terms join the FP64 sums once per group, as
+        // the forces do
+        if (EV)
+#pragma unroll
+          for (int k = 0; k < 7; k++) acc[k] += (double)ce[k];
         if (ISO) {
           fx = fma((double)cfx, qd, fx);
           fy = fma((double)cfy, qd, fy);
