@@ -1157,6 +1157,23 @@ def main():
             scu.close()
         cu["mixed_over_fp64"] = cu["mixed"] / cu["fp64"]
         extras["eam_cu_u3_32k"] = cu
+        # the plain LJ configuration of 32,000 atoms (fcc 20^3, Gaussian
+        # velocities, every 20 check no), the workload of the lj_32k CPU rows
+        from lammps_b200 import inputs as _inputs
+        a32 = _inputs.lj_lattice_constant("fcc", 0.8442)
+        x32 = _inputs.lattice("fcc", 20, 20, 20, a32)
+        v32 = _inputs.velocity_create(x32, np.ones(len(x32), np.int32), np.array([0.0, 1.0]),
+                                      1.44, 87287, "lj", gaussian=True, loop="geom")
+        lj32 = {"atoms": len(x32), "note": "fcc 20^3 rho* 0.8442, T* 1.44 Gaussian (seed 87287, "
+                "loop geom), rc 2.5, skin 0.3, every 20 check no; one bench step = the first 100 "
+                "NVE steps from the seeded state"}
+        for prec in ("mixed", "fp64"):
+            s32 = make_lj(prec, x32, v32, np.array([20 * a32] * 3))
+            t, _ = time_form(s32, torch, flush, K, W, (x32, v32))
+            lj32[prec] = s32.n * MD_STEPS * K / (t * 1e3)
+            s32.close()
+        lj32["mixed_over_fp64"] = lj32["mixed"] / lj32["fp64"]
+        extras["lj_32k"] = lj32
         # the EAM workload at 4M atoms: the density and force kernels at a
         # size where they are not launch- and latency-bound
         xe, ve, hie = eam4m_inputs()
