@@ -754,6 +754,13 @@ def profile_case(args):
     elif work == "lj4m":
         x, v, hi = lj4m_inputs()
         s = make_lj(prec, x, v, hi)
+    elif work == "lj32k":
+        from lammps_b200 import inputs
+        a = inputs.lj_lattice_constant("fcc", 0.8442)
+        x = inputs.lattice("fcc", 20, 20, 20, a)
+        v = inputs.velocity_create(x, np.ones(len(x), np.int32), np.array([0.0, 1.0]), 1.44,
+                                   87287, "lj", gaussian=True, loop="geom")
+        s = make_lj(prec, x, v, np.array([20 * a] * 3))
     elif work == "eam4m":
         tmp = tempfile.mkdtemp(prefix="b200prof_")
         from lammps_b200.eam_synth import write_setfl
@@ -1024,7 +1031,7 @@ def main():
     ap.add_argument("--tpa", type=int, default=0,
                     help="with --case: threads per atom of the pair kernels (0 = autotuned)")
     ap.add_argument("--case", default=None,
-                    help="profile one form only: eam32k-mixed, eam32k-fp64, lj4m-mixed, lj4m-fp64, "
+                    help="profile one form only: eam32k-mixed, eam32k-fp64, lj4m-mixed, lj4m-fp64, lj32k-mixed, lj32k-fp64, "
                          "eam4m-mixed, eam4m-fp64, c3-mixed, c3-fp64 (256 replicas)")
     args = ap.parse_args()
     if args.case:
