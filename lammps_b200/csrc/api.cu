@@ -514,7 +514,75 @@ int rebuild_sync(b200_ctx *c) {
   return set_err(c, B200_ERR_NEIGH_OVERFLOW, "Neighbor list overflow, boost neigh_modify one");
 }
 
+// Launch-shape search of a box that steps through the one-launch step kernel
+// (md_lj_step / md_eam_step): the step kernel itself is timed, for 1, 2, 4
+// and 8 threads per atom, since its best shape can differ from the two-kernel
+// pair pass's (at 32,000 LJ atoms, mixed: 2 and 4 tie for the pair pass, 4 is
+// 6 % faster for the step).  The steps run with a zero timestep, so
+// positions and velocities do not change; the status words, the decision
+// count and the mailbox that the steps advance are put back afterwards.
+int autotune_step(b200_ctx *c) {
+  int status_save[ST_COUNT], dcount_save = 0;
+  int rc0 = small_read(c, status_save, c->status, sizeof(status_save));
+  if (!rc0) rc0 = small_read(c, &dcount_save, c->dec_count, sizeof(int));
+  if (rc0) return rc0;
+  const int mail_save[2] = {c->mail_host[0], c->mail_host[1]};
+  const bool lj = c->pstyle == B200_PAIR_LJ_CUT;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  const int cand[4] = {1, 2, 4, 8};
+  float tmin[4] = {1e30f, 1e30f, 1e30f, 1e30f};
+  auto step = [&]() -> cudaError_t {
+    cudaError_t e = lj ? md_lj_step(c, 0.0, 0.0, false) : md_eam_step(c, 0.0, 0.0, false);
+    md_swap_positions(c);
+    return e;
+  };
+  int rc = B200_OK;
+  for (int round = 0; round < 3 && !rc; round++)
+    for (int k = 0; k < 4 && !rc; k++) {
+      c->tpa = cand[k];
+      cudaError_t e = step();
+      if (e == cudaSuccess) e = cudaEventRecord(e0, c->stream);
+      for (int r = 0; r < 5 && e == cudaSuccess; r++) e = step();
+      if (e == cudaSuccess) e = cudaEventRecord(e1, c->stream);
+      if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+      float ms = 0.f;
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+      if (e != cudaSuccess) rc = set_err(c, B200_ERR_CUDA, "launch-shape search: %s",
+                                         cudaGetErrorString(e));
+      else if (ms < tmin[k]) tmin[k] = ms;
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (c->pos_parity) md_swap_positions(c);  // 3 x 4 x 6 swaps: back to the first buffer
+  CK(cudaMemcpyAsync(c->status, status_save, sizeof(status_save), cudaMemcpyHostToDevice,
+                     c->stream));
+  CK(cudaMemcpyAsync(c->dec_count, &dcount_save, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->mail_host[0] = mail_save[0];
+  c->mail_host[1] = mail_save[1];
+  if (rc) return rc;
+  float best = 1e30f;
+  int best_tpa = 1;
+  for (int k = 0; k < 4; k++)
+    if (tmin[k] < best * 0.97f) {
+      best = tmin[k];
+      best_tpa = cand[k];
+    }
+  c->tpa = best_tpa;
+  c->tuned = true;
+  return B200_OK;
+}
+
 int autotune(b200_ctx *c) {
+  // a single box of lj/cut (equal edges in the mixed form) or eam steps
+  // through the one-launch step kernel: time that
+  const bool step_form =
+      c->nrep == 0 && !c->ghosts_on &&
+      ((c->pstyle == B200_PAIR_LJ_CUT && (c->prec != B200_PREC_MIXED || md_q_iso(c))) ||
+       c->pstyle == B200_PAIR_EAM);
+  if (step_form) return autotune_step(c);
   // Launch-shape search: time the force pass for each threads-per-atom
   // value and keep the fastest (ties to fewer threads per atom).  Each
   // candidate is timed in three rounds of five passes, the rounds
