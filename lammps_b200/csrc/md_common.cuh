@@ -204,6 +204,85 @@ __device__ __forceinline__ double dsq3(double a, double b, double c) {
   return __dadd_rn(__dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b)), __dmul_rn(c, c));
 }
 
+// The entries that one lane of an atom takes from the atom's list, G at a
+// time, with the next G already loading (streaming loads).  The list holds
+// each atom's entries in slabs of four: slab c of atom i is int4 number
+// c * stride + i.  Several lanes per atom (TPA > 1): the atom's lanes take
+// consecutive entries (lane s: entries s, s + TPA, s + 2 TPA, ...), so that
+// at each gather the lanes of one atom read neighbours that sit next to each
+// other in the cell-sorted order and share cache lines.  The lane's G
+// offsets from its row pointer are fixed, and the pointer advances by
+// TPA * G / 4 slab rows per step.  Entries past the atom's last slab read as
+// `pad`.  (One lane per atom reads whole slabs and does not use this.)
+template <int TPA, int G>
+struct ListWalk {
+  static_assert(TPA > 1 && (TPA * G) % 4 == 0, "whole slab rows per step");
+  const int *p;       // row pointer of the current step
+  long long off[G];   // offsets (in ints) of the lane's G entries from p
+  long long adv;      // ints between steps
+  int e0, ne;         // first entry of the current step; 4 x the slab count
+  unsigned pad;
+  unsigned cur[G], nxt[G];
+  __device__ __forceinline__ ListWalk(const int *nl, int stride, int i, int nslab, int lane,
+                                      unsigned pad_)
+      : p(nl + (size_t)i * 4), adv((long long)(TPA * G / 4) * stride * 4), e0(lane),
+        ne(nslab * 4), pad(pad_) {
+#pragma unroll
+    for (int u = 0; u < G; u++) {
+      const int e = lane + TPA * u;
+      off[u] = (long long)(e >> 2) * stride * 4 + (e & 3);
+    }
+    load(cur, p, e0);
+  }
+  __device__ __forceinline__ void load(unsigned (&v)[G], const int *q, int first) const {
+#pragma unroll
+    for (int u = 0; u < G; u++)
+      v[u] = first + TPA * u < ne ? (unsigned)__ldcs(q + off[u]) : pad;
+  }
+  __device__ __forceinline__ bool more() const { return e0 < ne; }
+  // start loading the next step's entries; cur holds this step's
+  __device__ __forceinline__ void prefetch() { load(nxt, p + adv, e0 + TPA * G); }
+  // how many of this step's entries lie before `num` (the rest are pads)
+  __device__ __forceinline__ int valid(int num) const {
+    return e0 >= num ? 0 : min(G, (num - e0 + TPA - 1) / TPA);
+  }
+  __device__ __forceinline__ void advance() {
+#pragma unroll
+    for (int u = 0; u < G; u++) cur[u] = nxt[u];
+    p += adv;
+    e0 += TPA * G;
+  }
+};
+
+// Calls f(ee, m) for each group of four entries that this lane takes from
+// atom i's list: ee the entries, m how many of them lie before the atom's
+// count num (the rest are pads).  One lane per atom: the slabs in order, the
+// next slab loading (streaming) while this one is used.  Several lanes per
+// atom: ListWalk's consecutive entries.
+template <int TPA, class F>
+__device__ __forceinline__ void walk_list(const int *nl, int stride, int i, int num, int lane,
+                                          F &&f) {
+  const int nslab = (num + 3) >> 2;
+  if constexpr (TPA == 1) {
+    const int4 *nl4 = reinterpret_cast<const int4 *>(nl);
+    int4 en = make_int4(0, 0, 0, 0);
+    if (nslab > 0) en = __ldcs(&nl4[i]);
+    for (int c4 = 0; c4 < nslab; c4++) {
+      const int4 e4 = en;
+      if (c4 + 1 < nslab) en = __ldcs(&nl4[(size_t)(c4 + 1) * stride + i]);
+      const unsigned ee[4] = {(unsigned)e4.x, (unsigned)e4.y, (unsigned)e4.z, (unsigned)e4.w};
+      f(ee, min(4, num - 4 * c4));
+    }
+  } else {
+    ListWalk<TPA, 4> w(nl, stride, i, nslab, lane, (unsigned)md_pad_entry(i));
+    while (w.more()) {
+      w.prefetch();
+      f(w.cur, w.valid(num));
+      w.advance();
+    }
+  }
+}
+
 template <int TPA>
 __device__ __forceinline__ double lane_sum(double v) {
 #pragma unroll

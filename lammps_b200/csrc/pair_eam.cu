@@ -118,16 +118,9 @@ __global__ void __launch_bounds__(128) k_eam_rho(EamArgs a, const double4 *__res
       // one element: the density spline row of every pair
       const double *rrow =
           SINGLE ? a.rhor + (size_t)s_t2rhor[a.ntp1 + 1] * (a.nr + 1) * 8 : nullptr;
-      const int4 *nl4 = reinterpret_cast<const int4 *>(a.nlist);
-      const int nslab = (num + 3) >> 2;
-      int4 en = make_int4(0, 0, 0, 0);
-      if (lane < nslab) en = __ldcs(&nl4[(size_t)lane * a.stride + i]);
-      for (int c4 = lane; c4 < nslab; c4 += TPA) {
-        const int4 e4 = en;
-        if (c4 + TPA < nslab) en = __ldcs(&nl4[(size_t)(c4 + TPA) * a.stride + i]);
-        const int mm = min(4, num - 4 * c4);
-        const unsigned int ee[4] = {(unsigned int)e4.x, (unsigned int)e4.y, (unsigned int)e4.z,
-                                    (unsigned int)e4.w};
+      // four entries ee of this lane (walk_list); the first mm lie before the
+      // atom's count
+      auto four = [&](const unsigned (&ee)[4], int mm) {
         double4 xq[4];
 #pragma unroll
         for (int u = 0; u < 4; u++) xq[u] = x4[u < mm ? md_entry_j(ee[u]) : i];
@@ -154,7 +147,8 @@ __global__ void __launch_bounds__(128) k_eam_rho(EamArgs a, const double4 *__res
             rho += ((v01.x * p + v01.y) * p + v23.x) * p + v23.y;
           }
         }
-      }
+      };
+      walk_list<TPA>(a.nlist, a.stride, i, num, lane, four);
     } else {
       const int4 xi = xq[i];
       ti = xi.w;
@@ -164,17 +158,10 @@ __global__ void __launch_bounds__(128) k_eam_rho(EamArgs a, const double4 *__res
       // one element: the density spline row of every pair
       const float *rrow =
           SINGLE ? a.rhor_f + (size_t)s_t2rhor[a.ntp1 + 1] * (a.nr + 1) * 8 : nullptr;
-      const int4 *nl4 = reinterpret_cast<const int4 *>(a.nlist);
-      const int nslab = (num + 3) >> 2;
-      int4 en = make_int4(0, 0, 0, 0);
-      if (lane < nslab) en = __ldcs(&nl4[(size_t)lane * a.stride + i]);
-      for (int c4 = lane; c4 < nslab; c4 += TPA) {
-        const int4 e4 = en;
-        if (c4 + TPA < nslab) en = __ldcs(&nl4[(size_t)(c4 + TPA) * a.stride + i]);
+      // four entries ee of this lane (walk_list)
+      auto four = [&](const unsigned (&ee)[4], int) {
         // whole slabs: pad entries in the last slab name the atom itself
         // (zero separation), which the r^2 > 0 test rejects
-        const unsigned int ee[4] = {(unsigned int)e4.x, (unsigned int)e4.y, (unsigned int)e4.z,
-                                    (unsigned int)e4.w};
         int4 xs[4];
 #pragma unroll
         for (int u = 0; u < 4; u++) xs[u] = xq[md_entry_j(ee[u])];
@@ -199,7 +186,8 @@ __global__ void __launch_bounds__(128) k_eam_rho(EamArgs a, const double4 *__res
           }
         }
         rho += (double)crho;
-      }
+      };
+      walk_list<TPA>(a.nlist, a.stride, i, num, lane, four);
     }
   }
   rho = lane_sum<TPA>(rho);
@@ -253,16 +241,9 @@ __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__r
       const double *rrow1 =
           SINGLE ? a.rhor + (size_t)s_t2rhor[a.ntp1 + 1] * (a.nr + 1) * 8 : nullptr;
       const double *zrow1 = SINGLE ? a.z2r + (size_t)s_t2z2r[a.ntp1 + 1] * (a.nr + 1) * 8 : nullptr;
-      const int4 *nl4 = reinterpret_cast<const int4 *>(a.nlist);
-      const int nslab = (num + 3) >> 2;
-      int4 en = make_int4(0, 0, 0, 0);
-      if (lane < nslab) en = __ldcs(&nl4[(size_t)lane * a.stride + i]);
-      for (int c4 = lane; c4 < nslab; c4 += TPA) {
-       const int4 e4 = en;
-       if (c4 + TPA < nslab) en = __ldcs(&nl4[(size_t)(c4 + TPA) * a.stride + i]);
-       const int mm = min(4, num - 4 * c4);
-       const unsigned int ee[4] = {(unsigned int)e4.x, (unsigned int)e4.y, (unsigned int)e4.z,
-                                   (unsigned int)e4.w};
+      // four entries ee of this lane (walk_list); the first mm lie before the
+      // atom's count
+      auto four = [&](const unsigned (&ee)[4], int mm) {
        double4 xq[4];
        double fpq[4];
 #pragma unroll
@@ -326,7 +307,8 @@ __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__r
           }
         }
        }
-      }
+      };
+      walk_list<TPA>(a.nlist, a.stride, i, num, lane, four);
     } else {
       const int4 xi = xq[i];
       const int ti = xi.w;
@@ -337,17 +319,10 @@ __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__r
       // one element: the density-derivative and pair spline rows of every pair
       const float *drow1 = SINGLE ? a.fz_f + 4 : nullptr;
       const float *zrow1 = SINGLE ? a.fz_f : nullptr;
-      const int4 *nl4 = reinterpret_cast<const int4 *>(a.nlist);
-      const int nslab = (num + 3) >> 2;
-      int4 en = make_int4(0, 0, 0, 0);
-      if (lane < nslab) en = __ldcs(&nl4[(size_t)lane * a.stride + i]);
-      for (int c4 = lane; c4 < nslab; c4 += TPA) {
-       const int4 e4 = en;
-       if (c4 + TPA < nslab) en = __ldcs(&nl4[(size_t)(c4 + TPA) * a.stride + i]);
+      // four entries ee of this lane (walk_list)
+      auto four = [&](const unsigned (&ee)[4], int) {
        // whole slabs: pad entries in the last slab name the atom itself
        // (zero separation), which the r^2 > 0 test rejects
-       const unsigned int ee[4] = {(unsigned int)e4.x, (unsigned int)e4.y, (unsigned int)e4.z,
-                                   (unsigned int)e4.w};
        int4 xs[4];
        float fpq[4];
 #pragma unroll
@@ -425,7 +400,8 @@ __global__ void __launch_bounds__(128) k_eam_force(EamArgs a, const double4 *__r
        if (EV)
 #pragma unroll
          for (int k = 0; k < 7; k++) acc[k] += (double)ce[k];
-      }
+      };
+      walk_list<TPA>(a.nlist, a.stride, i, num, lane, four);
     }
   }
   fx = lane_sum<TPA>(fx);

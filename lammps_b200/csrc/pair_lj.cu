@@ -114,15 +114,8 @@ __device__ __forceinline__ void lj_atom_fp64(const PairArgs &a, const double4 *_
     const int nslab = (num + 3) >> 2;
     auto slabs = [&](auto wrap_tag) {
     constexpr bool WRAP = decltype(wrap_tag)::value;
-    // the next slab's entries load (streaming) while this slab is used
-    int4 en = make_int4(0, 0, 0, 0);
-    if (lane < nslab) en = __ldcs(&nl4[(size_t)lane * a.stride + i]);
-    for (int c4 = lane; c4 < nslab; c4 += TPA) {
-      const int4 e4 = en;
-      if (c4 + TPA < nslab) en = __ldcs(&nl4[(size_t)(c4 + TPA) * a.stride + i]);
-      const int m = min(4, num - 4 * c4);
-      const unsigned int ee[4] = {(unsigned int)e4.x, (unsigned int)e4.y, (unsigned int)e4.z,
-                                  (unsigned int)e4.w};
+    // four entries ee, of which the first m lie before the atom's count
+    auto four = [&](const unsigned (&ee)[4], int m) {
       double4 xj[4];
 #pragma unroll
       for (int u = 0; u < 4; u++) xj[u] = x4[u < m ? md_entry_j(ee[u]) : i];
@@ -170,6 +163,26 @@ __device__ __forceinline__ void lj_atom_fp64(const PairArgs &a, const double4 *_
           }
         }
       }
+    };
+    if constexpr (TPA == 1) {
+      // the next slab's entries load (streaming) while this slab is used
+      int4 en = make_int4(0, 0, 0, 0);
+      if (nslab > 0) en = __ldcs(&nl4[i]);
+      for (int c4 = 0; c4 < nslab; c4++) {
+        const int4 e4 = en;
+        if (c4 + 1 < nslab) en = __ldcs(&nl4[(size_t)(c4 + 1) * a.stride + i]);
+        const unsigned int ee[4] = {(unsigned int)e4.x, (unsigned int)e4.y, (unsigned int)e4.z,
+                                    (unsigned int)e4.w};
+        four(ee, min(4, num - 4 * c4));
+      }
+    } else {
+      // the atom's lanes take consecutive entries (ListWalk)
+      ListWalk<TPA, 4> w(a.nlist, a.stride, i, nslab, lane, (unsigned)md_pad_entry(i));
+      while (w.more()) {
+        w.prefetch();
+        four(w.cur, w.valid(num));
+        w.advance();
+      }
     }
     };
     if (interior) slabs(std::false_type{});
@@ -192,52 +205,121 @@ __device__ __forceinline__ void lj_atom_fp64(const PairArgs &a, const double4 *_
 // bias every pair term the same way.
 // A pad entry names the atom itself (zero separation), which the r^2 > 0
 // test rejects.
+// One thread per atom (TPA 1): the thread walks its list four slabs (16
+// entries) at a time.  Several threads per atom: the atom's lanes take
+// consecutive entries (lane s: entries s, s + TPA, s + 2 TPA, ...), so that
+// at each gather the lanes of one atom read neighbours that sit next to each
+// other in the cell-sorted order and share cache lines; each lane then loads
+// one 4-byte entry per gather instead of a 16-byte slab per four.
 template <int TPA, bool EV, bool SINGLE, bool BATCH, bool ISO>
 __device__ __forceinline__ void lj_atom_mixed(const PairArgs &a, const int4 *__restrict__ xq,
                                               const float *tabf, int nt2, int i, int lane,
                                               bool active, double &fx, double &fy, double &fz,
                                               double (&acc)[7]) {
-  if (active) {
-    const BoxGeom &box = BATCH ? a.reps.box[a.reps.rep_of_atom[i]] : a.box;
-    const float qx = box.qs[0], qy = box.qs[1], qz = box.qs[2];
-    const float qxl = box.qs_lo[0], qyl = box.qs_lo[1], qzl = box.qs_lo[2];
-    // ISO: 1/r^2 in units times (q2h + q2l) is 1/r^2 in length units, and a
-    // force sum in units times qd (exact) is the force
-    const float q2h = box.q2inv, q2l = box.q2inv_lo;
-    const double qd = box.prd[0] * (1.0 / 4294967296.0);
-    float cutsq1 = 0, lj1 = 0, lj2 = 0, lj3 = 0, lj4 = 0, off = 0;
-    if (SINGLE) {
-      const int k11 = a.ntp1 + 1;
-      const double cs = __ldg(&a.tables[TAB_CUTSQ * TABSZ + k11]);
-      cutsq1 = ISO ? (float)(cs / (qd * qd)) : (float)cs;
-      lj1 = (float)__ldg(&a.tables[TAB_LJ1 * TABSZ + k11]);
-      lj2 = (float)__ldg(&a.tables[TAB_LJ2 * TABSZ + k11]);
-      lj3 = (float)__ldg(&a.tables[TAB_LJ3 * TABSZ + k11]);
-      lj4 = (float)__ldg(&a.tables[TAB_LJ4 * TABSZ + k11]);
-      off = (float)__ldg(&a.tables[TAB_OFFSET * TABSZ + k11]);
+  if (!active) return;
+  const BoxGeom &box = BATCH ? a.reps.box[a.reps.rep_of_atom[i]] : a.box;
+  const float qx = box.qs[0], qy = box.qs[1], qz = box.qs[2];
+  const float qxl = box.qs_lo[0], qyl = box.qs_lo[1], qzl = box.qs_lo[2];
+  // ISO: 1/r^2 in units times (q2h + q2l) is 1/r^2 in length units, and a
+  // force sum in units times qd (exact) is the force
+  const float q2h = box.q2inv, q2l = box.q2inv_lo;
+  const double qd = box.prd[0] * (1.0 / 4294967296.0);
+  float cutsq1 = 0, lj1 = 0, lj2 = 0, lj3 = 0, lj4 = 0, off = 0;
+  if (SINGLE) {
+    const int k11 = a.ntp1 + 1;
+    const double cs = __ldg(&a.tables[TAB_CUTSQ * TABSZ + k11]);
+    cutsq1 = ISO ? (float)(cs / (qd * qd)) : (float)cs;
+    lj1 = (float)__ldg(&a.tables[TAB_LJ1 * TABSZ + k11]);
+    lj2 = (float)__ldg(&a.tables[TAB_LJ2 * TABSZ + k11]);
+    lj3 = (float)__ldg(&a.tables[TAB_LJ3 * TABSZ + k11]);
+    lj4 = (float)__ldg(&a.tables[TAB_LJ4 * TABSZ + k11]);
+    off = (float)__ldg(&a.tables[TAB_OFFSET * TABSZ + k11]);
+  }
+  const int4 xi = xq[i];
+  const int ti = xi.w;
+  const int nslab = (a.numneigh[i] + 3) >> 2;
+  const int pe = md_pad_entry(i);
+  // The pair forces of N gathered neighbours, summed in FP32; the group sum
+  // (and, with EV, the group's energy and virial sums) joins the atom's FP64
+  // accumulators.
+  auto group = [&](const int4 *xj, auto n_c) {
+    constexpr int N = decltype(n_c)::value;
+    float cfx = 0.f, cfy = 0.f, cfz = 0.f;
+    float ce[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // EV: this group's FP32 sums
+#pragma unroll
+    for (int u = 0; u < N; u++) {
+      // x_i - x_j at the minimum image, in units (ISO) or lengths
+      float delx = md_qdiff(xi.x, xj[u].x);
+      float dely = md_qdiff(xi.y, xj[u].y);
+      float delz = md_qdiff(xi.z, xj[u].z);
+      if (!ISO) {
+        delx = md_qlen(delx, qx, qxl);
+        dely = md_qlen(dely, qy, qyl);
+        delz = md_qlen(delz, qz, qzl);
+      }
+      const float rsq = delx * delx + dely * dely + delz * delz;
+      const int tt = ti * a.ntp1 + xj[u].w;
+      // (the cutoff in units only selects pairs: its rounding biases no term)
+      const float cs = SINGLE ? cutsq1 : (ISO ? tabf[0 * nt2 + tt] * q2h : tabf[0 * nt2 + tt]);
+      const float c1 = SINGLE ? lj1 : tabf[1 * nt2 + tt];
+      const float c2 = SINGLE ? lj2 : tabf[2 * nt2 + tt];
+      const bool in = rsq < cs && rsq > 0.f;
+      const float r2inv = ISO ? md_qlen(rcp_approx_f32(rsq), q2h, q2l) : rcp_approx_f32(rsq);
+      const float r6inv = r2inv * r2inv * r2inv;
+      const float fpair = in ? r6inv * (c1 * r6inv - c2) * r2inv : 0.f;
+      cfx = fmaf(delx, fpair, cfx);
+      cfy = fmaf(dely, fpair, cfy);
+      cfz = fmaf(delz, fpair, cfz);
+      if (EV) {
+        const float c3 = SINGLE ? lj3 : tabf[3 * nt2 + tt];
+        const float c4 = SINGLE ? lj4 : tabf[4 * nt2 + tt];
+        const float co = SINGLE ? off : tabf[5 * nt2 + tt];
+        const float evdwl = in ? r6inv * (c3 * r6inv - c4) - co : 0.f;
+        ce[0] = fmaf(0.5f, evdwl, ce[0]);
+        // the virial wants separations in length units
+        const float lx = ISO ? md_qlen(delx, qx, qxl) : delx,
+                    ly = ISO ? md_qlen(dely, qx, qxl) : dely,
+                    lz = ISO ? md_qlen(delz, qx, qxl) : delz;
+        const float hf = 0.5f * fpair;
+        ce[1] = fmaf(lx * lx, hf, ce[1]);
+        ce[2] = fmaf(ly * ly, hf, ce[2]);
+        ce[3] = fmaf(lz * lz, hf, ce[3]);
+        ce[4] = fmaf(lx * ly, hf, ce[4]);
+        ce[5] = fmaf(lx * lz, hf, ce[5]);
+        ce[6] = fmaf(ly * lz, hf, ce[6]);
+      }
     }
-    const int4 xi = xq[i];
-    const int ti = xi.w;
-    const int nslab = (a.numneigh[i] + 3) >> 2;
-    const int4 *nl4 = reinterpret_cast<const int4 *>(a.nlist);
+    // the energy and virial terms join the FP64 sums once per group, as the
+    // forces do
+    if (EV)
+#pragma unroll
+      for (int k = 0; k < 7; k++) acc[k] += (double)ce[k];
+    if (ISO) {
+      fx = fma((double)cfx, qd, fx);
+      fy = fma((double)cfy, qd, fy);
+      fz = fma((double)cfz, qd, fz);
+    } else {
+      fx += (double)cfx;
+      fy += (double)cfy;
+      fz += (double)cfz;
+    }
+  };
+  if constexpr (TPA == 1) {
     // Four slabs (16 entries) per iteration: the sixteen gathers are in
     // flight together, and the next four slabs' entries are loaded
     // (streaming, evict-first) before these are used, so the list's DRAM
     // latency overlaps the gathers and the arithmetic of the slabs before
     // them.  Slabs past the atom's count, and the tail of its last slab, hold
-    // pad entries, which the r^2 > 0 test rejects, so no per-entry count check
-    // is needed.
-    const int pe = md_pad_entry(i);
+    // pad entries, which the r^2 > 0 test rejects, so no per-entry count
+    // check is needed.  The forces of each eight entries are summed in FP32.
+    const int4 *nl4 = reinterpret_cast<const int4 *>(a.nlist);
     const int4 pad4 = make_int4(pe, pe, pe, pe);
-    auto slab = [&](int c) {
-      return c < nslab ? __ldcs(&nl4[(size_t)c * a.stride + i]) : pad4;
-    };
-    int c4 = lane;
-    int4 a0 = slab(c4), a1 = slab(c4 + TPA), a2 = slab(c4 + 2 * TPA), a3 = slab(c4 + 3 * TPA);
+    auto slab = [&](int c) { return c < nslab ? __ldcs(&nl4[(size_t)c * a.stride + i]) : pad4; };
+    int c4 = 0;
+    int4 a0 = slab(0), a1 = slab(1), a2 = slab(2), a3 = slab(3);
     while (c4 < nslab) {
-      const int cn = c4 + 4 * TPA;
-      const int4 b0 = slab(cn), b1 = slab(cn + TPA), b2 = slab(cn + 2 * TPA),
-                 b3 = slab(cn + 3 * TPA);
+      const int cn = c4 + 4;
+      const int4 b0 = slab(cn), b1 = slab(cn + 1), b2 = slab(cn + 2), b3 = slab(cn + 3);
       const unsigned int eall[16] = {(unsigned)a0.x, (unsigned)a0.y, (unsigned)a0.z, (unsigned)a0.w,
                                      (unsigned)a1.x, (unsigned)a1.y, (unsigned)a1.z, (unsigned)a1.w,
                                      (unsigned)a2.x, (unsigned)a2.y, (unsigned)a2.z, (unsigned)a2.w,
@@ -245,77 +327,27 @@ __device__ __forceinline__ void lj_atom_mixed(const PairArgs &a, const int4 *__r
       int4 xall[16];
 #pragma unroll
       for (int u = 0; u < 16; u++) xall[u] = __ldg(&xq[md_entry_j(eall[u])]);
-      // the pair forces of each group of eight entries are summed in FP32,
-      // the group sum is added to the atom's FP64 accumulator
-#pragma unroll
-      for (int h = 0; h < 2; h++) {
-        const int4 *xj = xall + 8 * h;
-        float cfx = 0.f, cfy = 0.f, cfz = 0.f;
-        float ce[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // EV: this group's FP32 sums
-#pragma unroll
-        for (int u = 0; u < 8; u++) {
-          // x_i - x_j at the minimum image, in units (ISO) or lengths
-          float delx = md_qdiff(xi.x, xj[u].x);
-          float dely = md_qdiff(xi.y, xj[u].y);
-          float delz = md_qdiff(xi.z, xj[u].z);
-          if (!ISO) {
-            delx = md_qlen(delx, qx, qxl);
-            dely = md_qlen(dely, qy, qyl);
-            delz = md_qlen(delz, qz, qzl);
-          }
-          const float rsq = delx * delx + dely * dely + delz * delz;
-          const int tt = ti * a.ntp1 + xj[u].w;
-          // (the cutoff in units only selects pairs: its rounding biases no term)
-          const float cs = SINGLE ? cutsq1 : (ISO ? tabf[0 * nt2 + tt] * q2h : tabf[0 * nt2 + tt]);
-          const float c1 = SINGLE ? lj1 : tabf[1 * nt2 + tt];
-          const float c2 = SINGLE ? lj2 : tabf[2 * nt2 + tt];
-          const bool in = rsq < cs && rsq > 0.f;
-          const float r2inv =
-              ISO ? md_qlen(rcp_approx_f32(rsq), q2h, q2l) : rcp_approx_f32(rsq);
-          const float r6inv = r2inv * r2inv * r2inv;
-          const float fpair = in ? r6inv * (c1 * r6inv - c2) * r2inv : 0.f;
-          cfx = fmaf(delx, fpair, cfx);
-          cfy = fmaf(dely, fpair, cfy);
-          cfz = fmaf(delz, fpair, cfz);
-          if (EV) {
-            const float c3 = SINGLE ? lj3 : tabf[3 * nt2 + tt];
-            const float c4 = SINGLE ? lj4 : tabf[4 * nt2 + tt];
-            const float co = SINGLE ? off : tabf[5 * nt2 + tt];
-            const float evdwl = in ? r6inv * (c3 * r6inv - c4) - co : 0.f;
-            ce[0] = fmaf(0.5f, evdwl, ce[0]);
-            // the virial wants separations in length units
-            const float lx = ISO ? md_qlen(delx, qx, qxl) : delx,
-                        ly = ISO ? md_qlen(dely, qx, qxl) : dely,
-                        lz = ISO ? md_qlen(delz, qx, qxl) : delz;
-            const float hf = 0.5f * fpair;
-            ce[1] = fmaf(lx * lx, hf, ce[1]);
-            ce[2] = fmaf(ly * ly, hf, ce[2]);
-            ce[3] = fmaf(lz * lz, hf, ce[3]);
-            ce[4] = fmaf(lx * ly, hf, ce[4]);
-            ce[5] = fmaf(lx * lz, hf, ce[5]);
-            ce[6] = fmaf(ly * lz, hf, ce[6]);
-          }
-        }
-        // the energy and virial terms join the FP64 sums once per group, as
-        // the forces do
-        if (EV)
-#pragma unroll
-          for (int k = 0; k < 7; k++) acc[k] += (double)ce[k];
-        if (ISO) {
-          fx = fma((double)cfx, qd, fx);
-          fy = fma((double)cfy, qd, fy);
-          fz = fma((double)cfz, qd, fz);
-        } else {
-          fx += (double)cfx;
-          fy += (double)cfy;
-          fz += (double)cfz;
-        }
-      }
+      group(xall, std::integral_constant<int, 8>{});
+      group(xall + 8, std::integral_constant<int, 8>{});
       a0 = b0;
       a1 = b1;
       a2 = b2;
       a3 = b3;
       c4 = cn;
+    }
+  } else {
+    // G entries per lane per iteration (their gathers in flight together),
+    // the next G entries already loading; entries past the last slab are
+    // pads.  The forces of each lane's G entries are summed in FP32.
+    constexpr int G = TPA == 2 ? 8 : 4;
+    ListWalk<TPA, G> w(a.nlist, a.stride, i, nslab, lane, (unsigned)pe);
+    while (w.more()) {
+      w.prefetch();
+      int4 xall[G];
+#pragma unroll
+      for (int u = 0; u < G; u++) xall[u] = __ldg(&xq[md_entry_j(w.cur[u])]);
+      group(xall, std::integral_constant<int, G>{});
+      w.advance();
     }
   }
 }

@@ -167,6 +167,71 @@ def test_lj32k_gaussian_mixed(lj32k):
     check_forces(device(case, "mixed", snap), snap, MIXED_TOL)
 
 
+@pytest.mark.parametrize("tpa", [1, 2, 4, 8, 16, 32])
+def test_lj32k_mixed_every_launch_shape(lj32k, tpa):
+    """The mixed pair kernel in each launch shape: one thread per atom walks
+    its slabs; several lanes per atom take consecutive list entries."""
+    case, snap = lj32k
+    d = device(case, "mixed", snap)
+    d.set_launch(tpa)
+    check_forces(d, snap, MIXED_TOL)
+
+
+@pytest.mark.parametrize("tpa", [1, 2, 4, 8])
+@pytest.mark.parametrize("precision,bar", [("fp64", 1e-9), ("mixed", 1e-4)])
+def test_lj32k_step_every_launch_shape(lj32k, precision, bar, tpa):
+    """The one-launch MD step (forces and both half-steps) in each launch
+    shape.  The engine and the oracle both start from the oracle's state
+    after 10 steps and run 20 more with the same list schedule (a rebuild at
+    the start and every 20 steps after it), so they use the same lists.  With
+    rebuilds every 20 steps and no displacement check, some pairs come
+    within the cutoff between rebuilds, so two runs with different schedules
+    legitimately drift apart by ~1e-4 in 20 steps.  Positions must then agree
+    within 1e-9 (FP64).  For mixed precision, a pair within FP32 rounding of
+    the cutoff may be counted on one side and not the other for a step,
+    which moves positions by up to ~1e-5, so the bar is 1e-4.  A wiring
+    mistake in the step (a force lost or doubled) moves them by ~1e-2."""
+    case, _ = lj32k
+    steps = 20
+    s10 = oracle_sim(case)
+    s10.setup()
+    s10.run(10)
+    o10 = np.argsort(s10.tag)
+    x10, t10, v10 = s10.x[o10], s10.type[o10], s10.v[o10]
+    s10.close()
+    o = oracle.OracleSim(case["units"], threads=THREADS)
+    o.box([0.0, 0.0, 0.0], case["hi"])
+    o.atoms(x10, v=v10)
+    o.mass(1, 1.0)
+    o.lj_cut(2.5)
+    o.lj_coeff(1, 1, 1.0, 1.0, 2.5)
+    o.neighbor(case["skin"], case["every"], case["delay"], case["check"], 1000)
+    o.timestep(0.005)
+    o.setup()
+    o.run(steps)
+    order = np.argsort(o.tag)
+    d = System(case["units"], precision)
+    d.set_box([0.0, 0.0, 0.0], case["hi"])
+    p = PairLJCut(2.5)
+    p.coeff(1, 1, 1.0, 1.0, 2.5)
+    d.set_pair(p)
+    d.set_mass([1.0])
+    d.set_neighbor(case["skin"], case["every"], case["delay"], case["check"])
+    d.set_launch(tpa)
+    d.set_atoms(x10, t10, v10)
+    d.set_timestep(0.005)
+    d.setup()
+    d.run(steps)
+    st = d.download()
+    # the two runs wrap atoms into the box at different steps
+    d_x = st["x"] - o.x[order]
+    d_x -= case["hi"] * np.round(d_x / case["hi"])
+    dx = float(np.max(np.abs(d_x)))
+    print(precision, "tpa", tpa, "max |dx|", dx)
+    assert dx <= bar, dx
+    o.close()
+
+
 # ---------------------------------------------------------------------------
 # 32,000-atom EAM, synthetic 5000-point setfl tables
 
