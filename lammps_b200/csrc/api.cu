@@ -520,13 +520,15 @@ int rebuild_sync(b200_ctx *c) {
 // pair pass's (at 32,000 LJ atoms, mixed: 2 and 4 tie for the pair pass, 4 is
 // 6 % faster for the step).  The steps run with a zero timestep, so
 // positions and velocities do not change; the status words, the decision
-// count and the mailbox that the steps advance are put back afterwards.
+// count and the mailbox that the steps advance are put back afterwards.  It
+// runs at setup and, once, between two steps of the first run.
 int autotune_step(b200_ctx *c) {
   int status_save[ST_COUNT], dcount_save = 0;
   int rc0 = small_read(c, status_save, c->status, sizeof(status_save));
   if (!rc0) rc0 = small_read(c, &dcount_save, c->dec_count, sizeof(int));
   if (rc0) return rc0;
   const int mail_save[2] = {c->mail_host[0], c->mail_host[1]};
+  const int parity_save = c->pos_parity;
   const bool lj = c->pstyle == B200_PAIR_LJ_CUT;
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
@@ -538,24 +540,40 @@ int autotune_step(b200_ctx *c) {
     md_swap_positions(c);
     return e;
   };
+  // one timed block of `reps` steps at the current shape
+  auto block = [&](int reps, float &ms) -> cudaError_t {
+    cudaError_t e = cudaEventRecord(e0, c->stream);
+    for (int r = 0; r < reps && e == cudaSuccess; r++) e = step();
+    if (e == cudaSuccess) e = cudaEventRecord(e1, c->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    return e;
+  };
+  // Warm-up (clocks up, caches filled) at one thread per atom, which also
+  // sizes the timed blocks: about 2 ms of steps, 5 to 40 of them (a block
+  // of five 40-microsecond steps at 32,000 atoms picked different shapes
+  // from one context to the next).
   int rc = B200_OK;
+  c->tpa = 1;
+  float ms = 0.f;
+  cudaError_t e = block(10, ms);
+  int reps = 5;
+  if (e == cudaSuccess) reps = std::max(5, std::min(40, (int)ceilf(20.0f / std::max(ms, 1e-3f))));
+  else rc = set_err(c, B200_ERR_CUDA, "launch-shape search: %s", cudaGetErrorString(e));
   for (int round = 0; round < 3 && !rc; round++)
     for (int k = 0; k < 4 && !rc; k++) {
       c->tpa = cand[k];
-      cudaError_t e = step();
-      if (e == cudaSuccess) e = cudaEventRecord(e0, c->stream);
-      for (int r = 0; r < 5 && e == cudaSuccess; r++) e = step();
-      if (e == cudaSuccess) e = cudaEventRecord(e1, c->stream);
-      if (e == cudaSuccess) e = cudaEventSynchronize(e1);
-      float ms = 0.f;
-      if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+      e = step();
+      if (e == cudaSuccess) e = block(reps, ms);
       if (e != cudaSuccess) rc = set_err(c, B200_ERR_CUDA, "launch-shape search: %s",
                                          cudaGetErrorString(e));
       else if (ms < tmin[k]) tmin[k] = ms;
     }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  if (c->pos_parity) md_swap_positions(c);  // 3 x 4 x 6 swaps: back to the first buffer
+  // back to the buffer the search started from (after a zero-timestep step
+  // both buffers hold the same positions)
+  if (c->pos_parity != parity_save) md_swap_positions(c);
   CK(cudaMemcpyAsync(c->status, status_save, sizeof(status_save), cudaMemcpyHostToDevice,
                      c->stream));
   CK(cudaMemcpyAsync(c->dec_count, &dcount_save, sizeof(int), cudaMemcpyHostToDevice, c->stream));
@@ -575,14 +593,16 @@ int autotune_step(b200_ctx *c) {
   return B200_OK;
 }
 
+// a single box of lj/cut (equal edges in the mixed form) or eam steps
+// through the one-launch step kernel
+static bool step_form(const b200_ctx *c) {
+  return c->nrep == 0 && !c->ghosts_on &&
+         ((c->pstyle == B200_PAIR_LJ_CUT && (c->prec != B200_PREC_MIXED || md_q_iso(c))) ||
+          c->pstyle == B200_PAIR_EAM);
+}
+
 int autotune(b200_ctx *c) {
-  // a single box of lj/cut (equal edges in the mixed form) or eam steps
-  // through the one-launch step kernel: time that
-  const bool step_form =
-      c->nrep == 0 && !c->ghosts_on &&
-      ((c->pstyle == B200_PAIR_LJ_CUT && (c->prec != B200_PREC_MIXED || md_q_iso(c))) ||
-       c->pstyle == B200_PAIR_EAM);
-  if (step_form) return autotune_step(c);
+  if (step_form(c)) return autotune_step(c);
   // Launch-shape search: time the force pass for each threads-per-atom
   // value and keep the fastest (ties to fewer threads per atom).  Each
   // candidate is timed in three rounds of five passes, the rounds
@@ -1695,6 +1715,10 @@ int b200_setup(b200_ctx *c, double *row) {
     if (c->tpa == 0) {
       rc = autotune(c);
       if (rc) return rc;
+      // the step-form search leaves the state as it found it, so the first
+      // run can repeat it between two of its steps
+      c->retune_pending = step_form(c);
+      c->retune_step = -1;
     }
     c->tuned = true;
   }
@@ -1767,8 +1791,23 @@ int b200_run(b200_ctx *c, int nsteps, double dt, double ftm2v, int thermo_every,
   long long s = step0 + 1;
   int replays = 0;
   bool force_build = false;
+  // the one repeat of the launch-shape search, retune_steps steps into the
+  // first run after the setup-time search, at a chunk boundary (whole
+  // steps, forces stored)
+  constexpr int retune_steps = 50;
+  if (c->retune_pending && c->retune_step < 0) c->retune_step = step0 + retune_steps + 1;
   while (s <= last) {
-    const long long s_end = (last - s + 1) > chunk ? s + chunk - 1 : last;
+    if (c->retune_pending && s >= c->retune_step) {
+      int rc = autotune_step(c);
+      if (rc) return rc;
+      c->retune_pending = false;
+      invalidate_graphs(c);
+      rc = ensure_graphs(c, dtv, dtf, ftm2v);
+      if (rc) return rc;
+    }
+    long long s_end = (last - s + 1) > chunk ? s + chunk - 1 : last;
+    if (c->retune_pending && c->retune_step > s && c->retune_step - 1 < s_end)
+      s_end = c->retune_step - 1;
     // A list that outgrows its capacity during a chunk is recovered by
     // replaying the chunk from this snapshot with a larger list, starting
     // with a forced rebuild (the reference instead stops with "Neighbor list
@@ -1998,6 +2037,7 @@ int b200_set_launch(b200_ctx *c, int tpa, int block) {
   if (block != 0 && block != 128) return set_err(c, B200_ERR_ARG, "block size must be 128");
   c->tpa = tpa;
   c->tuned = tpa != 0;
+  c->retune_pending = false;
   invalidate_graphs(c);
   return B200_OK;
 }

@@ -187,6 +187,11 @@ struct b200_ctx {
   // launch shape of the pair kernels
   int tpa = 0, block = 128;
   bool tuned = false;
+  // The launch-shape search made at setup ran on the caller's starting
+  // state (often a perfect lattice, where the best shape can differ from
+  // the thermal one); the first run repeats it once, retune_steps steps in.
+  bool retune_pending = false;
+  long long retune_step = -1;
 
   // one-launch replica step (b200_set_replica_step): each thread-block
   // cluster of rep_cs CTAs of rep_block threads owns a fixed set of whole

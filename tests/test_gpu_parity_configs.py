@@ -177,22 +177,11 @@ def test_lj32k_mixed_every_launch_shape(lj32k, tpa):
     check_forces(d, snap, MIXED_TOL)
 
 
-@pytest.mark.parametrize("tpa", [1, 2, 4, 8])
-@pytest.mark.parametrize("precision,bar", [("fp64", 1e-9), ("mixed", 1e-4)])
-def test_lj32k_step_every_launch_shape(lj32k, precision, bar, tpa):
-    """The one-launch MD step (forces and both half-steps) in each launch
-    shape.  The engine and the oracle both start from the oracle's state
-    after 10 steps and run 20 more with the same list schedule (a rebuild at
-    the start and every 20 steps after it), so they use the same lists.  With
-    rebuilds every 20 steps and no displacement check, some pairs come
-    within the cutoff between rebuilds, so two runs with different schedules
-    legitimately drift apart by ~1e-4 in 20 steps.  Positions must then agree
-    within 1e-9 (FP64).  For mixed precision, a pair within FP32 rounding of
-    the cutoff may be counted on one side and not the other for a step,
-    which moves positions by up to ~1e-5, so the bar is 1e-4.  A wiring
-    mistake in the step (a force lost or doubled) moves them by ~1e-2."""
-    case, _ = lj32k
-    steps = 20
+def _run_from_oracle_state(case, precision, tpa, steps):
+    """Largest position difference (minimum image) between the engine and
+    the oracle after `steps` steps from the oracle's state after 10 steps,
+    both with the same list schedule (a rebuild at the start and every 20
+    steps after it)."""
     s10 = oracle_sim(case)
     s10.setup()
     s10.run(10)
@@ -209,7 +198,8 @@ def test_lj32k_step_every_launch_shape(lj32k, precision, bar, tpa):
     o.timestep(0.005)
     o.setup()
     o.run(steps)
-    order = np.argsort(o.tag)
+    ox = o.x[np.argsort(o.tag)]
+    o.close()
     d = System(case["units"], precision)
     d.set_box([0.0, 0.0, 0.0], case["hi"])
     p = PairLJCut(2.5)
@@ -217,19 +207,49 @@ def test_lj32k_step_every_launch_shape(lj32k, precision, bar, tpa):
     d.set_pair(p)
     d.set_mass([1.0])
     d.set_neighbor(case["skin"], case["every"], case["delay"], case["check"])
-    d.set_launch(tpa)
+    if tpa:
+        d.set_launch(tpa)
     d.set_atoms(x10, t10, v10)
     d.set_timestep(0.005)
     d.setup()
     d.run(steps)
     st = d.download()
+    d.close()
     # the two runs wrap atoms into the box at different steps
-    d_x = st["x"] - o.x[order]
+    d_x = st["x"] - ox
     d_x -= case["hi"] * np.round(d_x / case["hi"])
-    dx = float(np.max(np.abs(d_x)))
+    return float(np.max(np.abs(d_x)))
+
+
+@pytest.mark.parametrize("tpa", [1, 2, 4, 8])
+@pytest.mark.parametrize("precision,bar", [("fp64", 1e-9), ("mixed", 1e-4)])
+def test_lj32k_step_every_launch_shape(lj32k, precision, bar, tpa):
+    """The one-launch MD step (forces and both half-steps) in each launch
+    shape, 20 steps against the oracle's.  Two runs whose lists are rebuilt at
+    different steps legitimately drift apart by ~1e-4 in 20 steps here: with
+    rebuilds every 20 steps and no displacement check, pairs come within the
+    cutoff between rebuilds.  With the same schedule, positions must agree
+    within 1e-9 (FP64).  For mixed precision, a pair within FP32 rounding of
+    the cutoff may be counted on one side and not the other for a step,
+    which moves positions by up to ~1e-5, so the bar is 1e-4.  A wiring
+    mistake in the step (a force lost or doubled) moves them by ~1e-2."""
+    case, _ = lj32k
+    dx = _run_from_oracle_state(case, precision, tpa, 20)
     print(precision, "tpa", tpa, "max |dx|", dx)
     assert dx <= bar, dx
-    o.close()
+
+
+@pytest.mark.parametrize("precision,bar", [("fp64", 1e-9), ("mixed", 1e-3)])
+def test_lj32k_run_repeats_the_launch_shape_search(lj32k, precision, bar):
+    """With the launch shape left to the search, the first run repeats the
+    search 50 steps in, between two steps, and may switch shapes there; the
+    state is left as it was, so 100 steps stay on the oracle's own 100.  The
+    mixed bar is wider than over 20 steps: more cutoff-rounding events, each
+    grown over more steps; a lost or doubled force would move atoms ~0.1."""
+    case, _ = lj32k
+    dx = _run_from_oracle_state(case, precision, 0, 100)
+    print(precision, "searched", "max |dx|", dx)
+    assert dx <= bar, dx
 
 
 # ---------------------------------------------------------------------------
