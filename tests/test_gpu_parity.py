@@ -128,10 +128,12 @@ def test_device_run_reproduces_reference_log(name):
 
 def test_eager_launches_match_graph_replay():
     """The graph path (device-conditional rebuild) and the kernel-by-kernel
-    path run the same kernels in the same order: identical thermo."""
+    path run the same kernels in the same order: identical thermo.  Both
+    contexts get the same launch shape (the search picks one by timing, so
+    two searched contexts may sum in different orders)."""
     case = LOGS["potentials_lj"]
-    a = device_case(case, "fp64")
-    b = device_case(case, "fp64")
+    a = device_case(case, "fp64", tpa=2)
+    b = device_case(case, "fp64", tpa=2)
     b.set_graphs(False)
     ra = [a.setup()] + a.run(case["run"])
     rb = [b.setup()] + b.run(case["run"])
@@ -144,10 +146,11 @@ def test_eager_launches_match_graph_replay():
 def test_piece_timing_keeps_the_step_form():
     """Timing mode 2 brackets whole pieces with stream events and keeps the
     run's own step form (the one-launch lj/cut step): the thermo equals an
-    untimed run's, every step is timed, and the force pieces carry the time."""
+    untimed run's, every step is timed, and the force pieces carry the time.
+    Both contexts get the same launch shape, as above."""
     case = LOGS["potentials_lj"]
-    a = device_case(case, "fp64")
-    b = device_case(case, "fp64")
+    a = device_case(case, "fp64", tpa=2)
+    b = device_case(case, "fp64", tpa=2)
     b.set_timing(2)
     ra = [a.setup()] + a.run(case["run"])
     rb = [b.setup()] + b.run(case["run"])
