@@ -180,8 +180,8 @@ def test_lj32k_mixed_every_launch_shape(lj32k, tpa):
 def _run_from_oracle_state(case, precision, tpa, steps):
     """Largest position difference (minimum image) between the engine and
     the oracle after `steps` steps from the oracle's state after 10 steps,
-    both with the same list schedule (a rebuild at the start and every 20
-    steps after it)."""
+    both with the same list schedule (a rebuild at the start, then the
+    case's every / delay / check rule)."""
     s10 = oracle_sim(case)
     s10.setup()
     s10.run(10)
@@ -191,9 +191,12 @@ def _run_from_oracle_state(case, precision, tpa, steps):
     o = oracle.OracleSim(case["units"], threads=THREADS)
     o.box([0.0, 0.0, 0.0], case["hi"])
     o.atoms(x10, v=v10)
-    o.mass(1, 1.0)
-    o.lj_cut(2.5)
-    o.lj_coeff(1, 1, 1.0, 1.0, 2.5)
+    if case["kind"] == "lj":
+        o.mass(1, 1.0)
+        o.lj_cut(2.5)
+        o.lj_coeff(1, 1, 1.0, 1.0, 2.5)
+    else:
+        o.eam_setfl(case["setfl"], [0])
     o.neighbor(case["skin"], case["every"], case["delay"], case["check"], 1000)
     o.timestep(0.005)
     o.setup()
@@ -202,10 +205,15 @@ def _run_from_oracle_state(case, precision, tpa, steps):
     o.close()
     d = System(case["units"], precision)
     d.set_box([0.0, 0.0, 0.0], case["hi"])
-    p = PairLJCut(2.5)
-    p.coeff(1, 1, 1.0, 1.0, 2.5)
-    d.set_pair(p)
-    d.set_mass([1.0])
+    if case["kind"] == "lj":
+        p = PairLJCut(2.5)
+        p.coeff(1, 1, 1.0, 1.0, 2.5)
+        d.set_pair(p)
+        d.set_mass([1.0])
+    else:
+        p = PairEAMAlloy(1)
+        p.coeff(case["setfl"], ["Cu"])
+        d.set_pair(p)
     d.set_neighbor(case["skin"], case["every"], case["delay"], case["check"])
     if tpa:
         d.set_launch(tpa)
@@ -281,6 +289,21 @@ def test_eam32k_synthetic_fp64(eam32k):
 def test_eam32k_synthetic_mixed(eam32k):
     case, snap = eam32k
     check_forces(device(case, "mixed", snap), snap, MIXED_TOL)
+
+
+@pytest.mark.parametrize("tpa", [1, 2, 4, 8])
+@pytest.mark.parametrize("precision,bar", [("fp64", 1e-9), ("mixed", 1e-4)])
+def test_eam32k_step_every_launch_shape(eam32k, precision, bar, tpa):
+    """The one-launch EAM step (density pass, then forces and both
+    half-steps) in each launch shape, 20 steps against the oracle's from the
+    same state.  The lists are rebuilt on a displacement check with a 1.0 A
+    skin, so they hold every pair within the cutoff whenever they are
+    rebuilt.  A mixed decision that differs from the oracle's therefore
+    changes no force.  Bars as for the LJ step."""
+    case, _ = eam32k
+    dx = _run_from_oracle_state(case, precision, tpa, 20)
+    print("eam", precision, "tpa", tpa, "max |dx|", dx)
+    assert dx <= bar, dx
 
 
 # ---------------------------------------------------------------------------
