@@ -223,7 +223,12 @@ int b200_neigh_stats(b200_ctx *ctx, long long *full_total, int *ncalls, int *nda
 int b200_get_rho_fp(b200_ctx *ctx, double *rho, double *fp);
 
 /* Launch shape of the pair kernels: threads per atom (1,2,4,8,16,32; 0 = chosen by
-   the autotuner on the next b200_setup) and threads per block. */
+   the autotuner on the next b200_setup) and threads per block.  With 0, a box that
+   steps through the one-launch step kernel (a single box, no ghosts) is searched
+   once more between two steps, 50 steps into the first b200_run, on the evolved
+   state; the search leaves positions, velocities and counters as it found them.
+   Results are bit-reproducible at a fixed shape; two searched runs may pick
+   different shapes, and then differ in the last bits of FP64 sums. */
 int b200_set_launch(b200_ctx *ctx, int threads_per_atom, int block_size);
 int b200_get_launch(const b200_ctx *ctx, int *threads_per_atom, int *block_size);
 /* Phase timers of b200_run (the Timer categories of Verlet::run,
